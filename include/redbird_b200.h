@@ -1,0 +1,225 @@
+/*
+ * redbird_b200.h - C ABI of the B200 (sm_100a) FEM forward / Jacobian /
+ * Gauss-Newton engine that stands behind the redbirdpy-compatible Python API
+ * in redbirdpy_b200/.
+ *
+ * Conventions
+ *   - Every pointer is a DEVICE pointer unless its comment says "host".
+ *   - Indices are 0-based int32 (redbirdpy keeps 1-based indices in its cfg
+ *     dict; the host layer subtracts 1 once when it uploads).
+ *   - Dense multi-column arrays are row-major with the column index fastest:
+ *     X[i * ld + c] for node i, column c.  This is numpy's C order of
+ *     redbirdpy's Nn x Ncol `phi` and `rhs` arrays.
+ *   - Complex values are interleaved (re, im) pairs of the same type
+ *     (numpy complex128 / complex64 layout).
+ *   - `stream` is a cudaStream_t passed as void*; every call is asynchronous
+ *     on that stream unless noted.  No entry point allocates device memory
+ *     except where its comment says so; scratch comes from a caller-owned
+ *     workspace sized by the matching *_work_bytes() query.
+ *   - Return value: RB_OK or one of the RB_E* codes below; rb_last_error()
+ *     gives a human-readable message for the calling thread.
+ */
+#ifndef REDBIRD_B200_H
+#define REDBIRD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum rb_status {
+  RB_OK = 0,
+  RB_EARG = 1,       /* invalid argument (the message names it) */
+  RB_ECUDA = 2,      /* a CUDA runtime call failed */
+  RB_ESIZE = 3,      /* a size limit of this implementation was exceeded */
+  RB_ENOCONV = 4,    /* iterative solve hit its iteration cap (femsolve flag 1) */
+  RB_EBREAKDOWN = 5, /* Krylov breakdown (zero or non-finite pivot) */
+  RB_ENOTSPD = 6     /* Cholesky met a non-positive pivot */
+};
+
+enum rb_scalar { RB_F64 = 0, RB_C128 = 1, RB_F32 = 2, RB_C64 = 3 };
+enum rb_propkind { RB_PROP_NODE = 0, RB_PROP_ELEM = 1 };
+enum rb_precision { RB_MIXED = 0, RB_FP64 = 1 };
+
+const char* rb_last_error(void);
+int rb_version(void);
+
+/* ------------------------------------------------------------------ mesh
+ * Tetrahedral mesh resident on the device.  The incidence lists and the CSR
+ * pattern are produced once by rb_incidence / rb_csr_pattern_* and reused by
+ * every assembly.
+ */
+typedef struct rb_mesh {
+  int64_t nn, ne, nf, nnz;
+  const double* node;        /* nn x 3 (mm) */
+  const int32_t* elem;       /* ne x 4 */
+  const int32_t* face;       /* nf x 3 boundary triangles */
+  const double* area;        /* nf */
+  const int32_t* node_eptr;  /* nn+1: node -> incident tets */
+  const int32_t* node_elist; /* 4*ne, each node's tets ascending */
+  const int32_t* node_fptr;  /* nn+1: node -> incident boundary faces */
+  const int32_t* node_flist; /* 3*nf, ascending */
+  const int32_t* indptr;     /* nn+1 CSR row pointer */
+  const int32_t* indices;    /* nnz CSR column indices, ascending per row */
+} rb_mesh;
+
+/* Node -> cell incidence (cells are tets, nv=4, or triangles, nv=3):
+ * ptr[n]..ptr[n+1] lists the cells that contain node n, ascending.
+ * Replaces the per-element Python loop of `_femnz` (redbirdpy/utility.py:1020-1041)
+ * as the structure the assembly walks. */
+size_t rb_incidence_work_bytes(int64_t ncell, int32_t nv, int64_t nn);
+int rb_incidence(const int32_t* cells, int32_t nv, int64_t ncell, int64_t nn,
+                 int32_t* ptr, int32_t* list, void* work, size_t work_bytes, void* stream);
+
+/* CSR sparsity of the FEM matrix: row n holds every node that shares a tet
+ * with n (diagonal included), columns ascending.  Bit-identical to the
+ * indptr/indices scipy produces for femlhs's COO -> tocsr
+ * (redbirdpy/forward.py:254).  count fills indptr[0..nn]; the host reads
+ * indptr[nn] (= nnz), allocates indices and calls fill. */
+size_t rb_csr_pattern_work_bytes(int64_t nn);
+int rb_csr_pattern_count(const int32_t* elem, int64_t nn, const int32_t* node_eptr,
+                         const int32_t* node_elist, int32_t* indptr, void* work,
+                         size_t work_bytes, void* stream);
+int rb_csr_pattern_fill(const int32_t* elem, int64_t nn, const int32_t* node_eptr,
+                        const int32_t* node_elist, const int32_t* indptr, int32_t* indices,
+                        void* stream);
+
+/* ------------------------------------------------------------- assembly */
+typedef struct rb_optics {
+  int32_t kind;        /* RB_PROP_NODE: arrays have nn entries; RB_PROP_ELEM: ne */
+  const double* mua;   /* 1/mm */
+  const double* musp;  /* reduced scattering mus*(1-g), 1/mm */
+  const double* nref;  /* per node/elem refractive index, or NULL */
+  double nref_scalar;  /* used when nref == NULL */
+  double omega;        /* modulation angular frequency (rad/s); > 0 -> complex */
+  double reff;         /* effective reflection coefficient of the boundary */
+} rb_optics;
+
+/* femlhs (redbirdpy/forward.py:90-256): A = K*D + M*mua (+ i*omega/c*n*M)
+ * + Robin boundary terms, written into the fixed CSR pattern of `mesh`.
+ * One warp per matrix row gathers the contributions of the row's tets (the
+ * P1 gradients recomputed from node coordinates) and boundary faces in a
+ * fixed order, so results are deterministic.
+ *   val64  nnz doubles (real) or nnz complex128 (omega > 0), required
+ *   val32  optional FP32 / complex64 copy for the mixed-precision solver
+ *   dinv64 optional nn reciprocal diagonal (Jacobi), same scalar kind
+ *   dinv32 optional FP32 copy of dinv64 */
+int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, void* val64, void* val32,
+              void* dinv64, void* dinv32, void* stream);
+
+/* deldotdel (redbirdpy/utility.py:53-98): ne x 10 values V*grad(phi_i).grad(phi_j)
+ * for the pairs (0,0),(0,1),(0,2),(0,3),(1,1),(1,2),(1,3),(2,2),(2,3),(3,3). */
+int rb_deldotdel(const double* node, const int32_t* elem, int64_t ne, double* ddd, void* stream);
+
+/* ------------------------------------------------------------ optodes */
+/* Point location used by femrhs (iso2mesh.tsearchn at redbirdpy/forward.py:316,337):
+ * loc[k] = lowest tet index whose barycentric coordinates of pts[k] are all
+ * >= -1e-9 (or -1 when none), bary[k] = those 4 coordinates (NaN when
+ * outside).  pts is npts x 3. */
+int rb_tsearch(const double* node, const int32_t* elem, int64_t ne, const double* pts,
+               int64_t npts, int32_t* loc, double* bary, void* stream);
+
+/* Dense point-optode RHS (femrhs column fill, redbirdpy/forward.py:314-348):
+ * B (nn x ld, real, must be zeroed by the caller) gets bary[k][m] at row
+ * elem[loc[k]][m], column col0 + k; optodes with loc < 0 leave a zero column. */
+int rb_point_rhs(const int32_t* elem, const int32_t* loc, const double* bary, int64_t npts,
+                 int64_t nn, int64_t ld, int64_t col0, double* B, void* stream);
+
+/* femgetdet (redbirdpy/forward.py:365-442) for point detectors:
+ * detval[d * nsrc + s] = sum_m bary_det[d][m] * phi[elem[loc_det[d]][m] * ld + s]
+ * phi/detval scalar kind `kind` (RB_F64 or RB_C128). */
+int rb_femgetdet(const int32_t* elem, const int32_t* loc_det, const double* bary_det,
+                 int64_t ndet, const void* phi, int64_t ld, int64_t nsrc, int32_t kind,
+                 void* detval, void* stream);
+
+/* --------------------------------------------------------------- solve */
+typedef struct rb_csr {
+  int64_t n, nnz;
+  const int32_t* indptr;
+  const int32_t* indices;
+  const void* val64;   /* FP64 / complex128 values */
+  const void* val32;   /* FP32 / complex64 copy (required for RB_MIXED) */
+  const void* dinv64;  /* reciprocal diagonal, FP64 kind */
+  const void* dinv32;  /* reciprocal diagonal, FP32 kind (required for RB_MIXED) */
+  int32_t is_complex;
+} rb_csr;
+
+typedef struct rb_solve_opts {
+  int32_t precision;   /* RB_MIXED: FP32 Krylov + FP64 refinement; RB_FP64 */
+  int32_t max_outer;   /* refinement sweeps (mixed) */
+  int32_t maxiter;     /* cap on Krylov iterations per sweep */
+  int32_t check_every; /* iterations between host convergence checks */
+  double tol;          /* target max relative residual ||b-Ax||/||b|| */
+  double inner_tol;    /* relative residual of each FP32 correction solve */
+  int32_t profile;     /* nonzero: time the Krylov kernels with CUDA events */
+} rb_solve_opts;
+
+typedef struct rb_solve_info {
+  int32_t iters;       /* total Krylov iterations */
+  int32_t outer;       /* refinement sweeps done */
+  int32_t flag;        /* femsolve flag: 0 converged, 1 iteration cap, 2 breakdown */
+  int32_t launches;    /* kernels launched by this call */
+  double relres;       /* max over columns of ||b-Ax||/||b|| (FP64) */
+  double spmm_ms;      /* profile only: total time of the SpMM launches */
+  double update_ms;    /* profile only: total time of the vector-update launches */
+  int32_t spmm_launches;
+  int32_t update_launches;
+} rb_solve_info;
+
+/* femsolve (redbirdpy/solver.py:385-948) for all columns at once: Jacobi-
+ * preconditioned block CG (real SPD) or block COCG (complex symmetric,
+ * unconjugated bilinear form).  B is nn x nrhs real FP64; X is nn x nrhs of
+ * the matrix's FP64 kind.  All-zero columns of B give exactly zero columns
+ * (the reference skips them, solver.py:568-581). */
+size_t rb_femsolve_work_bytes(int64_t n, int64_t nrhs, int32_t is_complex, int32_t precision);
+int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs,
+                const rb_solve_opts* opts, rb_solve_info* info /* host */, void* work,
+                size_t work_bytes, void* stream);
+
+/* FP32 (complex64) copy of the values and the reciprocal diagonal of a CSR
+ * matrix given in FP64 (for matrices that did not come from rb_femlhs).
+ * Any of val32 / dinv64 / dinv32 may be NULL. */
+int rb_csr_prepare(const rb_csr* A, void* val32, void* dinv64, void* dinv32, void* stream);
+
+/* Y = A X for nrhs columns (rows of X/Y contiguous, ld = nrhs).
+ * kind: RB_F64/RB_C128 use val64, RB_F32/RB_C64 use val32. */
+int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs, void* stream);
+
+/* ------------------------------------------------------------ Jacobian */
+/* Adjoint Jacobian rows (jac, redbirdpy/forward.py:509-569) written straight
+ * to nodes, without the nsd x ne element matrix:
+ *   what RB_JAC_MUA_REF:   the reference's mua Jacobian,
+ *       Jn[k][n] = 1/4 sum_{tets e of n} Je[k][e],
+ *       Je[k][e] = -0.1 V_e (sum_i ps_i pd_i + 1/2 sum_{i!=j} ps_i pd_j)
+ *   what RB_JAC_MUA_NODAL: exact derivative of the node-based femlhs assembly
+ *       (forward.py:177-228 lumped mass weights) with respect to nodal mua at
+ *       fixed D
+ *   what RB_JAC_D:         exact derivative with respect to nodal diffusion
+ *       coefficient D: JD[k][n] = -1/4 sum_{tets e of n} ps_e^T K_e pd_e,
+ *       K_e = V grad(l_i).grad(l_j)
+ * Column map: the pairs read nc phi columns cols[0..nc); the ndet detector
+ * columns are the slots det0..det0+ndet-1.  Pair k uses source slot
+ * pair_src[k] (0..nc-1) and detector pair_det[k] (0..ndet-1).  J is nsd rows
+ * of leading dimension ldj >= nn (row k at J + k*ldj).  rmax / emax: the
+ * largest CSR row length and the largest number of tets at one node.
+ * phi_kind / out_kind: any real kind with a real kind, complex with complex;
+ * out RB_F32/RB_C64 computes in FP32.  evol: ne tet volumes; ddd: the ne x 10
+ * deldotdel rows (required for RB_JAC_D only), as jac receives them. */
+enum rb_jac_what { RB_JAC_MUA_REF = 0, RB_JAC_MUA_NODAL = 1, RB_JAC_D = 2 };
+int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
+           const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
+           const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
+           int32_t rmax, int32_t emax, const double* evol, const double* ddd, void* stream);
+
+/* Element Jacobian Je (nsd x ne, kind of phi: RB_F64 or RB_C128), the second
+ * output of jac (forward.py:527-557); src_col/det_col are phi columns. */
+int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,
+                const int32_t* src_col, const int32_t* det_col, int64_t nsd, void* je,
+                void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REDBIRD_B200_H */

@@ -43,7 +43,10 @@ def volface(elem):
     e0 = elem[:, :4].astype(np.int64) - 1
     faces = np.vstack([e0[:, [0, 2, 1]], e0[:, [0, 1, 3]], e0[:, [0, 3, 2]], e0[:, [1, 2, 3]]])
     srt = np.sort(faces, axis=1)
-    _, first, counts = np.unique(srt, axis=0, return_index=True, return_counts=True)
+    # row-wise unique through one lexicographic int64 key per sorted triple
+    nn = int(srt.max()) + 1 if srt.size else 1
+    key = (srt[:, 0] * nn + srt[:, 1]) * nn + srt[:, 2]
+    _, first, counts = np.unique(key, return_index=True, return_counts=True)
     return faces[first[counts == 1]] + 1
 
 

@@ -1,0 +1,302 @@
+// Adjoint Jacobians written straight into node rows.
+//
+// For every source/detector pair k and node n the Jacobian entry is a
+// bilinear form over the nodes N(n) that share a tet with n (the CSR row of
+// n):  J[k][n] = sum_{a,b in N(n)} phi_s(k)[a] B_n[a][b] phi_d(k)[b],  with
+// B_n = sum over tets e containing n of a 4x4 coefficient block w_e:
+//   mua, reference semantics:  w_e(i,j) = -0.025 V_e (1 + d_ij) / 2
+//        (element mass 0.1 V (diag + cross/2) then 1/4 lumping, forward.py:509-569)
+//   mua, node-based exact:     w_e(i,j) = -V_e/120 (1 + d_ni + d_nj)(1 + d_ij)
+//   D (diffusion), exact:      w_e(i,j) = -1/4 V_e grad(l_i).grad(l_j)
+// A CTA takes TN consecutive nodes: it stages the phi rows of their
+// neighbours for every column the pairs use, builds the TN small B_n, forms
+// C_n = B_n Phi_det once per detector, and then every pair costs |N(n)|
+// multiply-adds: J[k][n] = sum_a phi_s(k)[a] C_n[a][d(k)].  Threads that
+// write one row segment are consecutive, so the nsd x nn output (the
+// dominant HBM traffic) is written in full sectors.
+#include <algorithm>
+
+#include "rb_common.cuh"
+
+namespace rb {
+
+enum { JAC_MUA_REF = 0, JAC_MUA_NODAL = 1, JAC_D = 2 };
+constexpr int kJacThreads = 256;
+
+template <typename C> struct JacT;
+template <> struct JacT<float> { typedef float real; };
+template <> struct JacT<double> { typedef double real; };
+template <> struct JacT<cfloat> { typedef float real; };
+template <> struct JacT<cdouble> { typedef double real; };
+
+template <typename C, typename In> __device__ __forceinline__ C cvt(In v);
+template <> __device__ __forceinline__ float cvt<float, float>(float v) { return v; }
+template <> __device__ __forceinline__ float cvt<float, double>(double v) { return (float)v; }
+template <> __device__ __forceinline__ double cvt<double, float>(float v) { return v; }
+template <> __device__ __forceinline__ double cvt<double, double>(double v) { return v; }
+template <> __device__ __forceinline__ cfloat cvt<cfloat, cfloat>(cfloat v) { return v; }
+template <> __device__ __forceinline__ cfloat cvt<cfloat, cdouble>(cdouble v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ cdouble cvt<cdouble, cfloat>(cfloat v) { return make_double2(v.x, v.y); }
+template <> __device__ __forceinline__ cdouble cvt<cdouble, cdouble>(cdouble v) { return v; }
+
+__device__ __forceinline__ float scale_r(float b, float v) { return b * v; }
+__device__ __forceinline__ double scale_r(double b, double v) { return b * v; }
+__device__ __forceinline__ cfloat scale_r(float b, cfloat v) { return make_float2(b * v.x, b * v.y); }
+__device__ __forceinline__ cdouble scale_r(double b, cdouble v) { return make_double2(b * v.x, b * v.y); }
+
+struct JacArgs {
+  const int32_t* indptr;
+  const int32_t* indices;
+  const int32_t* eptr;
+  const int32_t* elist;
+  const int32_t* elem;
+  const double* evol;   // ne tet volumes
+  const double* ddd;    // ne x 10 deldotdel (RB_JAC_D only)
+  int64_t nn;
+  const int32_t* cols;  // nc staged phi columns
+  int32_t nc, det0, ndet;
+  const int32_t* psrc;  // nsd: staged slot of the source column
+  const int32_t* pdet;  // nsd: 0..ndet-1 index of the detector
+  int64_t nsd, ld, ldj;
+  int32_t rmax, emax, what;
+};
+
+// smem layout (bytes), TN nodes:
+//   phi [TN][rmax][nc] C | Bm [TN][rmax][rmax] R | Cm [TN][rmax][ndet] C |
+//   W [TN][emax][16] R | EN [TN][emax] int4 | nb [TN][rmax] int | rn [TN] int
+template <typename C>
+__host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, int emax) {
+  typedef typename JacT<C>::real R;
+  size_t s = 0;
+  s += (size_t)TN * rmax * nc * sizeof(C);
+  s += (size_t)TN * rmax * rmax * sizeof(R);
+  s += (size_t)TN * rmax * ndet * sizeof(C);
+  s += (size_t)TN * emax * 16 * sizeof(R);
+  s += (size_t)TN * emax * sizeof(int4);
+  s += (size_t)TN * rmax * sizeof(int) + TN * sizeof(int) * 2;
+  return (s + 15) / 16 * 16;
+}
+
+template <typename C, typename In, int TN>
+__global__ void __launch_bounds__(kJacThreads)
+jac_kernel(JacArgs a, const In* __restrict__ phi, C* __restrict__ J) {
+  typedef typename JacT<C>::real R;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax;
+  C* sphi = reinterpret_cast<C*>(smem);
+  R* sB = reinterpret_cast<R*>(sphi + (size_t)TN * rmax * nc);
+  C* sC = reinterpret_cast<C*>(sB + (size_t)TN * rmax * rmax);
+  R* sW = reinterpret_cast<R*>(sC + (size_t)TN * rmax * nd);
+  int4* sEN = reinterpret_cast<int4*>(sW + (size_t)TN * emax * 16);
+  int* snb = reinterpret_cast<int*>(sEN + (size_t)TN * emax);
+  int* srn = snb + TN * rmax;
+  int* sek = srn + TN;
+
+  const int64_t n0 = (int64_t)blockIdx.x * TN;
+  const int tid = threadIdx.x;
+  // 1. rows and incident tets of the TN nodes
+  if (tid < TN) {
+    const int64_t n = n0 + tid;
+    srn[tid] = (n < a.nn) ? a.indptr[n + 1] - a.indptr[n] : 0;
+    sek[tid] = (n < a.nn) ? a.eptr[n + 1] - a.eptr[n] : 0;
+  }
+  __syncthreads();
+  for (int i = tid; i < TN * rmax; i += kJacThreads) {
+    const int t = i / rmax, q = i % rmax;
+    snb[i] = (q < srn[t]) ? a.indices[a.indptr[n0 + t] + q] : -1;
+  }
+  // per (node, incident tet): node ids and the 16 coefficients w_e(i,j)
+  for (int i = tid; i < TN * emax; i += kJacThreads) {
+    const int t = i / emax, q = i % emax;
+    if (q >= sek[t]) continue;
+    const int64_t n = n0 + t;
+    const int32_t e = a.elist[a.eptr[n] + q];
+    const int4 en = reinterpret_cast<const int4*>(a.elem)[e];
+    sEN[i] = en;
+    const int32_t nd4[4] = {en.x, en.y, en.z, en.w};
+    const double vol = a.evol[e];
+    const double* dd = a.ddd ? a.ddd + 10 * (int64_t)e : nullptr;
+    R* W = sW + (size_t)i * 16;
+    for (int ii = 0; ii < 4; ++ii)
+      for (int jj = 0; jj < 4; ++jj) {
+        double wv;
+        if (a.what == JAC_MUA_REF) {
+          wv = -0.0125 * vol * (ii == jj ? 2.0 : 1.0);
+        } else if (a.what == JAC_MUA_NODAL) {
+          const double f = 1.0 + (nd4[ii] == n) + (nd4[jj] == n);
+          wv = -vol / 120.0 * f * (ii == jj ? 2.0 : 1.0);
+        } else {
+          // upper-triangle index of (min, max) in the 10-entry deldotdel row
+          const int lo = ii < jj ? ii : jj, hi = ii < jj ? jj : ii;
+          wv = -0.25 * dd[lo * 4 - lo * (lo - 1) / 2 + (hi - lo)];
+        }
+        W[ii * 4 + jj] = (R)wv;
+      }
+  }
+  __syncthreads();
+  // staged phi rows of the neighbours, converted to the compute type
+  for (int64_t i = tid; i < (int64_t)TN * rmax * nc; i += kJacThreads) {
+    const int slot = (int)(i / nc), c = (int)(i % nc);
+    const int nb = snb[slot];
+    C v;
+    if (nb >= 0) v = cvt<C, In>(phi[(int64_t)nb * a.ld + a.cols[c]]);
+    else v = s_zero(C());
+    sphi[i] = v;
+  }
+  // 2. B_n[a][b] = sum over the node's tets of w_e at the local positions
+  for (int i = tid; i < TN * rmax * rmax; i += kJacThreads) {
+    const int t = i / (rmax * rmax), ab = i % (rmax * rmax);
+    const int ia = ab / rmax, ib = ab % rmax;
+    R s = 0;
+    if (ia < srn[t] && ib < srn[t]) {
+      const int na = snb[t * rmax + ia], nbb = snb[t * rmax + ib];
+      for (int q = 0; q < sek[t]; ++q) {
+        const int4 en = sEN[t * emax + q];
+        const int32_t nd4[4] = {en.x, en.y, en.z, en.w};
+        int pa = -1, pb = -1;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          if (nd4[m] == na) pa = m;
+          if (nd4[m] == nbb) pb = m;
+        }
+        if (pa >= 0 && pb >= 0) s += sW[((size_t)t * emax + q) * 16 + pa * 4 + pb];
+      }
+    }
+    sB[i] = s;
+  }
+  __syncthreads();
+  // 3. C_n[a][d] = sum_b B_n[a][b] phi[b][det d]
+  for (int i = tid; i < TN * rmax * nd; i += kJacThreads) {
+    const int t = i / (rmax * nd), r = i % (rmax * nd);
+    const int ia = r / nd, d = r % nd;
+    C s = s_zero(C());
+    if (ia < srn[t]) {
+      const R* Brow = sB + ((size_t)t * rmax + ia) * rmax;
+      const C* P = sphi + (size_t)t * rmax * nc + a.det0 + d;
+      for (int b = 0; b < srn[t]; ++b) s = s_add(s, scale_r(Brow[b], P[(size_t)b * nc]));
+    }
+    sC[i] = s;
+  }
+  __syncthreads();
+  // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]; t fastest -> row segments
+  const int64_t total = a.nsd * TN;
+  for (int64_t i = tid; i < total; i += kJacThreads) {
+    const int t = (int)(i % TN);
+    const int64_t k = i / TN;
+    const int64_t n = n0 + t;
+    if (n >= a.nn) continue;
+    const int ps = a.psrc[k], pd = a.pdet[k];
+    const C* P = sphi + (size_t)t * rmax * nc + ps;
+    const C* Cn = sC + (size_t)t * rmax * nd + pd;
+    C s = s_zero(C());
+    for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
+    J[k * a.ldj + n] = s;
+  }
+}
+
+// Element Jacobian, reference semantics (forward.py:509-558):
+// Je[k][e] = -0.1 V (sum_i ps_i pd_i + 1/2 sum_{i!=j} ps_i pd_j)
+template <typename T>
+__global__ void jac_elem_kernel(const double* __restrict__ evol, const int32_t* __restrict__ elem, int64_t ne,
+                                const T* __restrict__ phi, int64_t ld, const int32_t* __restrict__ scol,
+                                const int32_t* __restrict__ dcol, int64_t nsd, T* __restrict__ Je) {
+  const int64_t total = nsd * ne;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = i / ne, e = i % ne;
+    const int4 en = reinterpret_cast<const int4*>(elem)[e];
+    const int32_t nd4[4] = {en.x, en.y, en.z, en.w};
+    const double vol = evol[e];
+    const int s = scol[k], d = dcol[k];
+    T ss = s_zero(T()), sd = s_zero(T()), dg = s_zero(T());
+    for (int m = 0; m < 4; ++m) {
+      const T a = phi[(int64_t)nd4[m] * ld + s], b = phi[(int64_t)nd4[m] * ld + d];
+      ss = s_add(ss, a);
+      sd = s_add(sd, b);
+      dg = s_fma(a, b, dg);
+    }
+    // diag + (total - diag)/2 = (diag + ss*sd)/2
+    const T tot = s_fma(ss, sd, dg);
+    Je[i] = scale_r((typename JacT<T>::real)(-0.05 * vol), tot);
+  }
+}
+
+template <typename C, typename In>
+static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
+  int TN = 8;
+  const size_t budget = 110 * 1024;
+  while (TN > 1 && jac_smem<C>(TN, a.rmax, a.nc, a.ndet, a.emax) > budget) TN >>= 1;
+  const size_t sm = jac_smem<C>(TN, a.rmax, a.nc, a.ndet, a.emax);
+  if (sm > 200 * 1024) return fail(RB_ESIZE, "rb_jac: staging needs %zu bytes of shared memory", sm);
+  const unsigned g = (unsigned)ceil_div(a.nn, TN);
+#define RB_JL(TN_)                                                                                     \
+  do {                                                                                                 \
+    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)sm));                                                        \
+    jac_kernel<C, In, TN_><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, (C*)J);                        \
+  } while (0)
+  switch (TN) {
+    case 8: RB_JL(8); break;
+    case 4: RB_JL(4); break;
+    case 2: RB_JL(2); break;
+    default: RB_JL(1); break;
+  }
+#undef RB_JL
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
+            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
+            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind, int32_t rmax,
+            int32_t emax, const double* evol, const double* ddd, void* stream) {
+  if (!mesh || !phi || !cols || !pair_src || !pair_det || !J || !evol) return fail(RB_EARG, "rb_jac: null argument");
+  if (what == JAC_D && !ddd) return fail(RB_EARG, "rb_jac: RB_JAC_D needs deldotdel");
+  if (what < JAC_MUA_REF || what > JAC_D) return fail(RB_EARG, "rb_jac: bad quantity");
+  if (nc < 1 || ndet < 1 || det0 < 0 || det0 + ndet > nc || nsd < 0 || ldj < mesh->nn)
+    return fail(RB_EARG, "rb_jac: bad column map");
+  if (rmax < 1 || rmax > 64 || emax < 1 || emax > 256) return fail(RB_ESIZE, "rb_jac: rmax/emax out of range");
+  if (nsd == 0) return RB_OK;
+  JacArgs a{mesh->indptr, mesh->indices, mesh->node_eptr, mesh->node_elist, mesh->elem, evol, ddd, mesh->nn,
+            cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what};
+  cudaStream_t st = as_stream(stream);
+  const bool cin = (phi_kind == RB_C128 || phi_kind == RB_C64);
+  const bool cout = (out_kind == RB_C128 || out_kind == RB_C64);
+  if (cin != cout) return fail(RB_EARG, "rb_jac: complex phi needs a complex output kind and vice versa");
+  switch (out_kind * 4 + phi_kind) {
+    case RB_F32 * 4 + RB_F32: return launch_jac<float, float>(a, phi, J, st);
+    case RB_F32 * 4 + RB_F64: return launch_jac<float, double>(a, phi, J, st);
+    case RB_F64 * 4 + RB_F32: return launch_jac<double, float>(a, phi, J, st);
+    case RB_F64 * 4 + RB_F64: return launch_jac<double, double>(a, phi, J, st);
+    case RB_C64 * 4 + RB_C64: return launch_jac<cfloat, cfloat>(a, phi, J, st);
+    case RB_C64 * 4 + RB_C128: return launch_jac<cfloat, cdouble>(a, phi, J, st);
+    case RB_C128 * 4 + RB_C64: return launch_jac<cdouble, cfloat>(a, phi, J, st);
+    case RB_C128 * 4 + RB_C128: return launch_jac<cdouble, cdouble>(a, phi, J, st);
+    default: return fail(RB_EARG, "rb_jac: bad kinds");
+  }
+}
+
+int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,
+                const int32_t* src_col, const int32_t* det_col, int64_t nsd, void* je, void* stream) {
+  if (!mesh || !evol || !phi || !src_col || !det_col || !je) return fail(RB_EARG, "rb_jac_elem: null argument");
+  if (nsd == 0 || mesh->ne == 0) return RB_OK;
+  const unsigned g = (unsigned)std::min<int64_t>(ceil_div(nsd * mesh->ne, 256), 148 * 32);
+  cudaStream_t st = as_stream(stream);
+  if (phi_kind == RB_F64)
+    jac_elem_kernel<double><<<g, 256, 0, st>>>(evol, mesh->elem, mesh->ne, (const double*)phi, ld, src_col,
+                                               det_col, nsd, (double*)je);
+  else if (phi_kind == RB_C128)
+    jac_elem_kernel<cdouble><<<g, 256, 0, st>>>(evol, mesh->elem, mesh->ne, (const cdouble*)phi, ld,
+                                                src_col, det_col, nsd, (cdouble*)je);
+  else
+    return fail(RB_EARG, "rb_jac_elem: phi kind must be RB_F64 or RB_C128");
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,869 @@
+// Multi-RHS sparse solve: CSR SpMM with fused column reductions, Jacobi-
+// preconditioned block CG (real SPD) / block COCG (complex symmetric) on all
+// right-hand sides at once, wrapped in FP64 iterative refinement.
+//
+// Layout: every n x k multi-vector is row-major (column index fastest).  A
+// group of L lanes owns one row at a time; lane l owns the V consecutive
+// columns [l*V, l*V+V) for the whole kernel, so per-column dot products are
+// accumulated per lane (in FP64) and reduced once per block into a
+// [grid x k] partials array.  A one-block "finalize" kernel then reduces the
+// partials in fixed order and updates the per-column CG scalars on the
+// device; the host only polls a counter of active columns every few
+// iterations.  Columns are frozen individually when they converge.
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "rb_common.cuh"
+
+namespace rb {
+
+constexpr int kBlk = 256;
+constexpr int kGridMax = 148 * 8;
+
+// ----------------------------------------------------------- vector access
+template <typename T, int V>
+__device__ __forceinline__ void ldv(const T* __restrict__ p, T (&o)[V]) {
+  constexpr int B = V * (int)sizeof(T);
+  if constexpr (B % 16 == 0) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    int4* d = reinterpret_cast<int4*>(o);
+#pragma unroll
+    for (int j = 0; j < B / 16; ++j) d[j] = __ldg(q + j);
+  } else if constexpr (B % 8 == 0) {
+    const int2* q = reinterpret_cast<const int2*>(p);
+    int2* d = reinterpret_cast<int2*>(o);
+#pragma unroll
+    for (int j = 0; j < B / 8; ++j) d[j] = __ldg(q + j);
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) o[j] = p[j];
+  }
+}
+template <typename T, int V>
+__device__ __forceinline__ void stv(T* __restrict__ p, const T (&o)[V]) {
+  constexpr int B = V * (int)sizeof(T);
+  if constexpr (B % 16 == 0) {
+    int4* q = reinterpret_cast<int4*>(p);
+    const int4* d = reinterpret_cast<const int4*>(o);
+#pragma unroll
+    for (int j = 0; j < B / 16; ++j) q[j] = d[j];
+  } else if constexpr (B % 8 == 0) {
+    int2* q = reinterpret_cast<int2*>(p);
+    const int2* d = reinterpret_cast<const int2*>(o);
+#pragma unroll
+    for (int j = 0; j < B / 8; ++j) q[j] = d[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) p[j] = o[j];
+  }
+}
+
+template <typename A> __device__ __forceinline__ A acc_zero();
+template <> __device__ __forceinline__ double acc_zero<double>() { return 0.0; }
+template <> __device__ __forceinline__ cdouble acc_zero<cdouble>() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double acc_add(double a, double b) { return a + b; }
+__device__ __forceinline__ cdouble acc_add(cdouble a, cdouble b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// Block-reduce per-lane column accumulators acc[V] (lane l owns columns
+// l*V..) into part[blockIdx.x * k + c].
+template <typename A, int L, int V>
+__device__ __forceinline__ void block_colreduce(const A (&acc)[V], A* __restrict__ part, int64_t k,
+                                                A* sm /* kBlk * V */) {
+  const int lane = threadIdx.x % L, grp = threadIdx.x / L;
+  constexpr int G = kBlk / L;
+#pragma unroll
+  for (int j = 0; j < V; ++j) sm[(grp * L + lane) * V + j] = acc[j];
+  __syncthreads();
+  for (int c = threadIdx.x; c < L * V; c += kBlk) {
+    if (c < k) {
+      const int l = c / V, j = c % V;
+      A s = acc_zero<A>();
+      for (int g = 0; g < G; ++g) s = acc_add(s, sm[(g * L + l) * V + j]);
+      part[(int64_t)blockIdx.x * k + c] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------ SpMM
+// Epilogues after y = (A x)[row, cols]:
+enum { EPI_STORE = 0, EPI_PQDOT = 1, EPI_RESID = 2 };
+
+// y_row = A_row x; EPI_STORE: Y = y; EPI_PQDOT: Y = y, acc += x_row*y (unconj);
+// EPI_RESID: Y = B - y, acc += |B - y|^2   (B real FP64)
+template <typename T, int L, int V, int EPI>
+__global__ void __launch_bounds__(kBlk)
+spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+            const T* __restrict__ val, const T* __restrict__ X, T* __restrict__ Y,
+            const double* __restrict__ B, void* __restrict__ part_) {
+  // residual norms accumulate |r|^2 in double; dot products in the acc type
+  typedef std::conditional_t<EPI == EPI_RESID, double, typename Scalar<T>::acc> A;
+  A* part = reinterpret_cast<A*>(part_);
+  __shared__ A sm[(EPI == EPI_STORE) ? 1 : kBlk * V];
+  const int lane = threadIdx.x % L;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
+  alignas(16) A acc[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) acc[j] = acc_zero<A>();
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+    const int32_t b = indptr[row], e = indptr[row + 1];
+    alignas(16) T y[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) y[j] = s_zero(T());
+    if (on) {
+      for (int32_t p = b; p < e; ++p) {
+        const T a = val[p];
+        alignas(16) T xv[V];
+        ldv<T, V>(X + (int64_t)indices[p] * k + c0, xv);
+#pragma unroll
+        for (int j = 0; j < V; ++j) y[j] = s_fma(a, xv[j], y[j]);
+      }
+      if constexpr (EPI == EPI_RESID) {
+        alignas(16) double bv[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) bv[j] = B[row * k + c0 + j];
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          T r = y[j];
+          if constexpr (Scalar<T>::is_complex) {
+            r.x = (typename Scalar<T>::real)bv[j] - r.x;
+            r.y = -r.y;
+          } else {
+            r = (T)bv[j] - r;
+          }
+          y[j] = r;
+          acc[j] += s_abs2(r);
+        }
+      }
+      if constexpr (EPI == EPI_PQDOT) {
+        alignas(16) T xv[V];
+        ldv<T, V>(X + row * k + c0, xv);
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          if constexpr (EPI == EPI_PQDOT) acc[j] = acc_fma(xv[j], y[j], acc[j]);
+        }
+      }
+      stv<T, V>(Y + row * k + c0, y);
+    }
+  }
+  if (EPI != EPI_STORE) block_colreduce<A, L, V>(acc, part, k, sm);
+}
+
+// ------------------------------------------------------- CG vector kernels
+// Per-column state of the inner Krylov iteration (device).
+struct ColState {
+  cdouble rz;      // (r, z) unconjugated (real solves use .x)
+  cdouble pq;      // (p, A p)
+  cdouble alpha;
+  cdouble beta;
+  double rr;       // ||r||^2
+  double rr0;      // ||r_0||^2
+  int32_t active;  // column still iterating
+  int32_t status;  // 0 running/converged, 2 breakdown
+  int32_t iters;
+  int32_t pad;
+};
+
+template <typename T> __device__ __forceinline__ T from_c(cdouble v);
+template <> __device__ __forceinline__ float from_c<float>(cdouble v) { return (float)v.x; }
+template <> __device__ __forceinline__ double from_c<double>(cdouble v) { return v.x; }
+template <> __device__ __forceinline__ cfloat from_c<cfloat>(cdouble v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ cdouble from_c<cdouble>(cdouble v) { return v; }
+__device__ __forceinline__ cdouble to_c(double v) { return make_double2(v, 0.0); }
+__device__ __forceinline__ cdouble to_c(cdouble v) { return v; }
+
+// init: p = Dinv r; acc0 += r.p (unconj), acc1 += |r|^2; x = 0
+template <typename T, int L, int V>
+__global__ void __launch_bounds__(kBlk)
+cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __restrict__ R, T* __restrict__ P,
+               T* __restrict__ Xs, typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
+  typedef typename Scalar<T>::acc A;
+  __shared__ A sm[kBlk * V];
+  __shared__ double smr[kBlk * V];
+  const int lane = threadIdx.x % L;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
+  alignas(16) A arz[V];
+  alignas(16) double arr[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+    if (!on) continue;
+    const T d = dinv[row];
+    alignas(16) T r[V], p[V], z[V];
+    ldv<T, V>(R + row * k + c0, r);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      p[j] = s_mul(d, r[j]);
+      z[j] = s_zero(T());
+      arz[j] = acc_fma(r[j], p[j], arz[j]);
+      arr[j] += s_abs2(r[j]);
+    }
+    stv<T, V>(P + row * k + c0, p);
+    stv<T, V>(Xs + row * k + c0, z);
+  }
+  block_colreduce<A, L, V>(arz, part_rz, k, sm);
+  block_colreduce<double, L, V>(arr, part_rr, k, smr);
+}
+
+// x += a p; r -= a q; z = Dinv r; acc rz += r.z, rr += |r|^2
+template <typename T, int L, int V>
+__global__ void __launch_bounds__(kBlk)
+cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
+                 T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
+                 typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
+  typedef typename Scalar<T>::acc A;
+  __shared__ A sm[kBlk * V];
+  __shared__ double smr[kBlk * V];
+  const int lane = threadIdx.x % L;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
+  alignas(16) T al[V];
+  bool act[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    act[j] = on && cs[c0 + j].active;
+    al[j] = act[j] ? from_c<T>(cs[c0 + j].alpha) : s_zero(T());
+  }
+  alignas(16) A arz[V];
+  alignas(16) double arr[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+    if (!on) continue;
+    const T d = dinv[row];
+    alignas(16) T x[V], r[V], p[V], q[V];
+    ldv<T, V>(Xs + row * k + c0, x);
+    ldv<T, V>(R + row * k + c0, r);
+    ldv<T, V>(P + row * k + c0, p);
+    ldv<T, V>(Q + row * k + c0, q);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      x[j] = s_fma(al[j], p[j], x[j]);
+      r[j] = s_sub(r[j], s_mul(al[j], q[j]));
+      const T z = s_mul(d, r[j]);
+      arz[j] = acc_fma(r[j], z, arz[j]);
+      arr[j] += s_abs2(r[j]);
+    }
+    stv<T, V>(Xs + row * k + c0, x);
+    stv<T, V>(R + row * k + c0, r);
+  }
+  block_colreduce<A, L, V>(arz, part_rz, k, sm);
+  block_colreduce<double, L, V>(arr, part_rr, k, smr);
+}
+
+// p = Dinv r + beta p  (active columns only)
+template <typename T, int L, int V>
+__global__ void __launch_bounds__(kBlk)
+cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
+                  const T* __restrict__ R, T* __restrict__ P) {
+  const int lane = threadIdx.x % L;
+  const int64_t c0 = (int64_t)lane * V;
+  if (c0 >= k) return;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
+  alignas(16) T be[V];
+  bool act[V], any = false;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    act[j] = cs[c0 + j].active;
+    be[j] = from_c<T>(cs[c0 + j].beta);
+    any |= act[j];
+  }
+  if (!any) return;
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+    const T d = dinv[row];
+    alignas(16) T r[V], p[V];
+    ldv<T, V>(R + row * k + c0, r);
+    ldv<T, V>(P + row * k + c0, p);
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+      if (act[j]) p[j] = s_fma(be[j], p[j], s_mul(d, r[j]));
+    stv<T, V>(P + row * k + c0, p);
+  }
+}
+
+// ----------------------------------------------------------- finalizers
+__device__ __forceinline__ cdouble cdiv(cdouble a, cdouble b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ bool finite_c(cdouble a) { return isfinite(a.x) && isfinite(a.y); }
+
+template <typename A>
+__device__ __forceinline__ cdouble sum_part(const A* part, int nb, int64_t k, int64_t c) {
+  A s = acc_zero<A>();
+  for (int b = 0; b < nb; ++b) s = acc_add(s, part[(int64_t)b * k + c]);
+  return to_c(s);
+}
+
+// after init: rz, rr0; a column is active iff its rhs is nonzero and enabled
+template <typename A>
+__global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
+                                const int32_t* __restrict__ enable) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= k) return;
+  ColState s = cs[c];
+  s.rz = sum_part<A>(part_rz, nb, k, c);
+  s.rr = to_c(sum_part<double>(part_rr, nb, k, c)).x;
+  s.rr0 = s.rr;
+  s.active = (enable == nullptr || enable[c]) && s.rr > 0.0;
+  s.status = 0;
+  s.iters = 0;
+  s.alpha = make_double2(0, 0);
+  s.beta = make_double2(0, 0);
+  cs[c] = s;
+}
+
+template <typename A>
+__global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= k) return;
+  ColState s = cs[c];
+  if (!s.active) return;
+  s.pq = sum_part<A>(part_pq, nb, k, c);
+  if (!finite_c(s.pq) || (s.pq.x == 0.0 && s.pq.y == 0.0)) {
+    s.active = 0;
+    s.status = 2;
+    s.alpha = make_double2(0, 0);
+  } else {
+    s.alpha = cdiv(s.rz, s.pq);
+  }
+  cs[c] = s;
+}
+
+// beta = rz_new / rz; convergence ||r|| <= tol ||r0||; counts active columns
+template <typename A>
+__global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
+                                double tol2, int32_t* nactive) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int act = 0;
+  if (c < k) {
+    ColState s = cs[c];
+    if (s.active) {
+      const cdouble rzn = sum_part<A>(part_rz, nb, k, c);
+      const double rr = to_c(sum_part<double>(part_rr, nb, k, c)).x;
+      s.iters += 1;
+      s.rr = rr;
+      if (!finite_c(rzn) || !isfinite(rr)) {
+        s.active = 0;
+        s.status = 2;
+      } else if (rr <= tol2 * s.rr0) {
+        s.active = 0;
+      } else if (s.rz.x == 0.0 && s.rz.y == 0.0) {
+        s.active = 0;
+        s.status = 2;
+      } else {
+        s.beta = cdiv(rzn, s.rz);
+        s.rz = rzn;
+      }
+      cs[c] = s;
+      act = s.active;
+    }
+  }
+  act = warp_sum_i(act);
+  if ((threadIdx.x & 31) == 0 && act) atomicAdd(nactive, act);
+}
+
+// --------------------------------------------------- refinement kernels
+// relres, stagnation and the per-column scale of the next correction
+struct OuterState {
+  double bnorm;
+  double relres;
+  double prev;
+  double scale;
+  int32_t active;
+  int32_t done;  // 1 converged, 2 stagnated
+};
+
+__global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterState* os) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= k) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
+  OuterState o;
+  o.bnorm = sqrt(s);
+  o.relres = (s > 0.0) ? 1.0 : 0.0;
+  o.prev = 2.0;
+  o.scale = 0.0;
+  o.active = s > 0.0;
+  o.done = (s > 0.0) ? 0 : 1;
+  os[c] = o;
+}
+
+__global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterState* os, double tol,
+                                 double stall, int32_t* nactive) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int act = 0;
+  if (c < k) {
+    OuterState o = os[c];
+    if (o.active) {
+      double s = 0.0;
+      for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
+      const double rel = sqrt(s) / o.bnorm;
+      o.prev = o.relres;
+      o.relres = rel;
+      if (!(rel > tol)) {
+        o.active = 0;
+        o.done = 1;
+      } else if (rel > stall * o.prev) {
+        o.active = 0;
+        o.done = 2;
+      } else {
+        o.scale = 1.0 / sqrt(s);
+      }
+      os[c] = o;
+      act = o.active;
+    }
+  }
+  act = warp_sum_i(act);
+  if ((threadIdx.x & 31) == 0 && act) atomicAdd(nactive, act);
+}
+
+// r_inner = T(R64 * scale) for active columns, 0 elsewhere
+template <typename T64, typename T>
+__global__ void cast_scale_kernel(int64_t n, int64_t k, const T64* __restrict__ R64, const OuterState* os,
+                                  T* __restrict__ R) {
+  const int64_t total = n * k;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i % k;
+    const double s = os[c].active ? os[c].scale : 0.0;
+    T64 v = R64[i];
+    if constexpr (Scalar<T>::is_complex) {
+      R[i] = T{(typename Scalar<T>::real)(v.x * s), (typename Scalar<T>::real)(v.y * s)};
+    } else {
+      R[i] = (T)(v * s);
+    }
+  }
+}
+
+// X64 += D / scale for active columns
+template <typename T64, typename T>
+__global__ void correct_kernel(int64_t n, int64_t k, const T* __restrict__ D, const OuterState* os,
+                               T64* __restrict__ X) {
+  const int64_t total = n * k;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i % k;
+    if (!os[c].active) continue;
+    const double inv = 1.0 / os[c].scale;
+    T d = D[i];
+    if constexpr (Scalar<T>::is_complex) {
+      X[i].x += (double)d.x * inv;
+      X[i].y += (double)d.y * inv;
+    } else {
+      X[i] += (double)d * inv;
+    }
+  }
+}
+
+// squared column norms of a real FP64 n x k array
+template <int L, int V>
+__global__ void __launch_bounds__(kBlk)
+colnorm_kernel(int64_t n, int64_t k, const double* __restrict__ B, double* __restrict__ part) {
+  __shared__ double sm[kBlk * V];
+  const int lane = threadIdx.x % L;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
+  alignas(16) double acc[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) acc[j] = 0.0;
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+    if (!on) continue;
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const double b = B[row * k + c0 + j];
+      acc[j] += b * b;
+    }
+  }
+  block_colreduce<double, L, V>(acc, part, k, sm);
+}
+
+// ------------------------------------------------------------- dispatch
+struct Shape {
+  int L, V;
+  unsigned grid;
+};
+
+static Shape pick_shape(int64_t n, int64_t k) {
+  Shape s;
+  s.V = (k % 4 == 0) ? 4 : (k % 2 == 0) ? 2 : 1;
+  int need = (int)ceil_div(k, s.V);
+  s.L = need <= 4 ? 4 : need <= 8 ? 8 : need <= 16 ? 16 : 32;
+  const int64_t groups = ceil_div(n, 1);
+  s.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(kGridMax, ceil_div(groups, kBlk / s.L)));
+  return s;
+}
+
+#define RB_DISPATCH_LV(sh, FN)                       \
+  switch (sh.L * 8 + sh.V) {                         \
+    case 4 * 8 + 1: FN(4, 1); break;                 \
+    case 4 * 8 + 2: FN(4, 2); break;                 \
+    case 4 * 8 + 4: FN(4, 4); break;                 \
+    case 8 * 8 + 1: FN(8, 1); break;                 \
+    case 8 * 8 + 2: FN(8, 2); break;                 \
+    case 8 * 8 + 4: FN(8, 4); break;                 \
+    case 16 * 8 + 1: FN(16, 1); break;               \
+    case 16 * 8 + 2: FN(16, 2); break;               \
+    case 16 * 8 + 4: FN(16, 4); break;               \
+    case 32 * 8 + 1: FN(32, 1); break;               \
+    case 32 * 8 + 2: FN(32, 2); break;               \
+    case 32 * 8 + 4: FN(32, 4); break;               \
+    default: return fail(RB_EARG, "bad shape");      \
+  }
+
+template <typename T, int EPI>
+int spmm_t(const rb_csr& A, const T* val, const T* X, T* Y, const double* B, void* part, int64_t k,
+           const Shape& sh, cudaStream_t st) {
+#define RB_SPMM(L_, V_) \
+  spmm_kernel<T, L_, V_, EPI><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part)
+  RB_DISPATCH_LV(sh, RB_SPMM);
+#undef RB_SPMM
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+// Workspace carving --------------------------------------------------------
+struct Carver {
+  char* p;
+  size_t left;
+  size_t used = 0;
+  template <typename X> X* take(size_t count) {
+    size_t bytes = (count * sizeof(X) + 255) / 256 * 256;
+    used += bytes;
+    if (bytes > left) return nullptr;
+    X* r = reinterpret_cast<X*>(p);
+    p += bytes;
+    left -= bytes;
+    return r;
+  }
+};
+
+constexpr int64_t kMaxCols = 128;  // columns per Krylov block
+
+template <typename T64, typename T>
+struct SolveBufs {
+  T64* R64;
+  T *Xs, *R, *P, *Q;
+  void* part_a;   // kGridMax x k acc
+  double* part_b; // kGridMax x k double
+  ColState* cs;
+  OuterState* os;
+  int32_t* enable;
+  int32_t* counter;
+};
+
+template <typename T64, typename T>
+static size_t carve(Carver& cv, SolveBufs<T64, T>& b, int64_t n, int64_t k) {
+  b.R64 = cv.take<T64>(n * k);
+  b.Xs = cv.take<T>(n * k);
+  b.R = cv.take<T>(n * k);
+  b.P = cv.take<T>(n * k);
+  b.Q = cv.take<T>(n * k);
+  b.part_a = cv.take<cdouble>((size_t)kGridMax * k);
+  b.part_b = cv.take<double>((size_t)kGridMax * k);
+  b.cs = cv.take<ColState>(k);
+  b.os = cv.take<OuterState>(k);
+  b.enable = cv.take<int32_t>(k);
+  b.counter = cv.take<int32_t>(4);
+  return cv.used;
+}
+
+// Inner Jacobi-PCG / COCG on A x = R (scaled residuals), x -> b.Xs.
+// Optional per-kernel timing of the Krylov loop with CUDA events on the
+// launching stream (SpMM and vector-update kernels), read at the host sync
+// points the loop already has.
+struct KernelTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  int used = 0;
+  double spmm_ms = 0, upd_ms = 0;
+  int spmm_n = 0, upd_n = 0;
+  int ensure(int n) {
+    while ((int)ev.size() < n) {
+      cudaEvent_t e;
+      RB_CUDA_TRY(cudaEventCreate(&e));
+      ev.push_back(e);
+    }
+    return RB_OK;
+  }
+  int record(cudaStream_t st) {
+    if (!on) return RB_OK;
+    RB_TRY(ensure(used + 1));
+    RB_CUDA_TRY(cudaEventRecord(ev[used++], st));
+    return RB_OK;
+  }
+  // events come in triples: before spmm, after spmm, after update
+  int harvest() {
+    if (!on) return RB_OK;
+    for (int i = 0; i + 2 < used; i += 3) {
+      float a = 0, b = 0;
+      RB_CUDA_TRY(cudaEventElapsedTime(&a, ev[i], ev[i + 1]));
+      RB_CUDA_TRY(cudaEventElapsedTime(&b, ev[i + 1], ev[i + 2]));
+      spmm_ms += a;
+      upd_ms += b;
+      spmm_n++;
+      upd_n++;
+    }
+    used = 0;
+    return RB_OK;
+  }
+  ~KernelTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+template <typename T>
+static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, const Shape& sh, void* part_a,
+                       double* part_b, T* Xs, T* R, T* P, T* Q, ColState* cs, const int32_t* enable,
+                       int32_t* counter, double tol, int maxiter, int check_every, int* iters_out,
+                       int* launches, KernelTimer& tm, cudaStream_t st) {
+  typedef typename Scalar<T>::acc Acc;
+  const int64_t n = A.n;
+  const unsigned fg = (unsigned)ceil_div(k, 128);
+#define RB_INIT(L_, V_) \
+  cg_init_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, dinv, R, P, Xs, (Acc*)part_a, part_b)
+  RB_DISPATCH_LV(sh, RB_INIT);
+#undef RB_INIT
+  RB_LAUNCH_CHECK();
+  fin_init_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable);
+  RB_LAUNCH_CHECK();
+  *launches += 2;
+  int it = 0;
+  const double tol2 = tol * tol;
+  while (it < maxiter) {
+    const int burst = std::min(check_every, maxiter - it);
+    RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+    for (int b = 0; b < burst; ++b) {
+      RB_TRY(tm.record(st));
+      RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, sh, st)));
+      RB_TRY(tm.record(st));
+      fin_alpha_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, cs);
+#define RB_UPD(L_, V_) \
+  cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b)
+      RB_DISPATCH_LV(sh, RB_UPD);
+#undef RB_UPD
+      RB_TRY(tm.record(st));
+      if (b == burst - 1) RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+      fin_beta_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter);
+#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P)
+      RB_DISPATCH_LV(sh, RB_PUP);
+#undef RB_PUP
+      RB_LAUNCH_CHECK();
+      *launches += 5;
+    }
+    it += burst;
+    int32_t nact = 0;
+    RB_CUDA_TRY(cudaMemcpyAsync(&nact, counter, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    RB_CUDA_TRY(cudaStreamSynchronize(st));
+    RB_TRY(tm.harvest());
+    if (nact == 0) break;
+  }
+  *iters_out = it;
+  return RB_OK;
+}
+
+template <typename T64, typename T>
+static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, int64_t k, const rb_solve_opts& o,
+                       rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv, cudaStream_t st) {
+  const int64_t n = A.n;
+  const Shape sh = pick_shape(n, k);
+  const unsigned fg = (unsigned)ceil_div(k, 128);
+  const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
+  int launches = 0;
+  if (ldx != k) return fail(RB_EARG, "solve_block: internal ldx");
+  // ||b|| per column
+#define RB_CN(L_, V_) colnorm_kernel<L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, B, b.part_b)
+  RB_DISPATCH_LV(sh, RB_CN);
+#undef RB_CN
+  RB_LAUNCH_CHECK();
+  fin_bnorm_kernel<<<fg, 128, 0, st>>>(k, (int)sh.grid, b.part_b, b.os);
+  RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
+  launches += 2;
+  const double stall = 0.25;
+  KernelTimer tm;
+  tm.on = o.profile != 0;
+  int total_iters = 0, outer = 0;
+  int sweep_flag = 0;
+  for (outer = 0; outer <= o.max_outer; ++outer) {
+    // R64 = B - A X (FP64)
+    RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh, st)));
+    RB_CUDA_TRY(cudaMemsetAsync(b.counter + 1, 0, sizeof(int32_t), st));
+    fin_outer_kernel<<<fg, 128, 0, st>>>(k, (int)sh.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
+    RB_LAUNCH_CHECK();
+    launches += 2;
+    int32_t nact = 0;
+    RB_CUDA_TRY(cudaMemcpyAsync(&nact, b.counter + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    RB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (nact == 0 || outer == o.max_outer) break;
+    cast_scale_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.R64, b.os, b.R);
+    RB_LAUNCH_CHECK();
+    launches += 1;
+    int it = 0;
+    RB_TRY(inner_solve<T>(A, val, dinv, k, sh, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
+                          b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, st));
+    total_iters += it;
+    if (it >= o.maxiter) sweep_flag = 1;
+    correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, b.os, X);
+    RB_LAUNCH_CHECK();
+    launches += 1;
+  }
+  // summary
+  std::vector<OuterState> hos(k);
+  RB_CUDA_TRY(cudaMemcpyAsync(hos.data(), b.os, sizeof(OuterState) * k, cudaMemcpyDeviceToHost, st));
+  std::vector<ColState> hcs(k);
+  RB_CUDA_TRY(cudaMemcpyAsync(hcs.data(), b.cs, sizeof(ColState) * k, cudaMemcpyDeviceToHost, st));
+  RB_CUDA_TRY(cudaStreamSynchronize(st));
+  double worst = 0.0;
+  int flag = 0;
+  for (int64_t c = 0; c < k; ++c) {
+    worst = std::max(worst, hos[c].relres);
+    if (hos[c].done == 0 || (hos[c].done == 2 && hos[c].relres > 1e-10)) flag = std::max(flag, 1);
+    if (hcs[c].status == 2 && hos[c].relres > 1e-10) flag = 2;
+  }
+  if (flag == 1 && sweep_flag == 0 && worst <= o.tol) flag = 0;
+  info.iters += total_iters;
+  info.outer = std::max(info.outer, outer);
+  info.flag = std::max(info.flag, flag);
+  info.launches += launches;
+  info.relres = std::max(info.relres, worst);
+  info.spmm_ms += tm.spmm_ms;
+  info.spmm_launches += tm.spmm_n;
+  info.update_ms += tm.upd_ms;
+  info.update_launches += tm.upd_n;
+  return RB_OK;
+}
+
+template <typename T64, typename T>
+static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, const rb_solve_opts& o,
+                      rb_solve_info& info, void* work, size_t work_bytes, const T* val, const T* dinv,
+                      cudaStream_t st) {
+  const int64_t n = A.n;
+  const int64_t kb = std::min<int64_t>(nrhs, kMaxCols);
+  Carver cv{reinterpret_cast<char*>(work), work_bytes};
+  SolveBufs<T64, T> b;
+  carve(cv, b, n, kb);
+  if (!b.counter) return fail(RB_EARG, "rb_femsolve: workspace too small");
+  const bool split = nrhs > kMaxCols;
+  for (int64_t c0 = 0; c0 < nrhs; c0 += kMaxCols) {
+    const int64_t k = std::min<int64_t>(kMaxCols, nrhs - c0);
+    if (!split) {
+      RB_TRY((solve_block<T64, T>(A, B, X, k, k, o, info, b, val, dinv, st)));
+    } else {
+      return fail(RB_ESIZE, "rb_femsolve: more than %lld right-hand sides per call", (long long)kMaxCols);
+    }
+  }
+  return RB_OK;
+}
+
+// FP32 copy of the values and reciprocal diagonal of a CSR matrix
+template <typename T64, typename T32>
+__global__ void csr_prepare_kernel(int64_t n, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                   const T64* __restrict__ v64, T32* __restrict__ v32, T64* __restrict__ d64,
+                                   T32* __restrict__ d32) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x) {
+    T64 dg = s_zero(T64());
+    for (int32_t p = indptr[row]; p < indptr[row + 1]; ++p) {
+      const T64 v = v64[p];
+      if (v32) {
+        if constexpr (Scalar<T64>::is_complex) v32[p] = T32{(float)v.x, (float)v.y};
+        else v32[p] = (T32)v;
+      }
+      if (indices[p] == row) dg = s_add(dg, v);
+    }
+    T64 r;
+    if constexpr (Scalar<T64>::is_complex) {
+      const double d = dg.x * dg.x + dg.y * dg.y;
+      r = make_double2(dg.x / d, -dg.y / d);
+    } else {
+      r = 1.0 / dg;
+    }
+    if (d64) d64[row] = r;
+    if (d32) {
+      if constexpr (Scalar<T64>::is_complex) d32[row] = T32{(float)r.x, (float)r.y};
+      else d32[row] = (T32)r;
+    }
+  }
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" {
+
+size_t rb_femsolve_work_bytes(int64_t n, int64_t nrhs, int32_t is_complex, int32_t precision) {
+  const int64_t k = std::min<int64_t>(nrhs, kMaxCols);
+  Carver cv{nullptr, 0};
+  if (is_complex) {
+    if (precision == RB_FP64) { SolveBufs<cdouble, cdouble> b; return carve(cv, b, n, k) + 4096; }
+    SolveBufs<cdouble, cfloat> b;
+    return carve(cv, b, n, k) + 4096;
+  }
+  if (precision == RB_FP64) { SolveBufs<double, double> b; return carve(cv, b, n, k) + 4096; }
+  SolveBufs<double, float> b;
+  return carve(cv, b, n, k) + 4096;
+}
+
+int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs, const rb_solve_opts* opts,
+                rb_solve_info* info, void* work, size_t work_bytes, void* stream) {
+  if (!A || !B || !X || !opts || !info || !work) return fail(RB_EARG, "rb_femsolve: null argument");
+  if (nrhs < 1 || A->n < 1) return fail(RB_EARG, "rb_femsolve: empty system");
+  if (nrhs > kMaxCols) return fail(RB_ESIZE, "rb_femsolve: at most %lld right-hand sides per call", (long long)kMaxCols);
+  const rb_solve_opts& o = *opts;
+  if (o.precision != RB_MIXED && o.precision != RB_FP64) return fail(RB_EARG, "rb_femsolve: bad precision");
+  if (!A->val64 || !A->dinv64 || !A->indptr || !A->indices) return fail(RB_EARG, "rb_femsolve: matrix arrays missing");
+  if (o.precision == RB_MIXED && (!A->val32 || !A->dinv32)) return fail(RB_EARG, "rb_femsolve: mixed precision needs val32/dinv32");
+  if (o.maxiter < 1 || o.check_every < 1 || o.max_outer < 1 || !(o.tol > 0) || !(o.inner_tol > 0))
+    return fail(RB_EARG, "rb_femsolve: bad options");
+  if (work_bytes < rb_femsolve_work_bytes(A->n, nrhs, A->is_complex, o.precision))
+    return fail(RB_EARG, "rb_femsolve: workspace too small");
+  *info = rb_solve_info{};
+  cudaStream_t st = as_stream(stream);
+  if (A->is_complex) {
+    if (o.precision == RB_FP64)
+      return femsolve_t<cdouble, cdouble>(*A, B, (cdouble*)X, nrhs, o, *info, work, work_bytes,
+                                          (const cdouble*)A->val64, (const cdouble*)A->dinv64, st);
+    return femsolve_t<cdouble, cfloat>(*A, B, (cdouble*)X, nrhs, o, *info, work, work_bytes,
+                                       (const cfloat*)A->val32, (const cfloat*)A->dinv32, st);
+  }
+  if (o.precision == RB_FP64)
+    return femsolve_t<double, double>(*A, B, (double*)X, nrhs, o, *info, work, work_bytes,
+                                      (const double*)A->val64, (const double*)A->dinv64, st);
+  return femsolve_t<double, float>(*A, B, (double*)X, nrhs, o, *info, work, work_bytes,
+                                   (const float*)A->val32, (const float*)A->dinv32, st);
+}
+
+int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs, void* stream) {
+  if (!A || !X || !Y || nrhs < 1) return fail(RB_EARG, "rb_spmm: bad arguments");
+  if (nrhs > kMaxCols) return fail(RB_ESIZE, "rb_spmm: at most %lld columns", (long long)kMaxCols);
+  const Shape sh = pick_shape(A->n, nrhs);
+  cudaStream_t st = as_stream(stream);
+  switch (kind) {
+    case RB_F64: return spmm_t<double, EPI_STORE>(*A, (const double*)A->val64, (const double*)X, (double*)Y, nullptr, nullptr, nrhs, sh, st);
+    case RB_C128: return spmm_t<cdouble, EPI_STORE>(*A, (const cdouble*)A->val64, (const cdouble*)X, (cdouble*)Y, nullptr, nullptr, nrhs, sh, st);
+    case RB_F32: return spmm_t<float, EPI_STORE>(*A, (const float*)A->val32, (const float*)X, (float*)Y, nullptr, nullptr, nrhs, sh, st);
+    case RB_C64: return spmm_t<cfloat, EPI_STORE>(*A, (const cfloat*)A->val32, (const cfloat*)X, (cfloat*)Y, nullptr, nullptr, nrhs, sh, st);
+    default: return fail(RB_EARG, "rb_spmm: bad kind");
+  }
+}
+
+int rb_csr_prepare(const rb_csr* A, void* val32, void* dinv64, void* dinv32, void* stream) {
+  if (!A || !A->indptr || !A->indices || !A->val64 || A->n < 1) return fail(RB_EARG, "rb_csr_prepare: bad matrix");
+  const unsigned g = (unsigned)std::min<int64_t>(ceil_div(A->n, 256), 148 * 16);
+  cudaStream_t st = as_stream(stream);
+  if (A->is_complex)
+    csr_prepare_kernel<cdouble, cfloat><<<g, 256, 0, st>>>(A->n, A->indptr, A->indices, (const cdouble*)A->val64,
+                                                           (cfloat*)val32, (cdouble*)dinv64, (cfloat*)dinv32);
+  else
+    csr_prepare_kernel<double, float><<<g, 256, 0, st>>>(A->n, A->indptr, A->indices, (const double*)A->val64,
+                                                         (float*)val32, (double*)dinv64, (float*)dinv32);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,410 @@
+"""Device-resident FEM engine: the layer between the redbirdpy-style dict API
+and the CUDA library.
+
+``DeviceMesh`` holds one tetrahedral mesh on the GPU with the structures the
+kernels walk (node->tet and node->boundary-face incidence, the CSR pattern,
+tet volumes and deldotdel rows), built once by CUDA kernels.  The functions
+below run the hot path on device tensors only: assembly, point-optode RHS,
+the multi-RHS solve, detector readout and the adjoint Jacobians.  Nothing
+here computes on the CPU; every numerical step is a call into
+``librbb200.so``.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr, stream
+
+C0 = 299792458000.0  # mm/s (redbirdpy/forward.py:36)
+
+
+def _dev():
+    return _lib.require_cuda()
+
+
+def _i32(a, device):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=device)
+
+
+def _f64(a, device):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
+
+
+class DeviceMesh:
+    """One mesh on the device.  ``elem``/``face`` are given 1-based (cfg)."""
+
+    def __init__(self, node, elem, face, area, evol=None):
+        dev = _dev()
+        self.device = dev
+        node = np.asarray(node, dtype=np.float64)
+        self.nn = int(node.shape[0])
+        self.ne = int(elem.shape[0])
+        self.node = _f64(node[:, :3], dev)
+        self.elem = _i32(np.asarray(elem)[:, :4].astype(np.int64) - 1, dev)
+        face = np.zeros((0, 3), np.int64) if face is None else np.asarray(face)
+        self.nf = int(face.shape[0])
+        self.face = _i32(face[:, :3].astype(np.int64) - 1, dev) if self.nf else torch.zeros(3, dtype=torch.int32, device=dev)
+        self.area = _f64(area, dev) if self.nf else torch.zeros(1, dtype=torch.float64, device=dev)
+        st = stream()
+        self.eptr, self.elist = self._incidence(self.elem, 4, self.ne, st)
+        if self.nf:
+            self.fptr, self.flist = self._incidence(self.face, 3, self.nf, st)
+        else:
+            self.fptr = torch.zeros(self.nn + 1, dtype=torch.int32, device=dev)
+            self.flist = torch.zeros(1, dtype=torch.int32, device=dev)
+        # CSR pattern
+        self.indptr = torch.empty(self.nn + 1, dtype=torch.int32, device=dev)
+        wb = _lib.lib().rb_csr_pattern_work_bytes(self.nn)
+        work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        call("rb_csr_pattern_count", ptr(self.elem), self.nn, ptr(self.eptr), ptr(self.elist),
+             ptr(self.indptr), ptr(work), wb, st)
+        self.nnz = int(self.indptr[-1].item())
+        self.indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        call("rb_csr_pattern_fill", ptr(self.elem), self.nn, ptr(self.eptr), ptr(self.elist),
+             ptr(self.indptr), ptr(self.indices), st)
+        rowlen = self.indptr[1:] - self.indptr[:-1]
+        self.rmax = int(rowlen.max().item())
+        self.emax = int((self.eptr[1:] - self.eptr[:-1]).max().item())
+        self.evol = _f64(evol, dev) if evol is not None else None
+        self._ddd = None
+        self.struct = _lib.RbMesh(
+            self.nn, self.ne, self.nf, self.nnz, self.node.data_ptr(), self.elem.data_ptr(),
+            self.face.data_ptr(), self.area.data_ptr(), self.eptr.data_ptr(), self.elist.data_ptr(),
+            self.fptr.data_ptr(), self.flist.data_ptr(), self.indptr.data_ptr(), self.indices.data_ptr())
+
+    def _incidence(self, cells, nv, ncell, st):
+        p = torch.empty(self.nn + 1, dtype=torch.int32, device=self.device)
+        lst = torch.empty(max(ncell * nv, 1), dtype=torch.int32, device=self.device)
+        wb = _lib.lib().rb_incidence_work_bytes(ncell, nv, self.nn)
+        work = torch.empty(wb, dtype=torch.uint8, device=self.device)
+        call("rb_incidence", ptr(cells), nv, ncell, self.nn, ptr(p), ptr(lst), ptr(work), wb, st)
+        return p, lst
+
+    # -------------------------------------------------------------- geometry
+    @property
+    def ddd(self):
+        """Ne x 10 deldotdel rows on the device (computed once)."""
+        if self._ddd is None:
+            self._ddd = torch.empty((self.ne, 10), dtype=torch.float64, device=self.device)
+            call("rb_deldotdel", ptr(self.node), ptr(self.elem), self.ne, ptr(self._ddd), stream())
+        return self._ddd
+
+    def deldotdel_host(self):
+        return self.ddd.cpu().numpy()
+
+    def adjacency_host(self):
+        """(rows, cols, count) of the off-diagonal pattern, like _femnz
+        (utility.py:1020-1041) but with each row's columns ascending."""
+        indptr = self.indptr.cpu().numpy().astype(np.int64)
+        indices = self.indices[: self.nnz].cpu().numpy().astype(np.int64)
+        rows = np.repeat(np.arange(self.nn), np.diff(indptr))
+        off = indices != rows
+        return rows[off], indices[off], np.diff(indptr) - 1
+
+    def csr_host(self, val):
+        """scipy CSR with this pattern and the given device values."""
+        from scipy import sparse
+
+        v = val.cpu().numpy()
+        return sparse.csr_matrix((v, self.indices[: self.nnz].cpu().numpy(), self.indptr.cpu().numpy()),
+                                 shape=(self.nn, self.nn))
+
+
+def topology_of(elem, nn):
+    """A DeviceMesh built from connectivity alone (coordinates zero), enough
+    for the Jacobian kernels, which take volumes and deldotdel explicitly.
+    Cached per elem array."""
+    key = (id(elem), np.shape(elem), int(nn))
+    hit = _TOPO.get("key")
+    if hit == key:
+        return _TOPO["mesh"]
+    m = DeviceMesh(np.zeros((nn, 3)), elem, None, None)
+    _TOPO.update(key=key, mesh=m, ref=elem)
+    return m
+
+
+_TOPO = {}
+
+
+def mesh_of(cfg):
+    """The DeviceMesh cached in ``cfg['_b200']`` (rebuilt when node/elem/face change)."""
+    key = (id(cfg["node"]), id(cfg["elem"]), id(cfg.get("face")), np.shape(cfg["node"]), np.shape(cfg["elem"]),
+           np.shape(cfg.get("face")))
+    cache = cfg.get("_b200")
+    if cache is not None and cache.get("key") == key:
+        return cache["mesh"]
+    m = DeviceMesh(cfg["node"], cfg["elem"], cfg.get("face"), cfg.get("area"), cfg.get("evol"))
+    cfg["_b200"] = {"key": key, "mesh": m}
+    return m
+
+
+# ------------------------------------------------------------------ optics
+class Optics:
+    """Per-node or per-tet optical properties on the device, as femlhs reads
+    them from cfg['prop'] (redbirdpy/forward.py:126-144)."""
+
+    def __init__(self, mesh, mua, musp, nref, omega, reff):
+        dev = mesh.device
+        mua = np.asarray(mua, dtype=np.float64)
+        if len(mua) == mesh.ne:
+            self.kind = _lib.RB_PROP_ELEM
+        elif len(mua) == mesh.nn:
+            self.kind = _lib.RB_PROP_NODE
+        else:
+            raise ValueError("Property format not recognized")
+        self.mua = _f64(mua, dev)
+        self.musp = _f64(musp, dev)
+        if np.ndim(nref) > 0 and len(nref) == len(mua):
+            self.nref = _f64(nref, dev)
+            self.nref_scalar = 0.0
+        else:
+            self.nref = None
+            self.nref_scalar = float(np.asarray(nref).ravel()[0]) if np.ndim(nref) > 0 else float(nref)
+        self.omega = float(omega)
+        self.reff = float(reff)
+        self.struct = _lib.RbOptics(self.kind, self.mua.data_ptr(), self.musp.data_ptr(),
+                                    None if self.nref is None else self.nref.data_ptr(),
+                                    self.nref_scalar, self.omega, self.reff)
+
+    @staticmethod
+    def from_cfg(mesh, cfg, mode=1):
+        props = np.atleast_2d(np.asarray(cfg["prop"], dtype=np.float64))
+        nn, ne = mesh.nn, mesh.ne
+        if props.shape[0] in (nn, ne):
+            mua = props[:, 0]
+            musp = props[:, 1] * (1 - props[:, 2]) if props.shape[1] >= 3 else props[:, 1]
+            nref = props[:, 3] if props.shape[1] >= 4 else 1.37
+        elif cfg.get("seg") is not None:
+            idx = np.clip(np.asarray(cfg["seg"]).astype(np.int32), 0, props.shape[0] - 1)
+            mua = props[idx, 0]
+            musp = props[idx, 1] * (1 - props[idx, 2]) if props.shape[1] >= 3 else props[idx, 1]
+            nref = props[idx[0], 3] if props.shape[1] >= 4 else 1.37
+        else:
+            raise ValueError("Property format not recognized")
+        omega = 0.0 if mode == 2 else float(cfg.get("omega", 0) or 0)
+        reff = cfg.get("reff", 0.493)
+        return Optics(mesh, mua, musp, nref, omega, reff)
+
+
+class DeviceMatrix:
+    """An assembled FEM matrix in the mesh's CSR pattern (FP64 + FP32 copy)."""
+
+    def __init__(self, mesh, is_complex, val64, val32, dinv64, dinv32):
+        self.mesh = mesh
+        self.n = mesh.nn
+        self.nnz = mesh.nnz
+        self.is_complex = bool(is_complex)
+        self.val64, self.val32, self.dinv64, self.dinv32 = val64, val32, dinv64, dinv32
+        self.indptr, self.indices = mesh.indptr, mesh.indices
+        self.struct = _lib.RbCsr(self.n, self.nnz, self.indptr.data_ptr(), self.indices.data_ptr(),
+                                 val64.data_ptr(), val32.data_ptr(), dinv64.data_ptr(), dinv32.data_ptr(),
+                                 int(self.is_complex))
+
+    @staticmethod
+    def from_scipy(A, device=None):
+        """Upload a scipy sparse matrix (any square CSR/COO/CSC) for femsolve."""
+        from scipy import sparse
+
+        dev = device or _dev()
+        A = sparse.csr_matrix(A)
+        A.sum_duplicates()
+        A.sort_indices()
+        cplx = np.iscomplexobj(A.data)
+
+        class _Pattern:
+            pass
+
+        pat = _Pattern()
+        pat.nn = A.shape[0]
+        pat.nnz = A.nnz
+        pat.indptr = _i32(A.indptr, dev)
+        pat.indices = _i32(A.indices, dev)
+        pat.device = dev
+        if cplx:
+            v64 = torch.as_tensor(np.ascontiguousarray(A.data, dtype=np.complex128), device=dev)
+            v32 = torch.empty(A.nnz, dtype=torch.complex64, device=dev)
+            d64 = torch.empty(pat.nn, dtype=torch.complex128, device=dev)
+            d32 = torch.empty(pat.nn, dtype=torch.complex64, device=dev)
+        else:
+            v64 = _f64(A.data, dev)
+            v32 = torch.empty(A.nnz, dtype=torch.float32, device=dev)
+            d64 = torch.empty(pat.nn, dtype=torch.float64, device=dev)
+            d32 = torch.empty(pat.nn, dtype=torch.float32, device=dev)
+        m = DeviceMatrix(pat, cplx, v64, v32, d64, d32)
+        call("rb_csr_prepare", ctypes.byref(m.struct), ptr(v32), ptr(d64), ptr(d32), stream())
+        return m
+
+
+def assemble(mesh, optics):
+    """femlhs on the device -> DeviceMatrix (redbirdpy/forward.py:90-256)."""
+    dev = mesh.device
+    cplx = optics.omega > 0
+    t64 = torch.complex128 if cplx else torch.float64
+    t32 = torch.complex64 if cplx else torch.float32
+    v64 = torch.empty(mesh.nnz, dtype=t64, device=dev)
+    v32 = torch.empty(mesh.nnz, dtype=t32, device=dev)
+    d64 = torch.empty(mesh.nn, dtype=t64, device=dev)
+    d32 = torch.empty(mesh.nn, dtype=t32, device=dev)
+    call("rb_femlhs", ctypes.byref(mesh.struct), ctypes.byref(optics.struct), ptr(v64), ptr(v32), ptr(d64),
+         ptr(d32), stream())
+    return DeviceMatrix(mesh, cplx, v64, v32, d64, d32)
+
+
+# ------------------------------------------------------------------ optodes
+class Optodes:
+    """Located point optodes: loc (int32, -1 outside), bary (npts x 4)."""
+
+    def __init__(self, mesh, pts, nsrc, ndet):
+        dev = mesh.device
+        self.nsrc, self.ndet = int(nsrc), int(ndet)
+        self.pts_host = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        self.npts = self.pts_host.shape[0]
+        self.pts = _f64(self.pts_host, dev) if self.npts else torch.zeros(3, dtype=torch.float64, device=dev)
+        self.loc = torch.empty(max(self.npts, 1), dtype=torch.int32, device=dev)
+        self.bary = torch.empty((max(self.npts, 1), 4), dtype=torch.float64, device=dev)
+        if self.npts:
+            call("rb_tsearch", ptr(mesh.node), ptr(mesh.elem), mesh.ne, ptr(self.pts), self.npts, ptr(self.loc),
+                 ptr(self.bary), stream())
+
+    def rhs(self, mesh):
+        """Dense nn x (nsrc+ndet) real RHS, columns [src | det]."""
+        B = torch.zeros((mesh.nn, self.npts), dtype=torch.float64, device=mesh.device)
+        if self.npts:
+            call("rb_point_rhs", ptr(mesh.elem), ptr(self.loc), ptr(self.bary), self.npts, mesh.nn, self.npts, 0,
+                 ptr(B), stream())
+        return B
+
+    def loc_bary_host(self):
+        loc = self.loc[: self.npts].cpu().numpy().astype(np.float64)
+        bary = self.bary[: self.npts].cpu().numpy()
+        outside = loc < 0
+        loc = loc + 1.0
+        loc[outside] = np.nan
+        return loc, bary
+
+
+def locate_optodes(mesh, cfg):
+    from .utility import getoptodes
+
+    src, det, wsrc, wdet = getoptodes(cfg)
+    if (wsrc is not None and np.size(wsrc)) or (wdet is not None and np.size(wdet)):
+        raise NotImplementedError("wide-field sources/detectors are outside this engine's scope")
+    parts = [p for p in (src, det) if p is not None]
+    pts = np.vstack(parts) if parts else np.zeros((0, 3))
+    return Optodes(mesh, pts, 0 if src is None else src.shape[0], 0 if det is None else det.shape[0])
+
+
+def getdet(mesh, opt, phi):
+    """detval (ndet x nsrc) = rhs_det^T phi_src (redbirdpy/forward.py:365-442)."""
+    kind = _lib.RB_C128 if phi.is_complex() else _lib.RB_F64
+    out = torch.empty((opt.ndet, opt.nsrc), dtype=phi.dtype, device=phi.device)
+    if opt.ndet and opt.nsrc:
+        call("rb_femgetdet", ptr(mesh.elem), ptr(opt.loc[opt.nsrc:]), ptr(opt.bary[opt.nsrc:]), opt.ndet,
+             ptr(phi), phi.shape[1], opt.nsrc, kind, ptr(out), stream())
+    return out
+
+
+# -------------------------------------------------------------------- solve
+DEFAULT_TOL = 1e-15
+
+
+def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=2000, max_outer=10,
+          check_every=10, profile=False):
+    """Solve mat X = B for all columns of B (device, nn x k FP64 real).
+
+    Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
+    corrections inside FP64 iterative refinement; ``'fp64'``: the same loop
+    entirely in FP64.  Up to 128 columns per library call; wider B is solved
+    in column blocks."""
+    prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
+    n, k = B.shape
+    xdt = torch.complex128 if mat.is_complex else torch.float64
+    X = torch.empty((n, k), dtype=xdt, device=B.device)
+    info = {"iters": 0, "outer": 0, "flag": 0, "launches": 0, "relres": 0.0, "spmm_ms": 0.0, "update_ms": 0.0,
+            "spmm_launches": 0, "update_launches": 0}
+    if prec == _lib.RB_FP64 and inner_tol > 1e-6:
+        inner_tol = max(tol, 1e-15)
+    opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
+                            int(bool(profile)))
+    for c0 in range(0, k, 128):
+        kb = min(128, k - c0)
+        Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
+        Xb = torch.empty((n, kb), dtype=xdt, device=B.device) if (c0 or kb != k) else X
+        wb = _lib.lib().rb_femsolve_work_bytes(n, kb, int(mat.is_complex), prec)
+        work = torch.empty(wb, dtype=torch.uint8, device=B.device)
+        inf = _lib.RbSolveInfo()
+        call("rb_femsolve", ctypes.byref(mat.struct), ptr(Bb), ptr(Xb), kb, ctypes.byref(opts), ctypes.byref(inf),
+             ptr(work), wb, stream())
+        if Xb is not X:
+            X[:, c0:c0 + kb] = Xb
+        info["iters"] += inf.iters
+        info["outer"] = max(info["outer"], inf.outer)
+        info["flag"] = max(info["flag"], inf.flag)
+        info["launches"] += inf.launches
+        info["relres"] = max(info["relres"], inf.relres)
+        for key in ("spmm_ms", "update_ms", "spmm_launches", "update_launches"):
+            info[key] += getattr(inf, key)
+    return X, info
+
+
+# ----------------------------------------------------------------- Jacobian
+def pair_map(sd, nsrc_cols=None):
+    """Column map of the active (src, det) pairs of an sd table for rb_jac:
+    (cols, det0, ndet, pair_src, pair_det, src_col, det_col)."""
+    sd = np.asarray(sd)
+    act = sd[sd[:, 2] == 1, :2] if sd.shape[1] >= 3 else sd[:, :2]
+    act = act.astype(np.int64)
+    s_u = np.unique(act[:, 0])
+    d_u = np.unique(act[:, 1])
+    cols = np.concatenate([s_u, d_u])
+    psrc = np.searchsorted(s_u, act[:, 0])
+    pdet = np.searchsorted(d_u, act[:, 1])
+    return cols, len(s_u), len(d_u), psrc, pdet, act[:, 0], act[:, 1]
+
+
+def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=None, evol=None, ddd=None):
+    """Adjoint Jacobian rows on the device (nsd x nn), see rb_jac.
+    what: 'mua' (reference semantics, forward.py:509-569), 'mua_nodal'
+    (exact for node-based properties at fixed D) or 'D'."""
+    dev = phi.device
+    cols, det0, ndet, psrc, pdet, _, _ = pair_map(sd)
+    nsd = len(psrc)
+    cplx = phi.is_complex()
+    if cplx and not out_dtype.is_complex:
+        out_dtype = torch.complex64 if out_dtype == torch.float32 else torch.complex128
+    if J is None:
+        J = torch.empty((nsd, mesh.nn), dtype=out_dtype, device=dev)
+        ldj = mesh.nn
+    phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
+                torch.complex64: _lib.RB_C64}[phi.dtype]
+    out_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
+                torch.complex64: _lib.RB_C64}[J.dtype]
+    w = {"mua": _lib.RB_JAC_MUA_REF, "mua_nodal": _lib.RB_JAC_MUA_NODAL, "D": _lib.RB_JAC_D}[what]
+    ev = evol if evol is not None else mesh.evol
+    if ev is None:
+        raise ValueError("tet volumes are required")
+    dd = ddd if ddd is not None else (mesh.ddd if w == _lib.RB_JAC_D else None)
+    colsd = _i32(cols, dev)
+    ps = _i32(psrc, dev)
+    pd = _i32(pdet, dev)
+    # pair groups: at most 128 staged columns / 64 detectors per launch
+    if len(cols) > 128 or ndet > 64:
+        raise ValueError("rb_jac stages at most 128 phi columns and 64 detectors per call")
+    call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0, ndet,
+         ptr(ps), ptr(pd), nsd, ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev), ptr(dd), stream())
+    return J
+
+
+def jacobian_elem(mesh, phi, sd, evol=None):
+    _, _, _, _, _, scol, dcol = pair_map(sd)
+    nsd = len(scol)
+    Je = torch.empty((nsd, mesh.ne), dtype=phi.dtype, device=phi.device)
+    kind = _lib.RB_C128 if phi.is_complex() else _lib.RB_F64
+    ev = evol if evol is not None else mesh.evol
+    sc, dc = _i32(scol, phi.device), _i32(dcol, phi.device)  # kept alive across the launch
+    call("rb_jac_elem", ctypes.byref(mesh.struct), ptr(ev), ptr(phi), kind, phi.shape[1], ptr(sc), ptr(dc), nsd,
+         ptr(Je), stream())
+    return Je

@@ -1,0 +1,280 @@
+"""Mesh preparation and optode bookkeeping (host side of the drop-in API).
+
+Mirrors redbirdpy's ``utility`` functions that the FEM path consumes
+(redbirdpy/utility.py).  Index convention as in redbirdpy: ``elem``/``face``
+in ``cfg`` are 1-based; the device layer converts once.  Heavy mesh work
+(node incidence, the CSR pattern, element gradients) runs on the GPU through
+``redbirdpy_b200.engine``.
+"""
+
+import numpy as np
+
+__all__ = [
+    "meshprep", "deldotdel", "sdmap", "getoptodes", "getdistance", "getltr", "getreff",
+    "getbulk", "forcearray", "elem2node",
+]
+
+_ARRAY_KEYS = ["node", "elem", "face", "srcpos", "srcdir", "detpos", "detdir", "prop", "seg",
+               "widesrc", "widedet"]
+
+
+def forcearray(cfg, keys=_ARRAY_KEYS):
+    """List-valued cfg entries -> numpy arrays (utility.py:1112-1117)."""
+    for key in keys:
+        if key in cfg and isinstance(cfg[key], list):
+            cfg[key] = np.array(cfg[key])
+    return cfg
+
+
+def _signed_volume6(node, e0):
+    x0 = node[e0[:, 0]]
+    return np.einsum("ij,ij->i", np.cross(node[e0[:, 1]] - x0, node[e0[:, 2]] - x0), node[e0[:, 3]] - x0)
+
+
+def _reorient(node, elem):
+    """Swap nodes 0 and 1 of negatively oriented tets (utility.py:1047-1063)."""
+    elem = np.array(elem, copy=True)
+    neg = _signed_volume6(node, elem[:, :4].astype(np.int64) - 1) < 0
+    elem[neg, 0], elem[neg, 1] = elem[neg, 1].copy(), elem[neg, 0].copy()
+    return elem
+
+
+def _volface(elem, nn):
+    """Boundary triangles, in the order redbirdpy's fallback returns them
+    (utility.py:1066-1087): sorted by their sorted node triple, keeping the
+    orientation of the owning tet.  One int64 key per face replaces the
+    row-wise unique."""
+    e0 = elem[:, :4].astype(np.int64) - 1
+    faces = np.concatenate([e0[:, [0, 2, 1]], e0[:, [0, 1, 3]], e0[:, [0, 3, 2]], e0[:, [1, 2, 3]]])
+    s = np.sort(faces, axis=1)
+    key = (s[:, 0] * nn + s[:, 1]) * nn + s[:, 2]
+    _, first, counts = np.unique(key, return_index=True, return_counts=True)
+    return faces[first[counts == 1]] + 1
+
+
+def _elemvolume(node, cells):
+    """|volume| of tets or area of triangles (utility.py:1090-1109)."""
+    c0 = cells.astype(np.int64) - 1
+    if c0.shape[1] >= 4:
+        return np.abs(_signed_volume6(node, c0)) / 6.0
+    v = np.cross(node[c0[:, 1]] - node[c0[:, 0]], node[c0[:, 2]] - node[c0[:, 0]])
+    return 0.5 * np.sqrt(np.einsum("ij,ij->i", v, v))
+
+
+def _nodevolume(nn, elem, evol):
+    """Quarter of the incident tet volumes per node (utility.py:1005-1017)."""
+    e0 = elem[:, :4].astype(np.int64) - 1
+    return 0.25 * np.bincount(e0.ravel(), weights=np.repeat(evol, 4), minlength=nn)
+
+
+def getreff(n_in, n_out=1.0):
+    """Effective reflection coefficient, 2000-step quadrature (utility.py:879-904)."""
+    if n_in <= n_out:
+        return 0.0
+    oc = np.arcsin(n_out / n_in)
+    step = np.pi / 2000
+    o = np.arange(0, oc, step)
+    cos_t = np.sqrt(1 - (n_in * np.sin(o)) ** 2)
+    cos_i = np.cos(o)
+    fres = 0.5 * ((n_in * cos_t - n_out * cos_i) / (n_in * cos_t + n_out * cos_i)) ** 2
+    fres = fres + 0.5 * ((n_in * cos_i - n_out * cos_t) / (n_in * cos_i + n_out * cos_t)) ** 2
+    full = np.arange(0, np.pi / 2, step)
+    rf = np.ones(len(full))
+    rf[: len(fres)] = fres
+    cf = np.cos(full)
+    r_phi = 2 * np.sum(np.sin(full) * cf * rf) * step
+    r_j = 3 * np.sum(np.sin(full) * cf ** 2 * rf) * step
+    return (r_phi + r_j) / (2 - r_phi + r_j)
+
+
+def getbulk(cfg):
+    """Bulk [mua, mus, g, n] at the air interface (property.py:216-332)."""
+    default = np.array([0.0, 0.0, 0.0, 1.37])
+    if "bulk" in cfg:
+        b = cfg["bulk"]
+        out = default.copy()
+        if "mua" in b:
+            out[0] = b["mua"]
+        if "dcoeff" in b:
+            out[1], out[2] = 1.0 / (3 * b["dcoeff"]), 0
+        if "musp" in b:
+            out[1], out[2] = b["musp"], 0
+        if "g" in b:
+            out[2] = b["g"]
+        if "n" in b:
+            out[3] = b["n"]
+        return out
+    prop = cfg.get("prop")
+    if prop is None:
+        return default
+    if isinstance(prop, dict):
+        raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
+    prop = np.atleast_2d(prop)
+    nn = cfg["node"].shape[0]
+    ne = cfg["elem"].shape[0]
+    face = cfg.get("face")
+    if prop.shape[0] < min(nn, ne):
+        seg = cfg.get("seg")
+        if seg is None:
+            return prop[1] if prop.shape[0] > 1 else default
+        seg = np.asarray(seg)
+        if face is not None and len(seg) == nn:
+            label = seg[face[0, 0] - 1]
+        elif face is not None and len(seg) == ne:
+            hit = np.nonzero(np.any(cfg["elem"][:, :4] == face[0, 0], axis=1))[0]
+            label = seg[hit[0]] if len(hit) else 0
+        else:
+            label = seg[0]
+        label = int(label)
+        if prop.shape[0] > label:
+            return prop[label]
+        return prop[1] if prop.shape[0] > 1 else default
+    if prop.shape[0] == nn:
+        return prop[face[0, 0] - 1] if face is not None else prop[0]
+    if prop.shape[0] == ne:
+        if face is not None:
+            hit = np.nonzero(np.any(cfg["elem"][:, :4] == face[0, 0], axis=1))[0]
+            if len(hit):
+                return prop[hit[0]]
+        return prop[0]
+    return default
+
+
+def getltr(cfg, wv=""):
+    """Transport mean free path 1/(mua + musp) of the bulk (utility.py:862-876)."""
+    bk = getbulk(cfg)
+    return 1.0 / (bk[0] + bk[1] * (1 - bk[2]))
+
+
+def getoptodes(cfg, wv=""):
+    """Point optodes moved inward by ltr along their direction (utility.py:799-822).
+    Returns (pointsrc, pointdet, widesrc, widedet)."""
+    ltr = getltr(cfg, wv)
+    src = det = None
+    if cfg.get("srcpos") is not None and np.size(cfg["srcpos"]) > 0:
+        sp = np.atleast_2d(np.asarray(cfg["srcpos"], dtype=np.float64))
+        sdir = np.atleast_2d(np.asarray(cfg["srcdir"], dtype=np.float64))
+        if sdir.shape[0] == 1:
+            sdir = np.tile(sdir, (sp.shape[0], 1))
+        src = sp[:, :3] + sdir[:, :3] * ltr
+    if cfg.get("detpos") is not None and np.size(cfg["detpos"]) > 0:
+        dp = np.atleast_2d(np.asarray(cfg["detpos"], dtype=np.float64))
+        ddir = np.atleast_2d(np.asarray(cfg.get("detdir", cfg["srcdir"]), dtype=np.float64))
+        if ddir.shape[0] == 1:
+            ddir = np.tile(ddir, (dp.shape[0], 1))
+        det = dp[:, :3] + ddir[:, :3] * ltr
+    return src, det, cfg.get("widesrc"), cfg.get("widedet")
+
+
+def getdistance(srcpos, detpos, badsrc=None, baddet=None, widesrc=None, widedet=None):
+    """Source-detector distances, Ndet x Nsrc, inf for excluded (utility.py:825-859)."""
+    badsrc, baddet = badsrc or [], baddet or []
+    srcpos, detpos = np.atleast_2d(srcpos), np.atleast_2d(detpos)
+    dist = np.full((detpos.shape[0], srcpos.shape[0]), np.inf)
+    gs = sorted(set(range(srcpos.shape[0])) - set(badsrc))
+    gd = sorted(set(range(detpos.shape[0])) - set(baddet))
+    if gs and gd:
+        diff = srcpos[gs, None, :3] - detpos[None, gd, :3]
+        dist[np.ix_(gd, gs)] = np.sqrt(np.sum(diff.transpose(1, 0, 2) ** 2, axis=2))
+    return dist
+
+
+def sdmap(cfg, maxdist=np.inf, **kwargs):
+    """Source/detector pair table [src_col, det_col, active] (utility.py:675-796,
+    single-wavelength point-optode case).  Rows are detector-major (meshgrid)."""
+    ns = np.atleast_2d(cfg["srcpos"]).shape[0] if cfg.get("srcpos") is not None and np.size(cfg["srcpos"]) else 0
+    nd = np.atleast_2d(cfg["detpos"]).shape[0] if cfg.get("detpos") is not None and np.size(cfg["detpos"]) else 0
+    if ns == 0 or nd == 0:
+        raise ValueError("Must define at least one source and detector")
+    badsrc = kwargs.get("excludesrc", cfg.get("excludesrc", []))
+    baddet = kwargs.get("excludedet", cfg.get("excludedet", []))
+    gs = sorted(set(range(ns)) - set(badsrc))
+    gd = sorted(set(range(nd)) - set(baddet))
+    ss, dd = np.meshgrid(gs, [ns + d for d in gd])
+    sd = np.column_stack([ss.ravel(), dd.ravel()])
+    if maxdist < np.inf:
+        dist = getdistance(cfg["srcpos"], cfg["detpos"], badsrc, baddet)
+        active = np.array([1.0 if dist[int(d) - ns, int(s)] < maxdist else 0.0 for s, d in sd])
+        return np.column_stack([sd, active])
+    return np.column_stack([sd, np.ones(len(sd))])
+
+
+def elem2node(elem, elemval, nodelen=None):
+    """Average element values onto nodes (utility.py:910-929)."""
+    if isinstance(elem, dict):
+        nodelen = elem["node"].shape[0]
+        elem = elem["elem"]
+    e0 = elem[:, :4].astype(np.int64) - 1
+    ev = elemval[:, None] if elemval.ndim == 1 else elemval
+    out = np.zeros((nodelen, ev.shape[1]))
+    for j in range(4):
+        np.add.at(out, e0[:, j], ev)
+    return (0.25 * out).squeeze()
+
+
+def deldotdel(cfg):
+    """V grad(phi_i).grad(phi_j) for the 10 pairs i<=j, computed on the GPU
+    (utility.py:53-98).  Returns ``(ddd, None)``; the reference's second
+    output (the 3x4xNe gradients) is not materialised."""
+    from . import engine
+
+    return engine.mesh_of(cfg).deldotdel_host(), None
+
+
+def meshprep(cfg):
+    """Prepare the mesh dict in place (utility.py:101-246): reorientation,
+    boundary faces, areas/volumes, nodal volumes, reff/musp0, the sparse
+    pattern (rows/cols/idxcount/idxsum), deldotdel, omega and the sd table.
+    The reorientation, faces and volumes follow redbirdpy's own fallbacks, so
+    ``cfg`` comes out identical to the reference's."""
+    cfg = forcearray(cfg)
+    if "node" not in cfg or "elem" not in cfg:
+        raise ValueError("cfg must contain 'node' and 'elem'")
+    node = np.asarray(cfg["node"], dtype=np.float64)
+    cfg["node"] = node
+    elem = cfg["elem"]
+    nn = node.shape[0]
+    if elem.shape[1] > 4 and cfg.get("seg") is None:
+        cfg["seg"] = elem[:, 4].astype(int)
+    if not cfg.get("isreoriented", False):
+        r = _reorient(node, elem[:, :4])
+        cfg["elem"] = np.column_stack([r, elem[:, 4:]]) if elem.shape[1] > 4 else r
+        cfg["isreoriented"] = True
+    if cfg.get("face") is None:
+        cfg["face"] = _volface(cfg["elem"], nn)
+    if cfg.get("area") is None:
+        cfg["area"] = _elemvolume(node, cfg["face"])
+    if cfg.get("evol") is None:
+        cfg["evol"] = _elemvolume(node, cfg["elem"][:, :4])
+    if np.any(cfg["evol"] == 0):
+        bad = np.where(cfg["evol"] == 0)[0]
+        raise ValueError(f"Degenerate elements detected at indices: {bad}")
+    if cfg.get("nvol") is None:
+        cfg["nvol"] = _nodevolume(nn, cfg["elem"], cfg["evol"])
+    if "srcpos" not in cfg:
+        raise ValueError("cfg.srcpos is required")
+    if "srcdir" not in cfg:
+        raise ValueError("cfg.srcdir is required")
+    if isinstance(cfg.get("prop"), dict):
+        raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
+    if cfg.get("reff") is None:
+        bk = getbulk(cfg)
+        cfg["reff"] = getreff(bk[3], 1.0)
+        cfg["musp0"] = bk[1] * (1 - bk[2])
+    srctype = cfg.get("srctype", "pencil")
+    dettype = cfg.get("dettype", "pencil")
+    if srctype not in ("pencil", "isotropic") or dettype not in ("pencil", "isotropic") \
+            or "widesrcid" in cfg or "widedetid" in cfg:
+        raise NotImplementedError("wide-field sources/detectors are outside this engine's scope")
+    from . import engine
+
+    dm = engine.mesh_of(cfg)
+    if cfg.get("cols") is None:
+        cfg["rows"], cfg["cols"], cfg["idxcount"] = dm.adjacency_host()
+    if cfg.get("idxsum") is None:
+        cfg["idxsum"] = np.cumsum(cfg["idxcount"])
+    if cfg.get("deldotdel") is None:
+        cfg["deldotdel"] = dm.deldotdel_host()
+    if "omega" not in cfg:
+        cfg["omega"] = 0
+    return cfg, sdmap(cfg)

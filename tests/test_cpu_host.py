@@ -1,0 +1,73 @@
+"""CPU-only checks: the C-ABI library loads and exports every declared entry
+point, and the host-side mesh preparation matches the oracle."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "redbird_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(rb_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_header_symbols():
+    from redbirdpy_b200 import _lib
+
+    lib = _lib.lib()  # loads without a GPU
+    names = header_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(_lib.exported_symbols()), set(names) ^ set(_lib.exported_symbols())
+    assert lib.rb_version() >= 1
+
+
+def test_host_meshprep_helpers_match_oracle(golden):
+    from redbirdpy_b200 import utility as ut
+    from oracle import femoracle as fo
+
+    g = golden("c1_cw")
+    from redbirdpy_b200.meshgen import kuhn_box
+
+    node, elem = kuhn_box([60, 60, 30], 5)
+    r = ut._reorient(node, elem)
+    assert np.array_equal(r, g["elem"])
+    f = ut._volface(r, node.shape[0])
+    assert np.array_equal(f, g["face"]) and np.array_equal(f, fo.volface(r))
+    np.testing.assert_allclose(ut._elemvolume(node, f), g["area"], rtol=1e-14)
+    np.testing.assert_allclose(ut._elemvolume(node, r), g["evol"], rtol=1e-14)
+    np.testing.assert_allclose(ut._nodevolume(node.shape[0], r, g["evol"]), g["nvol"], rtol=1e-13)
+    assert ut.getreff(1.37) == pytest.approx(float(g["reff"]), abs=1e-15)
+    assert ut.getreff(1.0) == 0.0
+
+
+def test_sdmap_and_optodes_match_oracle(golden):
+    from redbirdpy_b200 import utility as ut
+    from oracle import femoracle as fo
+
+    g = golden("nodal_cw")
+    cfg = dict(node=g["node"], elem=g["elem"], face=g["face"], prop=g["prop"], srcpos=g["srcpos"],
+               srcdir=np.array([[0, 0, 1.0]]), detpos=g["detpos"], detdir=np.array([[0, 0, 1.0]]))
+    assert np.array_equal(ut.sdmap(cfg), g["sd"])
+    s, d, _, _ = ut.getoptodes(cfg)
+    os_, od_ = fo.getoptodes(cfg)
+    np.testing.assert_allclose(np.vstack([s, d]), g["optode"], rtol=1e-15)
+    np.testing.assert_allclose(np.vstack([os_, od_]), g["optode"], rtol=1e-15)
+    sd = ut.sdmap(cfg, maxdist=15.0)
+    dist = ut.getdistance(cfg["srcpos"], cfg["detpos"])
+    for s_, d_, a in sd:
+        assert a == (1.0 if dist[int(d_) - 4, int(s_)] < 15.0 else 0.0)
+
+
+def test_kuhn_box_counts():
+    from redbirdpy_b200.meshgen import kuhn_box
+
+    node, elem = kuhn_box([100, 100, 50], 1)
+    assert node.shape == (520251, 3) and elem.shape == (3000000, 4)
+    assert elem.min() == 1 and elem.max() == 520251

@@ -1,0 +1,206 @@
+"""GPU parity of the forward path against the reference's own outputs
+(golden fixtures) and the CPU oracle.  Tolerances: CSR indices bit-exact,
+assembled values relative <= 1e-12 (FP64), detector values <= 1e-6 relative
+after refinement."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import redbirdpy_b200 as rbb  # noqa: E402
+from redbirdpy_b200 import engine  # noqa: E402
+from oracle import femoracle as fo  # noqa: E402
+
+
+def cfg_from(g, prepared=True):
+    cfg = dict(node=g["node"].copy(), elem=g["elem"].copy(), prop=g["prop"].copy(), srcpos=g["srcpos"],
+               srcdir=np.array([[0, 0, 1.0]]), detpos=g["detpos"], detdir=np.array([[0, 0, 1.0]]),
+               omega=float(g["omega"]))
+    if "seg" in g:
+        cfg["seg"] = g["seg"]
+    if prepared:
+        for k in ("face", "area", "evol", "reff", "deldotdel"):
+            cfg[k] = g[k]
+        cfg["isreoriented"] = True
+    return cfg
+
+
+CASES = ["c1_cw", "c1_fd", "nodal_cw", "nodal_fd"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_csr_pattern_bit_exact(golden, case):
+    g = golden(case)
+    m = engine.mesh_of(cfg_from(g))
+    assert np.array_equal(m.indptr.cpu().numpy(), g["A_indptr"])
+    assert np.array_equal(m.indices[: m.nnz].cpu().numpy(), g["A_indices"])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_femlhs_values(golden, case):
+    g = golden(case)
+    A = rbb.femlhs(cfg_from(g), g["deldotdel"])
+    assert A.indices.dtype == np.int32 and A.indptr.dtype == np.int32
+    assert np.array_equal(A.indptr, g["A_indptr"]) and np.array_equal(A.indices, g["A_indices"])
+    rel = np.abs(A.data - g["A_data"]).max() / np.abs(g["A_data"]).max()
+    assert rel <= 1e-12, rel
+    # entrywise relative check as well (no entry is tiny in these matrices)
+    assert np.max(np.abs(A.data - g["A_data"]) / np.abs(g["A_data"])) <= 1e-12
+
+
+def test_femlhs_elemprop_complex(golden):
+    g, m = golden("c1_elemprop_fd"), golden("c1_cw")
+    cfg = cfg_from(m)
+    cfg.pop("seg")
+    cfg["prop"], cfg["omega"] = g["prop"], float(g["omega"])
+    A = rbb.femlhs(cfg, None)
+    assert np.array_equal(A.indices, g["A_indices"])
+    assert np.abs(A.data - g["A_data"]).max() / np.abs(g["A_data"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_femrhs(golden, case):
+    g = golden(case)
+    rhs, loc, bary, optode = rbb.femrhs(cfg_from(g))
+    np.testing.assert_array_equal(loc, g["loc"])
+    np.testing.assert_allclose(bary, g["bary"], atol=1e-13)
+    np.testing.assert_allclose(rhs.toarray(), g["rhs"], atol=1e-13)
+    np.testing.assert_allclose(optode, g["optode"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_runforward_detval(golden, case, precision):
+    g = golden(case)
+    det, phi = rbb.runforward(cfg_from(g), precision=precision)
+    ref = g["detval"]
+    assert det.shape == ref.shape and phi.shape == g["phi"].shape
+    err = np.abs(det - ref) / np.abs(ref)
+    assert err.max() <= 1e-6, err.max()
+    perr = np.abs(phi - g["phi"]).max() / np.abs(g["phi"]).max()
+    assert perr <= 1e-9, perr
+
+
+def test_run_facade_and_meshprep(golden):
+    g = golden("c1_cw")
+    cfg = cfg_from(g, prepared=False)
+    cfg, sd = rbb.meshprep(cfg)
+    assert np.array_equal(cfg["elem"], g["elem"]) and np.array_equal(cfg["face"], g["face"])
+    np.testing.assert_allclose(cfg["deldotdel"], g["deldotdel"], rtol=1e-10,
+                               atol=1e-14 * np.abs(g["deldotdel"]).max())
+    assert np.array_equal(sd, g["sd"])
+    det, phi = rbb.run(cfg)
+    np.testing.assert_allclose(det, g["detval"], rtol=1e-6)
+    # known answer from the reference on this workload
+    np.testing.assert_allclose(det.ravel(), [9.6445e-4] * 2, rtol=1e-4)
+
+
+def test_femgetdet_drop_in(golden):
+    g = golden("nodal_fd")
+    cfg = cfg_from(g)
+    rhs, loc, bary, _ = rbb.femrhs(cfg)
+    d1 = rbb.femgetdet(g["phi"], cfg, rhs, loc, bary)
+    d0 = fo.femgetdet(g["phi"], cfg, rhs)
+    np.testing.assert_allclose(d1, d0, rtol=1e-12)
+    np.testing.assert_allclose(rbb.femgetdet(g["phi"], cfg, rhs), d0, rtol=1e-12)
+
+
+def spd(n, seed):
+    rng = np.random.default_rng(seed)
+    from scipy import sparse
+
+    M = sparse.random(n, n, density=0.05, random_state=rng)
+    A = (M @ M.T + 10 * sparse.eye(n)).tocsr()
+    return A
+
+
+def test_femsolve_spd_and_edge_cases():
+    from scipy.sparse.linalg import spsolve
+
+    A = spd(300, 1)
+    rng = np.random.default_rng(2)
+    b = rng.standard_normal((300, 5))
+    b[:, 2] = 0.0  # zero column -> exact zeros (solver.py:568-581)
+    x, flag = rbb.femsolve(A, b)
+    assert flag == 0
+    assert np.all(x[:, 2] == 0.0)
+    ref = np.column_stack([spsolve(A.tocsc(), b[:, i]) if np.any(b[:, i]) else np.zeros(300) for i in range(5)])
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-13)
+    # 1-D in -> 1-D out; residual as in test_solver.py:68-83
+    x1, flag = rbb.femsolve(A, b[:, 0])
+    assert x1.ndim == 1 and flag == 0
+    assert np.linalg.norm(A @ x1 - b[:, 0]) / np.linalg.norm(b[:, 0]) < 1e-8
+    # identity / diagonal known answers (test_solver.py:1660-1681)
+    from scipy import sparse
+
+    I = sparse.eye(50).tocsr()
+    xi, _ = rbb.femsolve(I, np.arange(50.0))
+    np.testing.assert_allclose(xi, np.arange(50.0), rtol=1e-14)
+    D = sparse.diags(np.arange(1.0, 51.0)).tocsr()
+    xd, _ = rbb.femsolve(D, np.ones(50))
+    np.testing.assert_allclose(xd, 1.0 / np.arange(1.0, 51.0), rtol=1e-13)
+
+
+def test_femsolve_complex_symmetric(golden):
+    from scipy.sparse.linalg import splu
+
+    g = golden("nodal_fd")
+    from scipy import sparse
+
+    A = sparse.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"]))
+    b = g["rhs"]
+    for prec in ("mixed", "fp64"):
+        x, flag = rbb.femsolve(A, b, precision=prec)
+        ref = splu(A.tocsc()).solve(b.astype(complex))
+        assert flag == 0
+        assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-10
+
+
+def test_femsolve_many_columns(golden):
+    """More than one 128-column block."""
+    from scipy import sparse
+    from scipy.sparse.linalg import splu
+
+    g = golden("c1_cw")
+    A = sparse.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"]))
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal((A.shape[0], 130))
+    x, flag = rbb.femsolve(A, b)
+    ref = splu(A.tocsc()).solve(b)
+    assert flag == 0
+    assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-11
+
+
+def test_femsolve_iteration_cap_flag(golden):
+    from scipy import sparse
+
+    g = golden("c1_cw")
+    A = sparse.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"]))
+    b = g["rhs"]
+    x, flag = rbb.femsolve(A, b, method="cg", maxiter=3, max_outer=1, tol=1e-14)
+    assert flag == 1
+
+
+def test_large_pattern_vs_scipy():
+    """51x51x26 box (375k tets): pattern and values against the oracle's scipy assembly."""
+    from redbirdpy_b200.meshgen import kuhn_box
+
+    node, elem = kuhn_box([100, 100, 50], 2)
+    rng = np.random.default_rng(0)
+    nn = node.shape[0]
+    prop = np.column_stack([rng.uniform(0.008, 0.012, nn), rng.uniform(0.9, 1.1, nn), np.zeros(nn),
+                            np.full(nn, 1.37)])
+    cfg = dict(node=node, elem=elem, prop=prop, srcpos=np.array([[50, 50, 0.0]]), srcdir=np.array([[0, 0, 1.0]]),
+               detpos=np.array([[60, 50, 0.0]]), omega=2 * np.pi * 1e8)
+    cfg, _ = rbb.meshprep(cfg)
+    A = rbb.femlhs(cfg, None)
+    ocfg = dict(cfg)
+    R = fo.femlhs(ocfg, fo.deldotdel(cfg["node"], cfg["elem"], cfg["evol"]))
+    assert A.nnz == 972876
+    assert np.array_equal(A.indptr, R.indptr) and np.array_equal(A.indices, R.indices)
+    assert np.abs(A.data - R.data).max() / np.abs(R.data).max() <= 1e-12
