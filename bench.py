@@ -216,6 +216,24 @@ def run_b200(args):
     sp_gbs = spmm_bytes / (sp_ms * 1e-3) / 1e9 if sp_ms > 0 else None
     up_gbs = upd_bytes / (up_ms * 1e-3) / 1e9 if up_ms > 0 else None
 
+    # assembly alone (femlhs kernel pair), CUDA events around 10 launches
+    for _ in range(2):
+        engine.assemble(mesh, optics)
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ea.record()
+    for _ in range(10):
+        engine.assemble(mesh, optics)
+    eb.record()
+    torch.cuda.synchronize()
+    asm_ms = ea.elapsed_time(eb) / 10
+    ne, nf = mesh.ne, mesh.nf
+    pk = 8 if optics.kind == 0 else 8  # mua/musp per entity
+    nprop = mesh.nn if optics.kind == 0 else ne
+    asm_bytes = (ne * (16 + 80 + 8 + 16) + nprop * (2 * pk + 8) + nnz * (4 + 8 + 4) + n * (4 * 3 + 12)
+                 + nf * (12 + 8 + 12))
+    asm_gbs = asm_bytes / (asm_ms * 1e-3) / 1e9
+
     # end to end through the public API (host arrays in, numpy out)
     host_cfg = cfg
     for _ in range(1):
@@ -253,6 +271,9 @@ def run_b200(args):
         "roofline_update": {"kernel": "cg_update_kernel<float>", "achieved": round(up_gbs, 1) if up_gbs else None,
                             "unit": "GB/s", "frac": round(up_gbs / peak, 4) if up_gbs else None,
                             "algorithmic_bytes": upd_bytes, "launch_ms": round(up_ms, 4)},
+        "roofline_assembly": {"kernel": "femlhs_rows_kernel (+ dcoeff prologue)", "achieved": round(asm_gbs, 1),
+                              "unit": "GB/s", "frac": round(asm_gbs / peak, 4), "algorithmic_bytes": asm_bytes,
+                              "launch_ms": round(asm_ms, 4)},
         "e2e": {"value": round(world * nrhs / e2e_s, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,

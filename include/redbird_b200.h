@@ -99,19 +99,26 @@ typedef struct rb_optics {
 
 /* femlhs (redbirdpy/forward.py:90-256): A = K*D + M*mua (+ i*omega/c*n*M)
  * + Robin boundary terms, written into the fixed CSR pattern of `mesh`.
- * One warp per matrix row gathers the contributions of the row's tets (the
- * P1 gradients recomputed from node coordinates) and boundary faces in a
- * fixed order, so results are deterministic.
+ * Like the reference it combines the precomputed deldotdel rows `ddd`
+ * (ne x 10) and tet volumes `evol` (ne) with the current properties.  One
+ * warp per matrix row gathers the contributions of the row's tets and
+ * boundary faces in a fixed order, so results are deterministic.
  *   val64  nnz doubles (real) or nnz complex128 (omega > 0), required
  *   val32  optional FP32 / complex64 copy for the mixed-precision solver
  *   dinv64 optional nn reciprocal diagonal (Jacobi), same scalar kind
- *   dinv32 optional FP32 copy of dinv64 */
-int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, void* val64, void* val32,
-              void* dinv64, void* dinv32, void* stream);
+ *   dinv32 optional FP32 copy of dinv64
+ *   work   rb_femlhs_work_bytes(nn, ne) bytes of scratch */
+size_t rb_femlhs_work_bytes(int64_t nn, int64_t ne);
+int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, const double* evol, const double* ddd,
+              void* val64, void* val32, void* dinv64, void* dinv32, void* work, size_t work_bytes,
+              void* stream);
 
 /* deldotdel (redbirdpy/utility.py:53-98): ne x 10 values V*grad(phi_i).grad(phi_j)
- * for the pairs (0,0),(0,1),(0,2),(0,3),(1,1),(1,2),(1,3),(2,2),(2,3),(3,3). */
-int rb_deldotdel(const double* node, const int32_t* elem, int64_t ne, double* ddd, void* stream);
+ * for the pairs (0,0),(0,1),(0,2),(0,3),(1,1),(1,2),(1,3),(2,2),(2,3),(3,3),
+ * from the node coordinates; evol (optional, ne) receives |V| like
+ * elemvolume (utility.py:1090-1109). */
+int rb_deldotdel(const double* node, const int32_t* elem, int64_t ne, double* ddd, double* evol,
+                 void* stream);
 
 /* ------------------------------------------------------------ optodes */
 /* Point location used by femrhs (iso2mesh.tsearchn at redbirdpy/forward.py:316,337):

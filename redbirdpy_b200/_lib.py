@@ -59,8 +59,10 @@ _SIGS = {
     "rb_csr_pattern_work_bytes": (_sz, [_i64]),
     "rb_csr_pattern_count": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
     "rb_csr_pattern_fill": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    "rb_femlhs": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp]),
-    "rb_deldotdel": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "rb_femlhs_work_bytes": (_sz, [_i64, _i64]),
+    "rb_femlhs": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp, _vp,
+                                 _vp, _sz, _vp]),
+    "rb_deldotdel": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp]),
     "rb_tsearch": (ctypes.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "rb_point_rhs": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),
     "rb_femgetdet": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i64, _i64, _i32, _vp, _vp]),

@@ -1,14 +1,21 @@
 // FEM matrix assembly (femlhs) into a fixed CSR pattern.
 //
+// The geometry of a mesh is fixed across Gauss-Newton iterations, so its
+// per-tet gradient products (deldotdel, ne x 10) and volumes are computed
+// once by rb_deldotdel; every assembly then only combines them with the
+// current optical properties, as redbirdpy's femlhs does with cfg['deldotdel'].
+//
 // One warp owns one matrix row n.  Its lanes first evaluate, for up to 32
-// tets that contain n, the tet's contribution to row n (4 values: the row of
-// the local 4x4 stiffness*D + mass*mua (+ i*omega/c*n*mass) block), with the
-// P1 gradients recomputed from the node coordinates.  The lanes then switch
-// roles and each owns one CSR slot of the row, summing the staged
-// contributions whose column matches in ascending tet order, then the Robin
-// terms of the row's boundary faces.  No atomics: the result is
-// deterministic and written exactly once, FP64 plus an optional FP32 copy,
-// together with the reciprocal diagonal used by the Jacobi preconditioner.
+// tets that contain n, the tet's contribution to row n (4 values: row li of
+// the local 4x4 block D_e*K_e + mass(mua) (+ i*omega/c*mass(n))) and stage
+// them in shared memory.  The lanes then switch roles and each owns one CSR
+// slot of the row, summing the staged contributions whose column matches in
+// ascending tet order, then the Robin terms of the row's boundary faces.  No
+// atomics: the result is deterministic and written exactly once (FP64 plus an
+// optional FP32 copy), together with the reciprocal diagonal used by the
+// Jacobi preconditioner.  A prologue pass stores the diffusion coefficient
+// D = 1/(3(mua+musp)) per node (or per tet) in the workspace so that no
+// division is repeated per incidence.
 #include <algorithm>
 
 #include "rb_common.cuh"
@@ -20,34 +27,6 @@ constexpr int kAsmWarps = 8;
 template <bool CPLX> struct AsmVal;
 template <> struct AsmVal<false> { typedef double T; typedef float T32; };
 template <> struct AsmVal<true> { typedef cdouble T; typedef cfloat T32; };
-
-__device__ __forceinline__ void tet_geometry(const double* __restrict__ node, int4 e, double c[4][3],
-                                             double& det6) {
-  const double* p0 = node + 3 * (int64_t)e.x;
-  const double* p1 = node + 3 * (int64_t)e.y;
-  const double* p2 = node + 3 * (int64_t)e.z;
-  const double* p3 = node + 3 * (int64_t)e.w;
-  double a[3], b[3], d[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const double x0 = p0[k];
-    a[k] = p1[k] - x0;
-    b[k] = p2[k] - x0;
-    d[k] = p3[k] - x0;
-  }
-  c[1][0] = b[1] * d[2] - b[2] * d[1];
-  c[1][1] = b[2] * d[0] - b[0] * d[2];
-  c[1][2] = b[0] * d[1] - b[1] * d[0];
-  c[2][0] = d[1] * a[2] - d[2] * a[1];
-  c[2][1] = d[2] * a[0] - d[0] * a[2];
-  c[2][2] = d[0] * a[1] - d[1] * a[0];
-  c[3][0] = a[1] * b[2] - a[2] * b[1];
-  c[3][1] = a[2] * b[0] - a[0] * b[2];
-  c[3][2] = a[0] * b[1] - a[1] * b[0];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) c[0][k] = -(c[1][k] + c[2][k] + c[3][k]);
-  det6 = a[0] * c[1][0] + a[1] * c[1][1] + a[2] * c[1][2];
-}
 
 __device__ __forceinline__ void put(double& dst, double re, double) { dst = re; }
 __device__ __forceinline__ void put(cdouble& dst, double re, double im) { dst = make_double2(re, im); }
@@ -61,60 +40,79 @@ __device__ __forceinline__ cdouble recip(cdouble v) {
 __device__ __forceinline__ void add_real(double& a, double v) { a += v; }
 __device__ __forceinline__ void add_real(cdouble& a, double v) { a.x += v; }
 
+__global__ void dcoeff_kernel(int64_t m, const double* __restrict__ mua, const double* __restrict__ musp,
+                              double* __restrict__ dco) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    dco[i] = 1.0 / (3.0 * (mua[i] + musp[i]));
+}
+
+// deldotdel column of the pair (a, b), a, b in 0..3
+__device__ __forceinline__ int ddd_col(int a, int b) {
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return lo * 4 - (lo * (lo - 1)) / 2 + (hi - lo);
+}
+
 // Contribution of tet `e` (nodes en) to row `row`: the 4 entries (row, en[j]).
 template <bool CPLX, int KIND>
-__device__ __forceinline__ void tet_row(const rb_mesh& m, const rb_optics& o, double wc, int64_t e,
-                                        int4 en, int64_t row, typename AsmVal<CPLX>::T out[4]) {
-  double c[4][3], det6;
-  tet_geometry(m.node, en, c, det6);
-  const double vol = fabs(det6) * (1.0 / 6.0);
-  const double inv36v = 1.0 / (6.0 * fabs(det6));
-  const int32_t nd[4] = {en.x, en.y, en.z, en.w};
-  int li = 0;
+__device__ __forceinline__ void tet_row(const rb_mesh& m, const rb_optics& o, const double* __restrict__ evol,
+                                        const double* __restrict__ ddd, const double* __restrict__ dco, double wc,
+                                        int64_t e, int4 en, int64_t row, typename AsmVal<CPLX>::T out[4]) {
+  const int li = (en.y == row) ? 1 : (en.z == row) ? 2 : (en.w == row) ? 3 : 0;
+  const double vol = evol[e];
+  const double* dd = ddd + 10 * e;
+  double k4[4];
 #pragma unroll
-  for (int j = 1; j < 4; ++j)
-    if (nd[j] == row) li = j;
-  double dco, mu[4], msum = 0.0, nr[4], nsum = 0.0;
+  for (int j = 0; j < 4; ++j) k4[j] = dd[ddd_col(li, j)];
+  double d_e, mu[4], nr[4];
+  double msum = 0.0, nsum = 0.0, mli = 0.0, nli = 0.0;
   const bool nvec = (o.nref != nullptr);
+  const int32_t nd[4] = {en.x, en.y, en.z, en.w};
   if (KIND == RB_PROP_NODE) {
     double ds = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       mu[j] = o.mua[nd[j]];
       msum += mu[j];
-      ds += 1.0 / (3.0 * (mu[j] + o.musp[nd[j]]));
+      ds += dco[nd[j]];
       nr[j] = nvec ? o.nref[nd[j]] : o.nref_scalar;
       nsum += nr[j];
     }
-    dco = ds * 0.25;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j == li) {
+        mli = mu[j];
+        nli = nr[j];
+      }
+    }
+    d_e = 0.25 * ds;
   } else {
-    const double ma = o.mua[e];
-    dco = 1.0 / (3.0 * (ma + o.musp[e]));
+    d_e = dco[e];
+    const double ma = o.mua[e], ne_ = nvec ? o.nref[e] : o.nref_scalar;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       mu[j] = ma;
-      nr[j] = nvec ? o.nref[e] : o.nref_scalar;
+      nr[j] = ne_;
     }
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const double stiff = dco * (c[li][0] * c[j][0] + c[li][1] * c[j][1] + c[li][2] * c[j][2]) * inv36v;
+    const double stiff = d_e * k4[j];
+    const bool dg = (j == li);
     double mass, imag = 0.0;
     if (KIND == RB_PROP_NODE) {
-      // lumped-weight mass of node-based properties: (sum + mu_i + mu_j)/120
-      // off the diagonal, (sum + 2 mu_i)/60 on it
-      mass = (j == li) ? vol * (msum + 2.0 * mu[li]) * (1.0 / 60.0)
-                       : vol * (msum + mu[li] + mu[j]) * (1.0 / 120.0);
+      // lumped-weight mass of node-based properties (femlhs w1/w2):
+      // (sum + mu_i + mu_j)/120 off the diagonal, (sum + 2 mu_i)/60 on it
+      mass = dg ? vol * (msum + 2.0 * mli) * (1.0 / 60.0) : vol * (msum + mli + mu[j]) * (1.0 / 120.0);
       if (CPLX) {
         if (nvec)
-          imag = (j == li) ? wc * vol * (nsum + 2.0 * nr[li]) * (1.0 / 60.0)
-                           : wc * vol * (nsum + nr[li] + nr[j]) * (1.0 / 120.0);
+          imag = dg ? wc * vol * (nsum + 2.0 * nli) * (1.0 / 60.0)
+                    : wc * vol * (nsum + nli + nr[j]) * (1.0 / 120.0);
         else
-          imag = wc * o.nref_scalar * ((j == li) ? 0.10 : 0.05) * vol;
+          imag = wc * o.nref_scalar * (dg ? 0.10 : 0.05) * vol;
       }
     } else {
-      mass = ((j == li) ? 0.10 : 0.05) * mu[0] * vol;
-      if (CPLX) imag = ((j == li) ? 0.10 : 0.05) * wc * nr[0] * vol;
+      mass = (dg ? 0.10 : 0.05) * mu[0] * vol;
+      if (CPLX) imag = (dg ? 0.10 : 0.05) * wc * nr[0] * vol;
     }
     put(out[j], stiff + mass, imag);
   }
@@ -122,11 +120,10 @@ __device__ __forceinline__ void tet_row(const rb_mesh& m, const rb_optics& o, do
 
 template <bool CPLX, int KIND>
 __global__ void __launch_bounds__(kAsmWarps * 32)
-femlhs_rows_kernel(rb_mesh m, rb_optics o, double bc, double wc,
-                   typename AsmVal<CPLX>::T* __restrict__ val64,
-                   typename AsmVal<CPLX>::T32* __restrict__ val32,
-                   typename AsmVal<CPLX>::T* __restrict__ dinv64,
-                   typename AsmVal<CPLX>::T32* __restrict__ dinv32) {
+femlhs_rows_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, const double* __restrict__ ddd,
+                   const double* __restrict__ dco, double bc, double wc,
+                   typename AsmVal<CPLX>::T* __restrict__ val64, typename AsmVal<CPLX>::T32* __restrict__ val32,
+                   typename AsmVal<CPLX>::T* __restrict__ dinv64, typename AsmVal<CPLX>::T32* __restrict__ dinv32) {
   typedef typename AsmVal<CPLX>::T T;
   __shared__ int4 s_nodes[kAsmWarps][32];
   __shared__ T s_vals[kAsmWarps][32][4];
@@ -147,7 +144,7 @@ femlhs_rows_kernel(rb_mesh m, rb_optics o, double bc, double wc,
           const int64_t e = m.node_elist[eb + t0 + lane];
           const int4 en = reinterpret_cast<const int4*>(m.elem)[e];
           T v[4];
-          tet_row<CPLX, KIND>(m, o, wc, e, en, row, v);
+          tet_row<CPLX, KIND>(m, o, evol, ddd, dco, wc, e, en, row, v);
           s_nodes[w][lane] = en;
 #pragma unroll
           for (int j = 0; j < 4; ++j) s_vals[w][lane][j] = v[j];
@@ -155,11 +152,15 @@ femlhs_rows_kernel(rb_mesh m, rb_optics o, double bc, double wc,
         __syncwarp();
         for (int u = 0; u < kc; ++u) {
           const int4 en = s_nodes[w][u];
-          const int32_t nd[4] = {en.x, en.y, en.z, en.w};
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (nd[j] == col0) acc0 = s_add(acc0, s_vals[w][u][j]);
-            if (nd[j] == col1) acc1 = s_add(acc1, s_vals[w][u][j]);
+          if (en.x == col0) acc0 = s_add(acc0, s_vals[w][u][0]);
+          if (en.y == col0) acc0 = s_add(acc0, s_vals[w][u][1]);
+          if (en.z == col0) acc0 = s_add(acc0, s_vals[w][u][2]);
+          if (en.w == col0) acc0 = s_add(acc0, s_vals[w][u][3]);
+          if (col1 >= 0) {
+            if (en.x == col1) acc1 = s_add(acc1, s_vals[w][u][0]);
+            if (en.y == col1) acc1 = s_add(acc1, s_vals[w][u][1]);
+            if (en.z == col1) acc1 = s_add(acc1, s_vals[w][u][2]);
+            if (en.w == col1) acc1 = s_add(acc1, s_vals[w][u][3]);
           }
         }
         __syncwarp();
@@ -199,15 +200,18 @@ femlhs_rows_kernel(rb_mesh m, rb_optics o, double bc, double wc,
 }
 
 template <bool CPLX, int KIND>
-int launch_femlhs(const rb_mesh& m, const rb_optics& o, void* v64, void* v32, void* d64, void* d32,
-                  cudaStream_t st) {
+int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, const double* ddd, double* dco,
+                  void* v64, void* v32, void* d64, void* d32, cudaStream_t st) {
   typedef typename AsmVal<CPLX>::T T;
   typedef typename AsmVal<CPLX>::T32 T32;
   const double bc = (1.0 - o.reff) / (12.0 * (1.0 + o.reff));
   const double wc = o.omega / kC0;
+  const int64_t np = (KIND == RB_PROP_NODE) ? m.nn : m.ne;
+  dcoeff_kernel<<<(unsigned)std::min<int64_t>(ceil_div(np, 256), 148 * 16), 256, 0, st>>>(np, o.mua, o.musp, dco);
+  RB_LAUNCH_CHECK();
   unsigned g = (unsigned)std::min<int64_t>(ceil_div(m.nn, kAsmWarps), 148 * 64);
-  femlhs_rows_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(
-      m, o, bc, wc, (T*)v64, (T32*)v32, (T*)d64, (T32*)d32);
+  femlhs_rows_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, bc, wc, (T*)v64, (T32*)v32,
+                                                                 (T*)d64, (T32*)d32);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }
@@ -216,24 +220,32 @@ int launch_femlhs(const rb_mesh& m, const rb_optics& o, void* v64, void* v32, vo
 
 using namespace rb;
 
-extern "C" int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, void* val64, void* val32,
-                         void* dinv64, void* dinv32, void* stream) {
-  if (!mesh || !optics || !val64) return fail(RB_EARG, "rb_femlhs: mesh, optics and val64 are required");
+extern "C" size_t rb_femlhs_work_bytes(int64_t nn, int64_t ne) {
+  return (size_t)std::max(nn, ne) * sizeof(double) + 256;
+}
+
+extern "C" int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, const double* evol, const double* ddd,
+                         void* val64, void* val32, void* dinv64, void* dinv32, void* work, size_t work_bytes,
+                         void* stream) {
+  if (!mesh || !optics || !val64 || !evol || !ddd || !work)
+    return fail(RB_EARG, "rb_femlhs: mesh, optics, evol, ddd, val64 and work are required");
   const rb_mesh& m = *mesh;
   const rb_optics& o = *optics;
-  if (!m.node || !m.elem || !m.indptr || !m.indices || !m.node_eptr || !m.node_elist)
+  if (!m.elem || !m.indptr || !m.indices || !m.node_eptr || !m.node_elist || !m.node_fptr)
     return fail(RB_EARG, "rb_femlhs: mesh arrays missing");
-  if (m.nf > 0 && (!m.face || !m.area || !m.node_fptr || !m.node_flist))
-    return fail(RB_EARG, "rb_femlhs: boundary arrays missing");
-  if (m.nf == 0 && !m.node_fptr) return fail(RB_EARG, "rb_femlhs: node_fptr required (all zeros when nf == 0)");
+  if (m.nf > 0 && (!m.face || !m.area || !m.node_flist)) return fail(RB_EARG, "rb_femlhs: boundary arrays missing");
   if (!o.mua || !o.musp) return fail(RB_EARG, "rb_femlhs: mua and musp are required");
   if (o.kind != RB_PROP_NODE && o.kind != RB_PROP_ELEM) return fail(RB_EARG, "rb_femlhs: bad property kind");
   if (!(o.omega >= 0.0)) return fail(RB_EARG, "rb_femlhs: omega must be >= 0");
+  if (work_bytes < rb_femlhs_work_bytes(m.nn, m.ne)) return fail(RB_EARG, "rb_femlhs: workspace too small");
   cudaStream_t st = as_stream(stream);
+  double* dco = reinterpret_cast<double*>(work);
   const bool cplx = o.omega > 0.0;
   if (cplx)
-    return o.kind == RB_PROP_NODE ? launch_femlhs<true, RB_PROP_NODE>(m, o, val64, val32, dinv64, dinv32, st)
-                                  : launch_femlhs<true, RB_PROP_ELEM>(m, o, val64, val32, dinv64, dinv32, st);
-  return o.kind == RB_PROP_NODE ? launch_femlhs<false, RB_PROP_NODE>(m, o, val64, val32, dinv64, dinv32, st)
-                                : launch_femlhs<false, RB_PROP_ELEM>(m, o, val64, val32, dinv64, dinv32, st);
+    return o.kind == RB_PROP_NODE
+               ? launch_femlhs<true, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
+               : launch_femlhs<true, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
+  return o.kind == RB_PROP_NODE
+             ? launch_femlhs<false, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
+             : launch_femlhs<false, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
 }

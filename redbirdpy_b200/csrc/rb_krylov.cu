@@ -86,6 +86,15 @@ __device__ __forceinline__ void block_colreduce(const A (&acc)[V], A* __restrict
   __syncthreads();
 }
 
+__device__ __forceinline__ float shfl_s(float v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+__device__ __forceinline__ double shfl_s(double v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+__device__ __forceinline__ cfloat shfl_s(cfloat v, int l) {
+  return make_float2(__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l));
+}
+__device__ __forceinline__ cdouble shfl_s(cdouble v, int l) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l));
+}
+
 // ------------------------------------------------------------------ SpMM
 // Epilogues after y = (A x)[row, cols]:
 enum { EPI_STORE = 0, EPI_PQDOT = 1, EPI_RESID = 2 };
@@ -113,7 +122,48 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
     alignas(16) T y[V];
 #pragma unroll
     for (int j = 0; j < V; ++j) y[j] = s_zero(T());
-    if (on) {
+    if constexpr (L == 32) {
+      // whole warp on one row: lanes fetch the row's indices/values once,
+      // broadcast them by shuffle and keep 4 gathers of x in flight
+      for (int32_t p0 = b; p0 < e; p0 += 32) {
+        const int cnt = min(32, e - p0);
+        int32_t my_i = 0;
+        T my_v = s_zero(T());
+        if (lane < cnt) {
+          my_i = indices[p0 + lane];
+          my_v = val[p0 + lane];
+        }
+        int j = 0;
+        for (; j + 4 <= cnt; j += 4) {
+          int32_t ii[4];
+          T aa[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            ii[u] = __shfl_sync(0xffffffffu, my_i, j + u);
+            aa[u] = shfl_s(my_v, j + u);
+          }
+          if (on) {
+            alignas(16) T xv[4][V];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ldv<T, V>(X + (int64_t)ii[u] * k + c0, xv[u]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int q = 0; q < V; ++q) y[q] = s_fma(aa[u], xv[u][q], y[q]);
+          }
+        }
+        for (; j < cnt; ++j) {
+          const int32_t i0 = __shfl_sync(0xffffffffu, my_i, j);
+          const T a0 = shfl_s(my_v, j);
+          if (on) {
+            alignas(16) T xv[V];
+            ldv<T, V>(X + (int64_t)i0 * k + c0, xv);
+#pragma unroll
+            for (int q = 0; q < V; ++q) y[q] = s_fma(a0, xv[q], y[q]);
+          }
+        }
+      }
+    } else if (on) {
       for (int32_t p = b; p < e; ++p) {
         const T a = val[p];
         alignas(16) T xv[V];
@@ -121,6 +171,8 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
 #pragma unroll
         for (int j = 0; j < V; ++j) y[j] = s_fma(a, xv[j], y[j]);
       }
+    }
+    if (on) {
       if constexpr (EPI == EPI_RESID) {
         alignas(16) double bv[V];
 #pragma unroll
@@ -294,22 +346,41 @@ __device__ __forceinline__ cdouble cdiv(cdouble a, cdouble b) {
 }
 __device__ __forceinline__ bool finite_c(cdouble a) { return isfinite(a.x) && isfinite(a.y); }
 
+// One warp per column: lanes stride over the per-block partials (4 loads in
+// flight per lane), then a fixed shuffle tree; deterministic for a fixed grid.
+__device__ __forceinline__ double wsum(double v) { return warp_sum(v); }
+__device__ __forceinline__ cdouble wsum(cdouble v) { return make_double2(warp_sum(v.x), warp_sum(v.y)); }
+
 template <typename A>
-__device__ __forceinline__ cdouble sum_part(const A* part, int nb, int64_t k, int64_t c) {
-  A s = acc_zero<A>();
-  for (int b = 0; b < nb; ++b) s = acc_add(s, part[(int64_t)b * k + c]);
-  return to_c(s);
+__device__ __forceinline__ cdouble sum_part(const A* __restrict__ part, int nb, int64_t k, int64_t c, int lane) {
+  A s0 = acc_zero<A>(), s1 = acc_zero<A>(), s2 = acc_zero<A>(), s3 = acc_zero<A>();
+  int b = lane;
+  for (; b + 96 < nb; b += 128) {
+    s0 = acc_add(s0, part[(int64_t)b * k + c]);
+    s1 = acc_add(s1, part[(int64_t)(b + 32) * k + c]);
+    s2 = acc_add(s2, part[(int64_t)(b + 64) * k + c]);
+    s3 = acc_add(s3, part[(int64_t)(b + 96) * k + c]);
+  }
+  for (; b < nb; b += 32) s0 = acc_add(s0, part[(int64_t)b * k + c]);
+  return to_c(wsum(acc_add(acc_add(s0, s1), acc_add(s2, s3))));
 }
+
+#define RB_FIN_WARP()                                   \
+  const int lane = threadIdx.x & 31;                    \
+  const int64_t c = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); \
+  if (c >= k) return;
 
 // after init: rz, rr0; a column is active iff its rhs is nonzero and enabled
 template <typename A>
 __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
                                 const int32_t* __restrict__ enable) {
-  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= k) return;
+  RB_FIN_WARP();
+  const cdouble rz = sum_part<A>(part_rz, nb, k, c, lane);
+  const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
+  if (lane) return;
   ColState s = cs[c];
-  s.rz = sum_part<A>(part_rz, nb, k, c);
-  s.rr = to_c(sum_part<double>(part_rr, nb, k, c)).x;
+  s.rz = rz;
+  s.rr = rr;
   s.rr0 = s.rr;
   s.active = (enable == nullptr || enable[c]) && s.rr > 0.0;
   s.status = 0;
@@ -321,11 +392,12 @@ __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const doubl
 
 template <typename A>
 __global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs) {
-  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= k) return;
+  RB_FIN_WARP();
+  if (!cs[c].active) return;
+  const cdouble pq = sum_part<A>(part_pq, nb, k, c, lane);
+  if (lane) return;
   ColState s = cs[c];
-  if (!s.active) return;
-  s.pq = sum_part<A>(part_pq, nb, k, c);
+  s.pq = pq;
   if (!finite_c(s.pq) || (s.pq.x == 0.0 && s.pq.y == 0.0)) {
     s.active = 0;
     s.status = 2;
@@ -340,33 +412,28 @@ __global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* 
 template <typename A>
 __global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
                                 double tol2, int32_t* nactive) {
-  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int act = 0;
-  if (c < k) {
-    ColState s = cs[c];
-    if (s.active) {
-      const cdouble rzn = sum_part<A>(part_rz, nb, k, c);
-      const double rr = to_c(sum_part<double>(part_rr, nb, k, c)).x;
-      s.iters += 1;
-      s.rr = rr;
-      if (!finite_c(rzn) || !isfinite(rr)) {
-        s.active = 0;
-        s.status = 2;
-      } else if (rr <= tol2 * s.rr0) {
-        s.active = 0;
-      } else if (s.rz.x == 0.0 && s.rz.y == 0.0) {
-        s.active = 0;
-        s.status = 2;
-      } else {
-        s.beta = cdiv(rzn, s.rz);
-        s.rz = rzn;
-      }
-      cs[c] = s;
-      act = s.active;
-    }
+  RB_FIN_WARP();
+  if (!cs[c].active) return;
+  const cdouble rzn = sum_part<A>(part_rz, nb, k, c, lane);
+  const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
+  if (lane) return;
+  ColState s = cs[c];
+  s.iters += 1;
+  s.rr = rr;
+  if (!finite_c(rzn) || !isfinite(rr)) {
+    s.active = 0;
+    s.status = 2;
+  } else if (rr <= tol2 * s.rr0) {
+    s.active = 0;
+  } else if (s.rz.x == 0.0 && s.rz.y == 0.0) {
+    s.active = 0;
+    s.status = 2;
+  } else {
+    s.beta = cdiv(rzn, s.rz);
+    s.rz = rzn;
   }
-  act = warp_sum_i(act);
-  if ((threadIdx.x & 31) == 0 && act) atomicAdd(nactive, act);
+  cs[c] = s;
+  if (s.active) atomicAdd(nactive, 1);
 }
 
 // --------------------------------------------------- refinement kernels
@@ -381,14 +448,14 @@ struct OuterState {
 };
 
 __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterState* os) {
-  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= k) return;
-  double s = 0.0;
-  for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
+  RB_FIN_WARP();
+  const double s = sum_part<double>(part, nb, k, c, lane).x;
+  if (lane) return;
   OuterState o;
   o.bnorm = sqrt(s);
-  o.relres = (s > 0.0) ? 1.0 : 0.0;
-  o.prev = 2.0;
+  // no previous sweep yet: the first residual can never count as stagnation
+  o.relres = (s > 0.0) ? 1e300 : 0.0;
+  o.prev = 1e300;
   o.scale = 0.0;
   o.active = s > 0.0;
   o.done = (s > 0.0) ? 0 : 1;
@@ -397,31 +464,25 @@ __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterSta
 
 __global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterState* os, double tol,
                                  double stall, int32_t* nactive) {
-  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int act = 0;
-  if (c < k) {
-    OuterState o = os[c];
-    if (o.active) {
-      double s = 0.0;
-      for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
-      const double rel = sqrt(s) / o.bnorm;
-      o.prev = o.relres;
-      o.relres = rel;
-      if (!(rel > tol)) {
-        o.active = 0;
-        o.done = 1;
-      } else if (rel > stall * o.prev) {
-        o.active = 0;
-        o.done = 2;
-      } else {
-        o.scale = 1.0 / sqrt(s);
-      }
-      os[c] = o;
-      act = o.active;
-    }
+  RB_FIN_WARP();
+  if (!os[c].active) return;
+  const double s = sum_part<double>(part, nb, k, c, lane).x;
+  if (lane) return;
+  OuterState o = os[c];
+  const double rel = sqrt(s) / o.bnorm;
+  o.prev = o.relres;
+  o.relres = rel;
+  if (!(rel > tol)) {
+    o.active = 0;
+    o.done = 1;
+  } else if (rel > stall * o.prev) {
+    o.active = 0;
+    o.done = 2;
+  } else {
+    o.scale = 1.0 / sqrt(s);
   }
-  act = warp_sum_i(act);
-  if ((threadIdx.x & 31) == 0 && act) atomicAdd(nactive, act);
+  os[c] = o;
+  if (o.active) atomicAdd(nactive, 1);
 }
 
 // r_inner = T(R64 * scale) for active columns, 0 elsewhere
@@ -624,13 +685,13 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
                        int* launches, KernelTimer& tm, cudaStream_t st) {
   typedef typename Scalar<T>::acc Acc;
   const int64_t n = A.n;
-  const unsigned fg = (unsigned)ceil_div(k, 128);
+  const unsigned fg = (unsigned)ceil_div(k, 8);
 #define RB_INIT(L_, V_) \
   cg_init_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, dinv, R, P, Xs, (Acc*)part_a, part_b)
   RB_DISPATCH_LV(sh, RB_INIT);
 #undef RB_INIT
   RB_LAUNCH_CHECK();
-  fin_init_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable);
+  fin_init_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable);
   RB_LAUNCH_CHECK();
   *launches += 2;
   int it = 0;
@@ -642,14 +703,14 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       RB_TRY(tm.record(st));
       RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, sh, st)));
       RB_TRY(tm.record(st));
-      fin_alpha_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, cs);
+      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, cs);
 #define RB_UPD(L_, V_) \
   cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b)
       RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       RB_TRY(tm.record(st));
       if (b == burst - 1) RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-      fin_beta_kernel<Acc><<<fg, 128, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter);
+      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter);
 #define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P)
       RB_DISPATCH_LV(sh, RB_PUP);
 #undef RB_PUP
@@ -672,7 +733,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
                        rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv, cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k);
-  const unsigned fg = (unsigned)ceil_div(k, 128);
+  const unsigned fg = (unsigned)ceil_div(k, 8);
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
   int launches = 0;
   if (ldx != k) return fail(RB_EARG, "solve_block: internal ldx");
@@ -681,7 +742,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   RB_DISPATCH_LV(sh, RB_CN);
 #undef RB_CN
   RB_LAUNCH_CHECK();
-  fin_bnorm_kernel<<<fg, 128, 0, st>>>(k, (int)sh.grid, b.part_b, b.os);
+  fin_bnorm_kernel<<<fg, 256, 0, st>>>(k, (int)sh.grid, b.part_b, b.os);
   RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
   launches += 2;
   const double stall = 0.25;
@@ -693,7 +754,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     // R64 = B - A X (FP64)
     RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh, st)));
     RB_CUDA_TRY(cudaMemsetAsync(b.counter + 1, 0, sizeof(int32_t), st));
-    fin_outer_kernel<<<fg, 128, 0, st>>>(k, (int)sh.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
+    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
     RB_LAUNCH_CHECK();
     launches += 2;
     int32_t nact = 0;

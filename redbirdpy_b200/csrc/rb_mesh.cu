@@ -269,13 +269,14 @@ __device__ __forceinline__ void tet_cofactors(const double* __restrict__ node, i
 }
 
 __global__ void deldotdel_kernel(const double* __restrict__ node, const int32_t* __restrict__ elem,
-                                 int64_t ne, double* __restrict__ ddd) {
+                                 int64_t ne, double* __restrict__ ddd, double* __restrict__ evol) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
        e += (int64_t)gridDim.x * blockDim.x) {
     int4 en = reinterpret_cast<const int4*>(elem)[e];
     double c[4][3], det6;
     tet_cofactors(node, en, c, det6);
     const double s = 1.0 / (6.0 * fabs(det6));  // 1/(36 V)
+    if (evol) evol[e] = fabs(det6) * (1.0 / 6.0);
     int k = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -471,11 +472,11 @@ int rb_csr_pattern_fill(const int32_t* elem, int64_t nn, const int32_t* eptr, co
   return RB_OK;
 }
 
-int rb_deldotdel(const double* node, const int32_t* elem, int64_t ne, double* ddd, void* stream) {
+int rb_deldotdel(const double* node, const int32_t* elem, int64_t ne, double* ddd, double* evol, void* stream) {
   if (!node || !elem || !ddd || ne < 0) return fail(RB_EARG, "rb_deldotdel: bad arguments");
   if (ne == 0) return RB_OK;
   unsigned g = (unsigned)std::min<int64_t>(ceil_div(ne, 256), 148 * 32);
-  deldotdel_kernel<<<g, 256, 0, as_stream(stream)>>>(node, elem, ne, ddd);
+  deldotdel_kernel<<<g, 256, 0, as_stream(stream)>>>(node, elem, ne, ddd, evol);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }

@@ -68,8 +68,9 @@ class DeviceMesh:
         rowlen = self.indptr[1:] - self.indptr[:-1]
         self.rmax = int(rowlen.max().item())
         self.emax = int((self.eptr[1:] - self.eptr[:-1]).max().item())
-        self.evol = _f64(evol, dev) if evol is not None else None
+        self.evol_host = evol
         self._ddd = None
+        self._evol = None
         self.struct = _lib.RbMesh(
             self.nn, self.ne, self.nf, self.nnz, self.node.data_ptr(), self.elem.data_ptr(),
             self.face.data_ptr(), self.area.data_ptr(), self.eptr.data_ptr(), self.elist.data_ptr(),
@@ -84,13 +85,27 @@ class DeviceMesh:
         return p, lst
 
     # -------------------------------------------------------------- geometry
+    def _geometry(self):
+        self._ddd = torch.empty((self.ne, 10), dtype=torch.float64, device=self.device)
+        self._evol = torch.empty(self.ne, dtype=torch.float64, device=self.device)
+        call("rb_deldotdel", ptr(self.node), ptr(self.elem), self.ne, ptr(self._ddd), ptr(self._evol), stream())
+
     @property
     def ddd(self):
-        """Ne x 10 deldotdel rows on the device (computed once)."""
+        """Ne x 10 deldotdel rows on the device (computed once per mesh)."""
         if self._ddd is None:
-            self._ddd = torch.empty((self.ne, 10), dtype=torch.float64, device=self.device)
-            call("rb_deldotdel", ptr(self.node), ptr(self.elem), self.ne, ptr(self._ddd), stream())
+            self._geometry()
         return self._ddd
+
+    @property
+    def evol(self):
+        """Tet volumes on the device: cfg['evol'] when given, else |det|/6."""
+        if self._evol is None:
+            if self.evol_host is not None:
+                self._evol = _f64(self.evol_host, self.device)
+            else:
+                self._geometry()
+        return self._evol
 
     def deldotdel_host(self):
         return self.ddd.cpu().numpy()
@@ -121,7 +136,7 @@ def topology_of(elem, nn):
     hit = _TOPO.get("key")
     if hit == key:
         return _TOPO["mesh"]
-    m = DeviceMesh(np.zeros((nn, 3)), elem, None, None)
+    m = DeviceMesh(np.zeros((nn, 3)), elem, None, None, evol=np.zeros(elem.shape[0]))
     _TOPO.update(key=key, mesh=m, ref=elem)
     return m
 
@@ -238,9 +253,12 @@ class DeviceMatrix:
         return m
 
 
-def assemble(mesh, optics):
-    """femlhs on the device -> DeviceMatrix (redbirdpy/forward.py:90-256)."""
+def assemble(mesh, optics, ddd=None, evol=None):
+    """femlhs on the device -> DeviceMatrix (redbirdpy/forward.py:90-256).
+    ``ddd``/``evol`` default to the mesh's own deldotdel rows and volumes."""
     dev = mesh.device
+    ddd = mesh.ddd if ddd is None else ddd
+    evol = mesh.evol if evol is None else evol
     cplx = optics.omega > 0
     t64 = torch.complex128 if cplx else torch.float64
     t32 = torch.complex64 if cplx else torch.float32
@@ -248,8 +266,10 @@ def assemble(mesh, optics):
     v32 = torch.empty(mesh.nnz, dtype=t32, device=dev)
     d64 = torch.empty(mesh.nn, dtype=t64, device=dev)
     d32 = torch.empty(mesh.nn, dtype=t32, device=dev)
-    call("rb_femlhs", ctypes.byref(mesh.struct), ctypes.byref(optics.struct), ptr(v64), ptr(v32), ptr(d64),
-         ptr(d32), stream())
+    wb = _lib.lib().rb_femlhs_work_bytes(mesh.nn, mesh.ne)
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    call("rb_femlhs", ctypes.byref(mesh.struct), ctypes.byref(optics.struct), ptr(evol), ptr(ddd), ptr(v64), ptr(v32),
+         ptr(d64), ptr(d32), ptr(work), wb, stream())
     return DeviceMatrix(mesh, cplx, v64, v32, d64, d32)
 
 
@@ -384,8 +404,6 @@ def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=Non
                 torch.complex64: _lib.RB_C64}[J.dtype]
     w = {"mua": _lib.RB_JAC_MUA_REF, "mua_nodal": _lib.RB_JAC_MUA_NODAL, "D": _lib.RB_JAC_D}[what]
     ev = evol if evol is not None else mesh.evol
-    if ev is None:
-        raise ValueError("tet volumes are required")
     dd = ddd if ddd is not None else (mesh.ddd if w == _lib.RB_JAC_D else None)
     colsd = _i32(cols, dev)
     ps = _i32(psrc, dev)

@@ -63,12 +63,14 @@ def runforward(cfg, **kwargs):
 def femlhs(cfg, deldotdel_mat=None, wavelength="", mode=1):
     """FEM system matrix as scipy CSR (redbirdpy/forward.py:90-256).
 
-    Assembled on the GPU from the node coordinates; the element gradients are
-    recomputed there, so ``deldotdel_mat`` (accepted for signature
-    compatibility) must describe the same geometry as ``cfg['node']``."""
+    Assembled on the GPU from ``deldotdel_mat`` (as the reference does;
+    None = the mesh's own, computed on the GPU) and ``cfg['evol']``."""
     _check_single_wavelength(cfg)
     mesh = engine.mesh_of(cfg)
-    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode))
+    ddd = None
+    if deldotdel_mat is not None and deldotdel_mat is not cfg.get("deldotdel"):
+        ddd = torch.as_tensor(np.ascontiguousarray(deldotdel_mat, dtype=np.float64), device=mesh.device)
+    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode), ddd=ddd)
     A = mesh.csr_host(mat.val64)
     A.has_sorted_indices = True
     return A
