@@ -19,7 +19,14 @@
 namespace rb {
 
 constexpr int kBlk = 256;
-constexpr int kGridMax = 148 * 8;
+// resident blocks per SM of the row kernels, by scalar type: sets both the
+// register budget (__launch_bounds__) and the single-wave grid size
+template <typename T> struct Bps { static constexpr int value = 4; };
+template <> struct Bps<cdouble> { static constexpr int value = 3; };
+// the SpMM gathers are latency bound: give the FP32 one more resident warps
+template <typename T> struct BpsSpmm { static constexpr int value = Bps<T>::value; };
+template <> struct BpsSpmm<float> { static constexpr int value = 5; };
+constexpr int kGridMax = 148 * 8;       // upper bound of any grid (partials arrays)
 
 // ----------------------------------------------------------- vector access
 template <typename T, int V>
@@ -57,6 +64,18 @@ __device__ __forceinline__ void stv(T* __restrict__ p, const T (&o)[V]) {
 #pragma unroll
     for (int j = 0; j < V; ++j) p[j] = o[j];
   }
+}
+
+// Each block owns one contiguous chunk of rows (better L1 reuse of the x rows
+// that neighbouring matrix rows share); its kBlk/L groups walk the chunk.
+template <int L> __device__ __forceinline__ int64_t row_begin(int64_t n) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  return blockIdx.x * chunk + threadIdx.x / L;
+}
+template <int L> __device__ __forceinline__ int64_t row_end(int64_t n) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t e = (int64_t)(blockIdx.x + 1) * chunk;
+  return e < n ? e : n;
 }
 
 template <typename A> __device__ __forceinline__ A acc_zero();
@@ -102,7 +121,7 @@ enum { EPI_STORE = 0, EPI_PQDOT = 1, EPI_RESID = 2 };
 // y_row = A_row x; EPI_STORE: Y = y; EPI_PQDOT: Y = y, acc += x_row*y (unconj);
 // EPI_RESID: Y = B - y, acc += |B - y|^2   (B real FP64)
 template <typename T, int L, int V, int EPI>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, BpsSpmm<T>::value)
 spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
             const T* __restrict__ val, const T* __restrict__ X, T* __restrict__ Y,
             const double* __restrict__ B, void* __restrict__ part_) {
@@ -117,7 +136,7 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   alignas(16) A acc[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) acc[j] = acc_zero<A>();
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
     const int32_t b = indptr[row], e = indptr[row + 1];
     alignas(16) T y[V];
 #pragma unroll
@@ -229,7 +248,7 @@ __device__ __forceinline__ cdouble to_c(cdouble v) { return v; }
 
 // init: p = Dinv r; acc0 += r.p (unconj), acc1 += |r|^2; x = 0
 template <typename T, int L, int V>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __restrict__ R, T* __restrict__ P,
                T* __restrict__ Xs, typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
   typedef typename Scalar<T>::acc A;
@@ -243,7 +262,7 @@ cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __rest
   alignas(16) double arr[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
     if (!on) continue;
     const T d = dinv[row];
     alignas(16) T r[V], p[V], z[V];
@@ -264,7 +283,7 @@ cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __rest
 
 // x += a p; r -= a q; z = Dinv r; acc rz += r.z, rr += |r|^2
 template <typename T, int L, int V>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
                  T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
                  typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
@@ -286,7 +305,7 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
   alignas(16) double arr[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
     if (!on) continue;
     const T d = dinv[row];
     alignas(16) T x[V], r[V], p[V], q[V];
@@ -311,7 +330,7 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
 
 // p = Dinv r + beta p  (active columns only)
 template <typename T, int L, int V>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
                   const T* __restrict__ R, T* __restrict__ P) {
   const int lane = threadIdx.x % L;
@@ -327,7 +346,7 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
     any |= act[j];
   }
   if (!any) return;
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
     const T d = dinv[row];
     alignas(16) T r[V], p[V];
     ldv<T, V>(R + row * k + c0, r);
@@ -523,7 +542,7 @@ __global__ void correct_kernel(int64_t n, int64_t k, const T* __restrict__ D, co
 
 // squared column norms of a real FP64 n x k array
 template <int L, int V>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, 4)
 colnorm_kernel(int64_t n, int64_t k, const double* __restrict__ B, double* __restrict__ part) {
   __shared__ double sm[kBlk * V];
   const int lane = threadIdx.x % L;
@@ -533,7 +552,7 @@ colnorm_kernel(int64_t n, int64_t k, const double* __restrict__ B, double* __res
   alignas(16) double acc[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) acc[j] = 0.0;
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
     if (!on) continue;
 #pragma unroll
     for (int j = 0; j < V; ++j) {
@@ -550,13 +569,24 @@ struct Shape {
   unsigned grid;
 };
 
-static Shape pick_shape(int64_t n, int64_t k) {
+static int64_t num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (sms * 5 > kGridMax) sms = kGridMax / 5;  // partials arrays hold kGridMax blocks
+  }
+  return sms;
+}
+
+static Shape pick_shape(int64_t n, int64_t k, int bps) {
   Shape s;
   s.V = (k % 4 == 0) ? 4 : (k % 2 == 0) ? 2 : 1;
   int need = (int)ceil_div(k, s.V);
   s.L = need <= 4 ? 4 : need <= 8 ? 8 : need <= 16 ? 16 : 32;
-  const int64_t groups = ceil_div(n, 1);
-  s.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(kGridMax, ceil_div(groups, kBlk / s.L)));
+  // one resident wave: every block stays on its SM for the whole kernel
+  s.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(num_sms() * bps, ceil_div(n, kBlk / s.L)));
   return s;
 }
 
@@ -679,7 +709,8 @@ struct KernelTimer {
 };
 
 template <typename T>
-static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, const Shape& sh, void* part_a,
+static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, const Shape& sh, const Shape& shs,
+                       void* part_a,
                        double* part_b, T* Xs, T* R, T* P, T* Q, ColState* cs, const int32_t* enable,
                        int32_t* counter, double tol, int maxiter, int check_every, int* iters_out,
                        int* launches, KernelTimer& tm, cudaStream_t st) {
@@ -701,9 +732,9 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
     RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
     for (int b = 0; b < burst; ++b) {
       RB_TRY(tm.record(st));
-      RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, sh, st)));
+      RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, shs, st)));
       RB_TRY(tm.record(st));
-      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, cs);
+      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)shs.grid, (const Acc*)part_a, cs);
 #define RB_UPD(L_, V_) \
   cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b)
       RB_DISPATCH_LV(sh, RB_UPD);
@@ -732,17 +763,19 @@ template <typename T64, typename T>
 static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, int64_t k, const rb_solve_opts& o,
                        rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv, cudaStream_t st) {
   const int64_t n = A.n;
-  const Shape sh = pick_shape(n, k);
+  const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
+  const Shape shs = pick_shape(n, k, BpsSpmm<T>::value); // inner SpMM
+  const Shape sh64 = pick_shape(n, k, Bps<T64>::value);  // FP64 residual kernels
   const unsigned fg = (unsigned)ceil_div(k, 8);
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
   int launches = 0;
   if (ldx != k) return fail(RB_EARG, "solve_block: internal ldx");
   // ||b|| per column
-#define RB_CN(L_, V_) colnorm_kernel<L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, B, b.part_b)
-  RB_DISPATCH_LV(sh, RB_CN);
+#define RB_CN(L_, V_) colnorm_kernel<L_, V_><<<sh64.grid, kBlk, 0, st>>>(n, k, B, b.part_b)
+  RB_DISPATCH_LV(sh64, RB_CN);
 #undef RB_CN
   RB_LAUNCH_CHECK();
-  fin_bnorm_kernel<<<fg, 256, 0, st>>>(k, (int)sh.grid, b.part_b, b.os);
+  fin_bnorm_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os);
   RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
   launches += 2;
   const double stall = 0.25;
@@ -752,9 +785,9 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   int sweep_flag = 0;
   for (outer = 0; outer <= o.max_outer; ++outer) {
     // R64 = B - A X (FP64)
-    RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh, st)));
+    RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh64, st)));
     RB_CUDA_TRY(cudaMemsetAsync(b.counter + 1, 0, sizeof(int32_t), st));
-    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
+    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
     RB_LAUNCH_CHECK();
     launches += 2;
     int32_t nact = 0;
@@ -765,7 +798,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     RB_LAUNCH_CHECK();
     launches += 1;
     int it = 0;
-    RB_TRY(inner_solve<T>(A, val, dinv, k, sh, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
+    RB_TRY(inner_solve<T>(A, val, dinv, k, sh, shs, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
                           b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, st));
     total_iters += it;
     if (it >= o.maxiter) sweep_flag = 1;
@@ -902,7 +935,7 @@ int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs, const r
 int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs, void* stream) {
   if (!A || !X || !Y || nrhs < 1) return fail(RB_EARG, "rb_spmm: bad arguments");
   if (nrhs > kMaxCols) return fail(RB_ESIZE, "rb_spmm: at most %lld columns", (long long)kMaxCols);
-  const Shape sh = pick_shape(A->n, nrhs);
+  const Shape sh = pick_shape(A->n, nrhs, 3);
   cudaStream_t st = as_stream(stream);
   switch (kind) {
     case RB_F64: return spmm_t<double, EPI_STORE>(*A, (const double*)A->val64, (const double*)X, (double*)Y, nullptr, nullptr, nrhs, sh, st);

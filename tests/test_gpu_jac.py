@@ -81,10 +81,12 @@ def test_exact_jacobians_vs_central_fd(golden, omega):
     for n in nodes:
         # d/dmua at fixed musp = dA/dmua|_D + dD/dmua dA/dD ; d/dmus = dD/dmus dA/dD
         for col, expect in ((0, jm[:, n] - 3 * D[n] ** 2 * jd[:, n]), (1, -3 * D[n] ** 2 * jd[:, n])):
-            h = 1e-4 * prop[n, col]
+            # h = 1e-3 relative: below that the FD quotient is dominated by the
+            # rounding of the direct solves (checked on the CPU against h = 1e-2)
+            h = 1e-3 * prop[n, col]
             p1, p2 = prop.copy(), prop.copy()
             p1[n, col] += h
             p2[n, col] -= h
             fd = (_oracle_detvals(dict(ocfg, prop=p1)) - _oracle_detvals(dict(ocfg, prop=p2))) / (2 * h)
             scale = np.abs(fd).max()
-            assert np.abs(fd - expect).max() <= 1e-6 * scale, (n, col, np.abs(fd - expect).max() / scale)
+            assert np.abs(fd - expect).max() <= 1e-5 * scale, (n, col, np.abs(fd - expect).max() / scale)
