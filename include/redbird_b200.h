@@ -113,6 +113,19 @@ int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, const double* evol, 
               void* val64, void* val32, void* dinv64, void* dinv32, void* work, size_t work_bytes,
               void* stream);
 
+/* rb_femlhs without a workspace, for callers that cannot allocate device
+ * memory (no counterpart in the reference): the scratch array comes from a
+ * fixed 32 MiB device array inside this library, enough for 4,194,304 nodes
+ * (per-node properties) or tets (per-tet properties); larger meshes get
+ * RB_ESIZE.  The first call on each device looks up that array's address and
+ * should therefore come before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU (different streams or threads
+ * without ordering between them) race; calls on one stream are safe.
+ * Allocates nothing (no cudaMalloc/cudaFree). */
+int rb_femlhs_noalloc(const rb_mesh* mesh, const rb_optics* optics, const double* evol,
+                      const double* ddd, void* val64, void* val32, void* dinv64, void* dinv32,
+                      void* stream);
+
 /* deldotdel (redbirdpy/utility.py:53-98): ne x 10 values V*grad(phi_i).grad(phi_j)
  * for the pairs (0,0),(0,1),(0,2),(0,3),(1,1),(1,2),(1,3),(2,2),(2,3),(3,3),
  * from the node coordinates; evol (optional, ne) receives |V| like

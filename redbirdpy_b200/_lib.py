@@ -62,6 +62,8 @@ _SIGS = {
     "rb_femlhs_work_bytes": (_sz, [_i64, _i64]),
     "rb_femlhs": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp, _vp,
                                  _vp, _sz, _vp]),
+    "rb_femlhs_noalloc": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp,
+                                         _vp, _vp]),
     "rb_deldotdel": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp]),
     "rb_tsearch": (ctypes.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "rb_point_rhs": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),

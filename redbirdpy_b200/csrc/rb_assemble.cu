@@ -17,6 +17,7 @@
 // D = 1/(3(mua+musp)) per node (or per tet) in the workspace so that no
 // division is repeated per incidence.
 #include <algorithm>
+#include <mutex>
 
 #include "rb_common.cuh"
 
@@ -242,6 +243,85 @@ extern "C" int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, const dou
   double* dco = reinterpret_cast<double*>(work);
   const bool cplx = o.omega > 0.0;
   if (cplx)
+    return o.kind == RB_PROP_NODE
+               ? launch_femlhs<true, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
+               : launch_femlhs<true, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
+  return o.kind == RB_PROP_NODE
+             ? launch_femlhs<false, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
+             : launch_femlhs<false, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
+}
+
+// --------------------------------------------------------------------------
+// Assembly for callers that cannot allocate device memory.
+//
+// rb_femlhs needs one scratch array (the diffusion coefficient per node or
+// per tet) and takes it from a caller-provided workspace.  Some callers have
+// no way to provide one: host code in another language that binds this C ABI
+// and owns only its own input/output buffers, or code that runs where a
+// cudaMalloc is not allowed (it would synchronise the device, or the memory
+// pool belongs to someone else).  rb_femlhs_noalloc gives them the same
+// assembly with the scratch taken from a fixed array compiled into this
+// library instead.
+namespace rb {
+
+// Capacity of the fixed scratch: 4,194,304 doubles (32 MiB), i.e. meshes with
+// up to that many nodes (per-node properties) or tets (per-tet properties).
+// Every GPU that loads this library keeps these 32 MiB until the process ends.
+constexpr int64_t kNoallocScratchMax = 4 * 1024 * 1024;
+static __device__ __align__(256) double g_noalloc_dco[kNoallocScratchMax];
+
+// Host code cannot use g_noalloc_dco directly (on the host that name is only a
+// stand-in for the device array); its device address is looked up once per
+// device, with that device current, and cached here.
+constexpr int kNoallocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+static int noalloc_scratch(double** out) {
+  int dev = -1;
+  RB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return fail(RB_EARG, "rb_femlhs_noalloc: device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_dco);
+    if (e != cudaSuccess || !p)
+      return fail(RB_ECUDA, "rb_femlhs_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return RB_OK;
+}
+
+}  // namespace rb
+
+extern "C" int rb_femlhs_noalloc(const rb_mesh* mesh, const rb_optics* optics, const double* evol,
+                                 const double* ddd, void* val64, void* val32, void* dinv64, void* dinv32,
+                                 void* stream) {
+  if (!mesh || !optics || !val64 || !evol || !ddd)
+    return fail(RB_EARG, "rb_femlhs_noalloc: mesh, optics, evol, ddd and val64 are required");
+  const rb_mesh& m = *mesh;
+  const rb_optics& o = *optics;
+  if (o.kind != RB_PROP_NODE && o.kind != RB_PROP_ELEM) return fail(RB_EARG, "rb_femlhs_noalloc: bad property kind");
+  const int64_t np = (o.kind == RB_PROP_NODE) ? m.nn : m.ne;
+  if (np < 0 || np > kNoallocScratchMax)
+    return fail(RB_ESIZE,
+                "rb_femlhs_noalloc: %lld %s exceed the fixed scratch of %lld entries; use rb_femlhs with a workspace",
+                (long long)np, o.kind == RB_PROP_NODE ? "nodes" : "tets", (long long)kNoallocScratchMax);
+  if (!m.elem || !m.indptr || !m.indices || !m.node_eptr || !m.node_elist || !m.node_fptr)
+    return fail(RB_EARG, "rb_femlhs_noalloc: mesh arrays missing");
+  if (m.nf > 0 && (!m.face || !m.area || !m.node_flist))
+    return fail(RB_EARG, "rb_femlhs_noalloc: boundary arrays missing");
+  if (!o.mua || !o.musp) return fail(RB_EARG, "rb_femlhs_noalloc: mua and musp are required");
+  if (!(o.omega >= 0.0)) return fail(RB_EARG, "rb_femlhs_noalloc: omega must be >= 0");
+  double* dco = nullptr;
+  RB_TRY(noalloc_scratch(&dco));
+  // the prologue kernel overwrites every scratch entry the assembly reads, so
+  // nothing left by an earlier call needs clearing
+  cudaStream_t st = as_stream(stream);
+  if (o.omega > 0.0)
     return o.kind == RB_PROP_NODE
                ? launch_femlhs<true, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
                : launch_femlhs<true, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
