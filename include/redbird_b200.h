@@ -228,6 +228,10 @@ int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs,
  * out RB_F32/RB_C64 computes in FP32.  evol: ne tet volumes; ddd: the ne x 10
  * deldotdel rows (required for RB_JAC_D only), as jac receives them. */
 enum rb_jac_what { RB_JAC_MUA_REF = 0, RB_JAC_MUA_NODAL = 1, RB_JAC_D = 2 };
+/* extra out_kind values for complex phi: real FP32 / FP64 output with the
+ * real parts in rows 0..nsd-1 and the imaginary parts in rows nsd..2nsd-1
+ * (matreform 'real' stacking, redbirdpy/recon.py:532-546) */
+enum rb_jac_split { RB_JAC_SPLIT_F32 = 4, RB_JAC_SPLIT_F64 = 5 };
 int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
@@ -238,6 +242,34 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
 int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,
                 const int32_t* src_col, const int32_t* det_col, int64_t nsd, void* je,
                 void* stream);
+
+/* ------------------------------------------------------ Gauss-Newton step
+ * reginvunder (redbirdpy/recon.py:429-509) on the device:
+ *   H = alpha J J^T            rb_gram: tcgen05 tensor cores, TF32 inputs,
+ *                              FP32 accumulation, FP64 output (all of H).
+ *                              With Jlo != NULL (J = hi + lo, from
+ *                              rb_split_tf32) H = hi hi^T + hi lo^T + lo hi^T,
+ *                              close to FP32-input accuracy at 3x the work.
+ *                              J: M x K FP32 rows, ldj % 4 == 0, 16-B aligned.
+ *   H += lambda I, normalise   rb_reginv_prepare (_normalize_diag, recon.py:784-789)
+ *   H = L L^T                  rb_cholesky (FP64, in place, lower)
+ *   L L^T x = b                rb_chol_solve (in place on x)
+ *   out = alpha J^T y + beta out   rb_gemv_t
+ *   sum(J^2)                   rb_sumsq (Frobenius block scale, recon.py:235) */
+size_t rb_gram_work_bytes(void);
+int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha,
+            double* H, int64_t ldh, void* work, size_t work_bytes, void* stream);
+int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* stream);
+int rb_reginv_prepare(double* H, int64_t M, int64_t ldh, double lambda, double* di, void* stream);
+size_t rb_cholesky_work_bytes(void);
+int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes, void* stream);
+int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stream);
+int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha,
+              double beta, double* out, void* stream);
+size_t rb_sumsq_work_bytes(void);
+int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
+             size_t work_bytes, void* stream);
+int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream);
 
 #ifdef __cplusplus
 }

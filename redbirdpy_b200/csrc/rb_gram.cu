@@ -1,0 +1,304 @@
+// Gram matrix H = alpha * J J^T of the Gauss-Newton step on the 5th-generation
+// tensor cores (tcgen05, TF32 inputs, FP32 accumulation in tensor memory).
+//
+// J is M x K FP32, row-major (K contiguous): the Jacobian rows of redbirdpy's
+// jac / matreform layout.  Both MMA operands are row blocks of the same J and
+// are "K-major", so one TMA tensor map (box 32 x 128, 128-byte swizzle)
+// serves A (128 rows) and B (256 rows as two boxes).  One CTA computes one
+// 128 x 256 tile of H; only tiles that touch the upper triangle are launched
+// and a second kernel mirrors the upper triangle into the lower one.
+//
+// Warp roles (192 threads): warp 0 = TMA producer (one lane), warp 1 = TMEM
+// allocator + MMA issuer (one lane), warps 2..5 = epilogue (each reads the
+// 32 TMEM lanes of its quarter with tcgen05.ld and writes FP64 rows of H).
+// A 4-stage shared-memory ring (48 KB per stage) is synchronised with
+// mbarriers; every wait is bounded and reports a timeout through an error
+// word instead of hanging.
+#include <cuda.h>
+
+#include <algorithm>
+
+#include "rb_common.cuh"
+
+namespace rb {
+
+constexpr int kGM = 128;   // tile rows (A)
+constexpr int kGN = 256;   // tile columns (B rows)
+constexpr int kGK = 32;    // FP32 elements per 128-byte row of a stage
+constexpr int kGStages = 4;
+constexpr int kGABytes = kGM * kGK * 4;  // 16 KB
+constexpr int kGBBytes = kGN * kGK * 4;  // 32 KB
+constexpr int kGStageBytes = kGABytes + kGBBytes;
+constexpr int kGSmem = kGStages * kGStageBytes + 1024 + 256;
+constexpr int kGThreads = 192;
+constexpr uint32_t kGTmemCols = 256;
+constexpr long long kGWaitLimit = 1LL << 24;  // polls before a wait gives up (seconds)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bounded parity wait: false (and *err set) when the phase never completes
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+  for (long long i = 0; i < kGWaitLimit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  atomicExch(err, code);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major operand, 128-byte swizzle,
+// 8-row groups 1024 bytes apart (stride byte offset), descriptor version 1
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;                    // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;                    // version
+  d |= (uint64_t)2u << 61;                    // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 256
+constexpr uint32_t kGIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kGN >> 3) << 17) |
+                             ((uint32_t)(kGM >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kGIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// number of 128-row blocks of tile column bj that touch the upper triangle
+__device__ __host__ __forceinline__ int64_t gram_col_tiles(int64_t bj, int64_t nbi) {
+  const int64_t need = (bj * kGN + kGN - 1) / kGM + 1;
+  return need < nbi ? need : nbi;
+}
+
+__global__ void __launch_bounds__(kGThreads, 1)
+gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_lo, int segs,
+                 int64_t M, int64_t K, double* __restrict__ H, int64_t ldh, double alpha, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char gsm_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kGStages * kGStageBytes);
+  uint64_t* empty = full + kGStages;
+  uint64_t* accf = empty + kGStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+
+  // tile (bi, bj): walk the tile columns until this block's index falls inside
+  const int64_t nbi = (M + kGM - 1) / kGM, nbj = (M + kGN - 1) / kGN;
+  int64_t t = blockIdx.x, bj = 0;
+  while (bj < nbj && t >= gram_col_tiles(bj, nbi)) t -= gram_col_tiles(bj++, nbi);
+  if (bj >= nbj) return;
+  const int64_t bi = t;
+  const int i0 = (int)(bi * kGM), j0 = (int)(bj * kGN);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kGStages; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(accf), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kGTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  // segs == 1: H = J J^T.  segs == 3 (split precision, J = hi + lo):
+  // H = hi hi^T + hi lo^T + lo hi^T, one K sweep per product, one accumulator
+  const int nk1 = (int)((K + kGK - 1) / kGK);
+  const int nk = nk1 * segs;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % kGStages;
+        if (kb >= kGStages && !mbar_wait(smem_u32(&empty[s]), ((kb / kGStages) - 1) & 1, err, 1)) break;
+        const uint32_t a = smem_u32(sm + s * kGStageBytes);
+        const uint32_t b = a + kGABytes;
+        const uint32_t bar = smem_u32(&full[s]);
+        const int seg = kb / nk1, kx = (kb - seg * nk1) * kGK;
+        const CUtensorMap* ma = (seg == 2) ? &tmap_lo : &tmap;
+        const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
+        mbar_expect_tx(bar, kGStageBytes);
+        tma_load_2d(a, ma, bar, kx, i0);
+        tma_load_2d(b, mb, bar, kx, j0);
+        tma_load_2d(b + kGABytes, mb, bar, kx, j0 + kGM);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      bool ok = true;
+      for (int kb = 0; kb < nk && ok; ++kb) {
+        const int s = kb % kGStages;
+        ok = mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a = smem_u32(sm + s * kGStageBytes);
+        const uint32_t b = a + kGABytes;
+#pragma unroll
+        for (int k = 0; k < kGK / 8; ++k)  // kind::tf32 consumes K = 8 (32 bytes) per MMA
+          umma_tf32(tmem, umma_desc_sw128(a + 32 * k), umma_desc_sw128(b + 32 * k), (kb | k) != 0);
+        umma_commit(smem_u32(&empty[s]));
+      }
+      umma_commit(smem_u32(accf));
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 = tile rows
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    // warp-uniform outcome: tcgen05.ld below needs the whole warp
+    const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(accf), 0, err, 3));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (got) {
+      const int64_t gi = (int64_t)i0 + row;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kGN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (gi < M) {
+          double* dst = H + gi * ldh + j0 + c0;
+#pragma unroll
+          for (int u = 0; u < 32; ++u)
+            if ((int64_t)j0 + c0 + u < M) dst[u] = alpha * (double)__uint_as_float(v[u]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGTmemCols));
+}
+
+// H[j][i] = H[i][j] for i < j (upper triangle -> lower)
+__global__ void mirror_upper_kernel(double* __restrict__ H, int64_t M, int64_t ldh) {
+  __shared__ double tile[32][33];
+  const int64_t bi = blockIdx.y, bj = blockIdx.x;
+  if (bj < bi) return;  // tiles of the upper triangle only
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += blockDim.y) {
+    const int64_t i = bi * 32 + r, j = bj * 32 + tx;
+    tile[r][tx] = (i < M && j < M) ? H[i * ldh + j] : 0.0;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += blockDim.y) {
+    const int64_t i = bj * 32 + r, j = bi * 32 + tx;  // destination row i (lower part)
+    if (i < M && j < M && i > j) H[i * ldh + j] = tile[tx][r];
+  }
+}
+
+typedef decltype(&cuTensorMapEncodeTiled) EncodeTiledFn;
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+static int make_map(CUtensorMap* map, const float* J, int64_t M, int64_t K, int64_t ldj) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fail(RB_ECUDA, "rb_gram: cuTensorMapEncodeTiled unavailable");
+  cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)M};
+  cuuint64_t gstride[1] = {(cuuint64_t)ldj * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)kGK, (cuuint32_t)kGM};
+  cuuint32_t estride[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(J), gdim, gstride, box, estride,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(RB_ECUDA, "rb_gram: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return RB_OK;
+}
+
+extern "C" {
+
+size_t rb_gram_work_bytes(void) { return 256; }
+
+int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
+            void* work, size_t work_bytes, void* stream) {
+  if (!J || !H || !work || M < 1 || K < 1 || ldj < K || ldh < M)
+    return fail(RB_EARG, "rb_gram: bad arguments");
+  if (work_bytes < rb_gram_work_bytes()) return fail(RB_EARG, "rb_gram: workspace too small");
+  if ((reinterpret_cast<uintptr_t>(J) & 15) || (Jlo && (reinterpret_cast<uintptr_t>(Jlo) & 15)) || (ldj % 4))
+    return fail(RB_EARG, "rb_gram: J must be 16-byte aligned with a row stride that is a multiple of 4 floats");
+  if (M > (int64_t)1 << 30 || K > (int64_t)1 << 30) return fail(RB_ESIZE, "rb_gram: matrix too large");
+  CUtensorMap map, map_lo;
+  RB_TRY(make_map(&map, J, M, K, ldj));
+  RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj));
+  const int segs = Jlo ? 3 : 1;
+  cudaStream_t st = as_stream(stream);
+  int* err = reinterpret_cast<int*>(work);
+  RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+  const int64_t nbi = ceil_div(M, kGM), nbj = ceil_div(M, kGN);
+  int64_t tiles = 0;
+  for (int64_t bj = 0; bj < nbj; ++bj) tiles += gram_col_tiles(bj, nbi);
+  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  gram_tf32_kernel<<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, K, H, ldh, alpha, err);
+  RB_LAUNCH_CHECK();
+  dim3 mg((unsigned)ceil_div(M, 32), (unsigned)ceil_div(M, 32));
+  mirror_upper_kernel<<<mg, dim3(32, 8), 0, st>>>(H, M, ldh);
+  RB_LAUNCH_CHECK();
+  int herr = 0;
+  RB_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr) return fail(RB_ECUDA, "rb_gram: pipeline wait timed out (stage %d)", herr);
+  return RB_OK;
+}
+
+}  // extern "C"

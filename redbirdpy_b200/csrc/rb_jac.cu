@@ -77,9 +77,9 @@ __host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, i
   return (s + 15) / 16 * 16;
 }
 
-template <typename C, typename In, int TN>
+template <typename C, typename In, int TN, bool SPLIT>
 __global__ void __launch_bounds__(kJacThreads)
-jac_kernel(JacArgs a, const In* __restrict__ phi, C* __restrict__ J) {
+jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   typedef typename JacT<C>::real R;
   extern __shared__ __align__(16) unsigned char smem[];
   const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax;
@@ -190,7 +190,15 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, C* __restrict__ J) {
     const C* Cn = sC + (size_t)t * rmax * nd + pd;
     C s = s_zero(C());
     for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
-    J[k * a.ldj + n] = s;
+    if constexpr (SPLIT) {
+      // complex rows split into a block of real parts and a block of
+      // imaginary parts (matreform 'real', recon.py:532-546)
+      R* Jr = reinterpret_cast<R*>(Jout);
+      Jr[k * a.ldj + n] = s.x;
+      Jr[(a.nsd + k) * a.ldj + n] = s.y;
+    } else {
+      reinterpret_cast<C*>(Jout)[k * a.ldj + n] = s;
+    }
   }
 }
 
@@ -220,7 +228,7 @@ __global__ void jac_elem_kernel(const double* __restrict__ evol, const int32_t* 
   }
 }
 
-template <typename C, typename In>
+template <typename C, typename In, bool SPLIT = false>
 static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   int TN = 8;
   const size_t budget = 110 * 1024;
@@ -230,9 +238,9 @@ static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t s
   const unsigned g = (unsigned)ceil_div(a.nn, TN);
 #define RB_JL(TN_)                                                                                     \
   do {                                                                                                 \
-    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                      (int)sm));                                                        \
-    jac_kernel<C, In, TN_><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, (C*)J);                        \
+    jac_kernel<C, In, TN_, SPLIT><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);                      \
   } while (0)
   switch (TN) {
     case 8: RB_JL(8); break;
@@ -266,6 +274,14 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
             cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what};
   cudaStream_t st = as_stream(stream);
   const bool cin = (phi_kind == RB_C128 || phi_kind == RB_C64);
+  if (out_kind == RB_JAC_SPLIT_F32 || out_kind == RB_JAC_SPLIT_F64) {
+    if (!cin) return fail(RB_EARG, "rb_jac: split output needs complex phi");
+    if (out_kind == RB_JAC_SPLIT_F32)
+      return phi_kind == RB_C64 ? launch_jac<cfloat, cfloat, true>(a, phi, J, st)
+                                : launch_jac<cfloat, cdouble, true>(a, phi, J, st);
+    return phi_kind == RB_C64 ? launch_jac<cdouble, cfloat, true>(a, phi, J, st)
+                              : launch_jac<cdouble, cdouble, true>(a, phi, J, st);
+  }
   const bool cout = (out_kind == RB_C128 || out_kind == RB_C64);
   if (cin != cout) return fail(RB_EARG, "rb_jac: complex phi needs a complex output kind and vice versa");
   switch (out_kind * 4 + phi_kind) {

@@ -426,3 +426,92 @@ def jacobian_elem(mesh, phi, sd, evol=None):
     call("rb_jac_elem", ctypes.byref(mesh.struct), ptr(ev), ptr(phi), kind, phi.shape[1], ptr(sc), ptr(dc), nsd,
          ptr(Je), stream())
     return Je
+
+
+# ------------------------------------------------------------ Gauss-Newton
+def _pad4(n):
+    return (n + 3) // 4 * 4
+
+
+def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference"):
+    """The real FP32 Jacobian of the GN step, rows x columns = (nsd or 2 nsd)
+    x (len(params) * nn), stored with a row stride padded to 4 floats.
+    Complex fields give matreform 'real' stacking [Re; Im] (recon.py:532-546).
+    mode 'reference' = redbirdpy's jac for mua (forward.py:509-569);
+    'exact' = derivatives of the node-based assembly ('mua' at fixed D, 'D')."""
+    cols, det0, ndet, psrc, pdet, _, _ = pair_map(sd)
+    nsd = len(psrc)
+    cplx = phi.is_complex()
+    rows = 2 * nsd if cplx else nsd
+    nn = mesh.nn
+    ldj = _pad4(len(params) * nn)
+    J = torch.zeros((rows, ldj), dtype=torch.float32, device=phi.device)
+    out_kind = _lib.RB_JAC_SPLIT_F32 if cplx else _lib.RB_F32
+    phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
+                torch.complex64: _lib.RB_C64}[phi.dtype]
+    colsd, ps, pd = _i32(cols, phi.device), _i32(psrc, phi.device), _i32(pdet, phi.device)
+    for p, name in enumerate(params):
+        if name == "mua":
+            w = _lib.RB_JAC_MUA_REF if mode == "reference" else _lib.RB_JAC_MUA_NODAL
+        elif name == "D":
+            w = _lib.RB_JAC_D
+        else:
+            raise ValueError(f"unknown parameter {name}")
+        sub = J[:, p * nn:]
+        call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0,
+             ndet, ptr(ps), ptr(pd), nsd, ptr(sub), ldj, out_kind, mesh.rmax, mesh.emax, ptr(mesh.evol),
+             ptr(mesh.ddd if w == _lib.RB_JAC_D else None), stream())
+    return J, len(params) * nn
+
+
+def sumsq(J, K):
+    out = torch.empty(1, dtype=torch.float64, device=J.device)
+    wb = _lib.lib().rb_sumsq_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+    call("rb_sumsq", ptr(J), J.shape[0], K, J.shape[1], ptr(out), ptr(work), wb, stream())
+    return out
+
+
+def gram(J, K, alpha=1.0, precision="tf32"):
+    """H = alpha J J^T (M x M FP64) on the tensor cores.  precision 'tf32'
+    (one pass) or 'tf32x3' (split hi/lo, three passes; J is left as hi and
+    the returned lo completes it)."""
+    M, ldj = J.shape
+    H = torch.empty((M, M), dtype=torch.float64, device=J.device)
+    lo = None
+    if precision == "tf32x3":
+        lo = torch.empty_like(J)
+        call("rb_split_tf32", ptr(J), ptr(lo), M, K, ldj, stream())
+    elif precision != "tf32":
+        raise ValueError(f"unknown gram precision {precision}")
+    wb = _lib.lib().rb_gram_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+    call("rb_gram", ptr(J), ptr(lo), M, K, ldj, float(alpha), ptr(H), M, ptr(work), wb, stream())
+    return H, lo
+
+
+def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None):
+    """reginvunder (recon.py:429-509) for the rows of J (scaled by sqrt(alpha)):
+    H = alpha J J^T + lam I, unit-diagonal normalisation, FP64 Cholesky,
+    returns alpha J^T y on the device (K-vector, FP64)."""
+    M, ldj = J.shape
+    dev = J.device
+    H, lo = gram(J, K, alpha, precision)
+    if lam_rel is not None:  # lambda relative to the largest diagonal entry
+        lam = float(lam_rel) * float(H.diagonal().max().item())
+    di = torch.empty(M, dtype=torch.float64, device=dev)
+    call("rb_reginv_prepare", ptr(H), M, M, float(lam), ptr(di), stream())
+    wb = _lib.lib().rb_cholesky_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    call("rb_cholesky", ptr(H), M, M, ptr(work), wb, stream())
+    rr = torch.as_tensor(np.ascontiguousarray(r, dtype=np.float64), device=dev) if not torch.is_tensor(r) else r
+    t = torch.empty(M, dtype=torch.float64, device=dev)
+    call("rb_vec_mul", ptr(di), ptr(rr), ptr(t), M, stream())
+    call("rb_chol_solve", ptr(H), M, M, ptr(t), stream())
+    y = torch.empty(M, dtype=torch.float64, device=dev)
+    call("rb_vec_mul", ptr(di), ptr(t), ptr(y), M, stream())
+    out = torch.empty(K, dtype=torch.float64, device=dev)
+    call("rb_gemv_t", ptr(J), M, K, ldj, ptr(y), float(alpha), 0.0, ptr(out), stream())
+    if lo is not None:  # J = hi + lo
+        call("rb_gemv_t", ptr(lo), M, K, ldj, ptr(y), float(alpha), 1.0, ptr(out), stream())
+    return out

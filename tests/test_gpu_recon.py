@@ -1,0 +1,116 @@
+"""GPU parity of the Gauss-Newton pieces: the tcgen05 Gram kernel against
+FP64 numpy, the regularised solves against the reference's reginv*, and the
+device GN loop against the reference's runrecon (golden fixtures)."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import redbirdpy_b200 as rbb  # noqa: E402
+from redbirdpy_b200 import engine  # noqa: E402
+from redbirdpy_b200._lib import RedbirdError  # noqa: E402
+
+from test_gpu_forward import cfg_from  # noqa: E402
+
+
+@pytest.mark.parametrize("M,K", [(8, 40), (300, 1000), (513, 2048), (1024, 4100)])
+@pytest.mark.parametrize("precision,tol", [("tf32", 3e-3), ("tf32x3", 2e-6)])
+def test_gram_tensor_cores(M, K, precision, tol):
+    rng = np.random.default_rng(M + K)
+    A = rng.standard_normal((M, K))
+    J, Kc = rbb.recon._device_rows(A)
+    H, _ = engine.gram(J, Kc, 0.5, precision)
+    H = H.cpu().numpy()
+    A32 = A.astype(np.float32).astype(np.float64)
+    ref = 0.5 * (A32 @ A32.T)
+    err = np.abs(H - ref).max() / np.abs(ref).max()
+    assert err < tol, err
+    assert np.array_equal(H, H.T)
+
+
+def test_gram_long_k_accuracy():
+    """K ~ 1e5 (Jacobian-like rows of mixed sign and decaying scale)."""
+    rng = np.random.default_rng(1)
+    M, K = 256, 100003
+    A = rng.standard_normal((M, K)) * np.exp(-np.linspace(0, 8, K))[None, :]
+    J, Kc = rbb.recon._device_rows(A)
+    A32 = A.astype(np.float32).astype(np.float64)
+    ref = A32 @ A32.T
+    for precision, tol in (("tf32", 3e-3), ("tf32x3", 1e-5)):
+        J2 = J.clone()
+        H, _ = engine.gram(J2, Kc, 1.0, precision)
+        err = np.abs(H.cpu().numpy() - ref).max() / np.abs(ref).max()
+        assert err < tol, (precision, err)
+
+
+def test_reginv_matches_reference(golden):
+    g = golden("dense_recon")
+    np.testing.assert_allclose(rbb.reginvunder(g["Ju"], g["ru"], 0.1), g["under"], rtol=1e-5,
+                               atol=1e-6 * np.abs(g["under"]).max())
+    np.testing.assert_allclose(rbb.reginvover(g["Jo"], g["ro"], 0.1), g["over"], rtol=1e-5,
+                               atol=1e-6 * np.abs(g["over"]).max())
+    np.testing.assert_allclose(rbb.reginv(g["Ju"], g["ru"], 0.3), g["reginv_u"], rtol=1e-5,
+                               atol=1e-6 * np.abs(g["reginv_u"]).max())
+    # TF32 single pass: the tensor-core form of the GN step
+    d = rbb.reginvunder(g["Ju"], g["ru"], 0.1, precision="tf32")
+    assert np.abs(d - g["under"]).max() / np.abs(g["under"]).max() < 5e-3
+
+
+def test_matreform_matches_reference(golden):
+    g = golden("dense_recon")
+    for form, a, r in (("real", "Ar", "rr"), ("logphase", "Al", "rl"), ("reim", "Ae", "re")):
+        A, rhs, _ = rbb.matreform(g["Jc"], g["y0"], g["y1"], form)
+        np.testing.assert_allclose(A, g[a], rtol=1e-14)
+        np.testing.assert_allclose(rhs, g[r], rtol=1e-14)
+    with pytest.raises(ValueError):
+        rbb.matreform(g["Jc"], g["y0"], g["y1"], "nope")
+
+
+def test_cholesky_rejects_indefinite():
+    A = np.eye(70)
+    with pytest.raises(RedbirdError):
+        rbb.reginvunder(A, np.ones(70), -5.0)
+
+
+@pytest.mark.parametrize("gram,tol", [("tf32x3", 2e-5), ("tf32", 5e-3)])
+def test_runrecon_matches_reference(golden, gram, tol):
+    g, m = golden("nodal_gn"), golden("nodal_cw")
+    cfg = cfg_from(m)
+    cfg["prop"] = g["prop0"].copy()
+    recon = {"prop": g["prop0"].copy()}
+    recon, resid, cfg, upd, J, det, phi = rbb.run(cfg, recon, g["detphi0"], m["sd"], maxiter=2, lambda_=0.05,
+                                                  report=False, gram=gram)
+    np.testing.assert_allclose(resid, g["resid"], rtol=1e-5)
+    for k, key in enumerate(("dmu0", "dmu1")):
+        ref = g[key]
+        err = np.abs(upd[k]["mua"] - ref).max() / np.abs(ref).max()
+        assert err < tol, (key, err)
+    err = np.abs(recon["prop"][:, 0] - g["prop_out"][:, 0]).max() / np.abs(g["prop_out"][:, 0]).max()
+    assert err < tol * 0.1
+    jref = g["jn"]
+    assert np.linalg.norm(J["mua"] - jref) / np.linalg.norm(jref) < 1e-5
+
+
+def test_runrecon_residual_decreases_fd_mua_and_d(golden):
+    """Frequency domain, exact node-based Jacobians for mua and D: the
+    residual drops over the iterations (test_integration.py:292-311)."""
+    m = golden("nodal_fd")
+    cfg = cfg_from(m)
+    truth = cfg["prop"].copy()
+    nn = truth.shape[0]
+    bump = np.linalg.norm(cfg["node"] - np.array([20.0, 20.0, 6.0]), axis=1) < 8
+    truth[bump, 0] *= 1.5
+    cfg_t = dict(cfg)
+    cfg_t.pop("_b200", None)
+    cfg_t["prop"] = truth
+    det0, _ = rbb.run(cfg_t)
+    recon = {"prop": cfg["prop"].copy()}
+    recon, resid, cfg, upd, J, det, phi = rbb.run(cfg, recon, det0, m["sd"], maxiter=4, lambda_=0.01, report=False,
+                                                  param="mua+D", lambda_rule="maxdiag")
+    assert resid[-1] < 0.5 * resid[0], resid
+    assert "dcoeff" in upd[0] and upd[0]["mua"].shape == (nn,)
