@@ -29,9 +29,13 @@ constexpr int kGStages = 4;
 constexpr int kGABytes = kGM * kGK * 4;  // 16 KB
 constexpr int kGBBytes = kGN * kGK * 4;  // 32 KB
 constexpr int kGStageBytes = kGABytes + kGBBytes;
-constexpr int kGSmem = kGStages * kGStageBytes + 1024 + 256;
+constexpr int kGSmem = kGStages * kGStageBytes + 1024 + 256;  // ring + alignment + barriers
 constexpr int kGThreads = 192;
-constexpr uint32_t kGTmemCols = 256;
+constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators
+// K-blocks per accumulation chunk: the tensor cores' FP32 accumulator is
+// drained into the FP64 output every kGChunk * 32 K-elements, so that its
+// rounding never builds up over the (up to ~10^6 long) K dimension
+constexpr int kGChunk = 128;
 constexpr long long kGWaitLimit = 1LL << 24;  // polls before a wait gives up (seconds)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -113,8 +117,9 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kGStages * kGStageBytes);
   uint64_t* empty = full + kGStages;
-  uint64_t* accf = empty + kGStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* tfull = empty + kGStages;  // [2] accumulator ready for the epilogue
+  uint64_t* tempty = tfull + 2;        // [2] accumulator drained by the epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
 
   // tile (bi, bj): walk the tile columns until this block's index falls inside
   const int64_t nbi = (M + kGM - 1) / kGM, nbj = (M + kGN - 1) / kGN;
@@ -130,7 +135,10 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(accf), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&tfull[b]), 1);
+      mbar_init(smem_u32(&tempty[b]), 4 * 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -165,34 +173,42 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      bool ok = true;
-      for (int kb = 0; kb < nk && ok; ++kb) {
+      for (int kb = 0; kb < nk; ++kb) {
         const int s = kb % kGStages;
-        ok = mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2);
-        if (!ok) break;
+        const int c = kb / kGChunk, acc = c & 1;
+        const bool first = (kb % kGChunk) == 0;
+        const bool last = (kb % kGChunk) == kGChunk - 1 || kb == nk - 1;
+        // reuse of an accumulator waits until the epilogue drained it
+        if (first && c >= 2 && !mbar_wait(smem_u32(&tempty[acc]), ((c >> 1) - 1) & 1, err, 4)) break;
+        if (!mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a = smem_u32(sm + s * kGStageBytes);
         const uint32_t b = a + kGABytes;
+        const uint32_t d = tmem + (uint32_t)(acc * kGN);
 #pragma unroll
         for (int k = 0; k < kGK / 8; ++k)  // kind::tf32 consumes K = 8 (32 bytes) per MMA
-          umma_tf32(tmem, umma_desc_sw128(a + 32 * k), umma_desc_sw128(b + 32 * k), (kb | k) != 0);
+          umma_tf32(d, umma_desc_sw128(a + 32 * k), umma_desc_sw128(b + 32 * k), !(first && k == 0));
         umma_commit(smem_u32(&empty[s]));
+        if (last) umma_commit(smem_u32(&tfull[acc]));
       }
-      umma_commit(smem_u32(accf));
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 = tile rows
+    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 = tile rows and adds
+    // each chunk's FP32 partial sums into the FP64 output row
     const int q = warp & 3;
     const int row = 32 * q + lane;
-    // warp-uniform outcome: tcgen05.ld below needs the whole warp
-    const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(accf), 0, err, 3));
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (got) {
-      const int64_t gi = (int64_t)i0 + row;
+    const int64_t gi = (int64_t)i0 + row;
+    const int nchunk = (nk + kGChunk - 1) / kGChunk;
+    for (int c = 0; c < nchunk; ++c) {
+      const int acc = c & 1;
+      // warp-uniform outcome: tcgen05.ld below needs the whole warp
+      const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[acc]), (c >> 1) & 1, err, 3));
+      if (!got) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
       for (int c0 = 0; c0 < kGN; c0 += 32) {
         uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kGN + c0);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
             "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -207,9 +223,14 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
           double* dst = H + gi * ldh + j0 + c0;
 #pragma unroll
           for (int u = 0; u < 32; ++u)
-            if ((int64_t)j0 + c0 + u < M) dst[u] = alpha * (double)__uint_as_float(v[u]);
+            if ((int64_t)j0 + c0 + u < M) {
+              const double x = alpha * (double)__uint_as_float(v[u]);
+              dst[u] = (c == 0) ? x : dst[u] + x;
+            }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[acc])) : "memory");
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
