@@ -278,6 +278,8 @@ def run_b200(args):
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,
     }
+    if not args.no_gn:
+        out["gn"] = run_gn_step(cfg, mesh, world, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         v, dt = cpu_sample_port(cfg, ncol=1)
         out["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": "port",
@@ -289,6 +291,168 @@ def run_b200(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def gn_truth(node):
+    """Two spherical inclusions (r = 8 mm): mua 0.025 at (35,50,20), mus 2.0 at (65,50,25)."""
+    nn = node.shape[0]
+    prop = np.column_stack([np.full(nn, 0.01), np.full(nn, 1.0), np.zeros(nn), np.full(nn, 1.37)])
+    prop[np.linalg.norm(node - [35.0, 50.0, 20.0], axis=1) < 8.0, 0] = 0.025
+    prop[np.linalg.norm(node - [65.0, 50.0, 25.0], axis=1) < 8.0, 1] = 2.0
+    return prop
+
+
+def run_gn_step(cfg, mesh, world, args):
+    """One Gauss-Newton iteration of the 3M-tet frequency-domain problem
+    (64 x 64 complex data -> 8192 real rows, node-wise mua and D -> 1,040,502
+    columns): forward (mixed COCG) -> exact adjoint Jacobian rows (FP32) ->
+    Frobenius scaling -> J J^T on the tensor cores (TF32) -> FP64 Cholesky ->
+    J^T y.  Beside it the plain FP64 form on the same GPU: FP64 COCG,
+    FP64 Jacobian, FP64 J J^T (cuBLAS DGEMM through torch, the library
+    baseline), the same FP64 Cholesky."""
+    import torch
+
+    from redbirdpy_b200 import engine
+    from redbirdpy_b200.forward import forward_device
+
+    gcfg = dict(cfg)
+    gcfg["omega"] = 2 * np.pi * 1e8
+    gcfg["prop"] = gn_truth(cfg["node"])
+    gcfg.pop("seg", None)
+    det_t, _, _, _, _ = forward_device(gcfg)
+    rng = np.random.default_rng(1)
+    d = det_t.cpu().numpy().ravel()
+    data = d * (1 + 0.01 * rng.standard_normal(d.shape)) * np.exp(1j * np.deg2rad(0.5) * rng.standard_normal(d.shape))
+    bg = gn_truth(cfg["node"])
+    bg[:, 0], bg[:, 1] = 0.01, 1.0
+    gcfg["prop"] = bg
+    sd = np.column_stack([np.meshgrid(np.arange(64), 64 + np.arange(64))[0].ravel(),
+                          np.meshgrid(np.arange(64), 64 + np.arange(64))[1].ravel(), np.ones(4096)])
+    stages = {}
+
+    def timed_stage(name, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        stages[name] = stages.get(name, 0.0) + e0.elapsed_time(e1)
+        return r
+
+    def step_mixed():
+        det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg))
+        J, K = timed_stage("jacobian", lambda: engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact"))
+        y = det.cpu().numpy().ravel()
+        mis = data - y
+        mis = np.concatenate([mis.real, mis.imag])
+        s2 = timed_stage("sumsq", lambda: 1.0 / float(engine.sumsq(J, K).item()))
+        H, _ = timed_stage("gram_tf32", lambda: engine.gram(J, K, s2, "tf32"))
+        lam = 0.05 * float(H.diagonal().max().item())
+        M = J.shape[0]
+        di = torch.empty(M, dtype=torch.float64, device=J.device)
+
+        def chol():
+            engine.call("rb_reginv_prepare", engine.ptr(H), M, M, lam, engine.ptr(di), engine.stream())
+            wb = engine._lib.lib().rb_cholesky_work_bytes()
+            work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+            engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), wb, engine.stream())
+
+        timed_stage("cholesky", chol)
+
+        def solve_apply():
+            r = torch.as_tensor(mis, device=J.device)
+            t = torch.empty(M, dtype=torch.float64, device=J.device)
+            engine.call("rb_vec_mul", engine.ptr(di), engine.ptr(r), engine.ptr(t), M, engine.stream())
+            engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.stream())
+            yv = torch.empty(M, dtype=torch.float64, device=J.device)
+            engine.call("rb_vec_mul", engine.ptr(di), engine.ptr(t), engine.ptr(yv), M, engine.stream())
+            out = torch.empty(K, dtype=torch.float64, device=J.device)
+            engine.call("rb_gemv_t", engine.ptr(J), M, K, J.shape[1], engine.ptr(yv), s2, 0.0, engine.ptr(out),
+                        engine.stream())
+            return out.cpu().numpy()
+
+        dmu = timed_stage("solve_jty", solve_apply)
+        del J, H
+        return dmu
+
+    # warm-up, then timed steps (device time, CUDA events around each stage)
+    step_mixed()
+    torch.cuda.synchronize()
+    stages.clear()
+    ks = max(1, min(args.steps, 2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(ks):
+        dmu_mixed = step_mixed()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
+    mixed_stages = {k: round(v / ks, 2) for k, v in stages.items()}
+
+    # plain FP64 form
+    def step_fp64():
+        det, phi, _, _, _ = forward_device(gcfg, precision="fp64")
+        cols, det0, ndet, psrc, pdet, _, _ = engine.pair_map(sd)
+        nn = mesh.nn
+        K = 2 * nn
+        M = 2 * len(psrc)
+        J = torch.zeros((M, K), dtype=torch.float64, device=phi.device)
+        colsd, ps, pd = engine._i32(cols, phi.device), engine._i32(psrc, phi.device), engine._i32(pdet, phi.device)
+        for p, w in enumerate((engine._lib.RB_JAC_MUA_NODAL, engine._lib.RB_JAC_D)):
+            engine.call("rb_jac", engine.ctypes.byref(mesh.struct), w, engine.ptr(phi), engine._lib.RB_C128,
+                        phi.shape[1], engine.ptr(colsd), len(cols), det0, ndet, engine.ptr(ps), engine.ptr(pd),
+                        len(psrc), engine.ptr(J[:, p * nn:]), K, engine._lib.RB_JAC_SPLIT_F64, mesh.rmax, mesh.emax,
+                        engine.ptr(mesh.evol), engine.ptr(mesh.ddd if p else None), engine.stream())
+        y = det.cpu().numpy().ravel()
+        mis = data - y
+        mis = np.concatenate([mis.real, mis.imag])
+        s2 = 1.0 / float(torch.linalg.vector_norm(J).item()) ** 2
+        H = torch.matmul(J, J.T) * s2
+        lam = 0.05 * float(H.diagonal().max().item())
+        di = torch.empty(M, dtype=torch.float64, device=J.device)
+        engine.call("rb_reginv_prepare", engine.ptr(H), M, M, lam, engine.ptr(di), engine.stream())
+        wb = engine._lib.lib().rb_cholesky_work_bytes()
+        work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+        engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), wb, engine.stream())
+        t = di * torch.as_tensor(mis, device=J.device)
+        engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.stream())
+        dmu = torch.mv(J.T, di * t) * s2
+        return dmu.cpu().numpy()
+
+    ms64 = None
+    err = None
+    if not args.no_fp64_gn:
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        dmu64 = step_fp64()
+        f1.record()
+        torch.cuda.synchronize()
+        ms64 = max_over_ranks(f0.elapsed_time(f1), world)
+        err = float(np.linalg.norm(dmu_mixed - dmu64) / np.linalg.norm(dmu64))
+    M, K = 8192, 2 * mesh.nn
+    nbi, nbj = M // 128, M // 256
+    tiles = sum(min(nbi, (bj * 256 + 255) // 128 + 1) for bj in range(nbj))
+    gram_flop = tiles * 128 * 256 * K * 2
+    gram_ms = mixed_stages.get("gram_tf32")
+    tflops = gram_flop / (gram_ms * 1e-3) / 1e12 if gram_ms else None
+    pk = None
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        pk = json.load(open(p)).get("bf16_tflops")
+    return {
+        "workload": "3M tets, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, mua+D nodal (K=1040502)",
+        "iters_per_s": round(1e3 / ms, 4) * world, "ms_per_iter": round(ms, 1), "breakdown_ms": mixed_stages,
+        "fp64_iters_per_s": round(1e3 / ms64, 4) * world if ms64 else None,
+        "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,
+        "speedup_vs_fp64": round(ms64 / ms, 3) if ms64 else None,
+        "dmu_rel_err_vs_fp64": err,
+        "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel (tcgen05 kind::tf32, 128x256 tiles)",
+                          "achieved": round(tflops, 1) if tflops else None, "unit": "TFLOP/s",
+                          "algorithmic_flop": gram_flop, "peak_bf16_measured": pk,
+                          "frac_of_bf16_measured": round(tflops / pk, 4) if (tflops and pk) else None,
+                          "note": "TF32 dense peak is half the BF16 one"},
+    }
 
 
 def _ref_worker(args):
@@ -360,6 +524,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration measurement")
+    ap.add_argument("--no-fp64-gn", action="store_true", help="skip the plain-FP64 GN comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
