@@ -284,13 +284,15 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
   int* err = reinterpret_cast<int*>(work);
   RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
   const int tthreads = 64;
+  const int trsm_smem = (int)(kNB * tthreads * sizeof(double));  // + 33 KB static: opt in above 48 KB
+  RB_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem));
   for (int64_t j0 = 0; j0 < M; j0 += kNB) {
     const int nb = (int)std::min<int64_t>(kNB, M - j0);
     potrf_diag_kernel<<<1, 256, 0, st>>>(H, ldh, j0, nb, err);
     RB_LAUNCH_CHECK();
     const int64_t rest = M - j0 - nb;
     if (rest <= 0) break;
-    trsm_panel_kernel<<<(unsigned)ceil_div(rest, tthreads), tthreads, kNB * tthreads * sizeof(double), st>>>(
+    trsm_panel_kernel<<<(unsigned)ceil_div(rest, tthreads), tthreads, trsm_smem, st>>>(
         H, ldh, M, j0, nb);
     RB_LAUNCH_CHECK();
     const int64_t T = ceil_div(rest, kNB);

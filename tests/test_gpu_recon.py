@@ -73,10 +73,29 @@ def test_matreform_matches_reference(golden):
         rbb.matreform(g["Jc"], g["y0"], g["y1"], "nope")
 
 
+@pytest.mark.parametrize("M", [5, 64, 65, 300, 1030])
+def test_cholesky_and_solve(M):
+    import ctypes
+
+    rng = np.random.default_rng(M)
+    B = rng.standard_normal((M, M + 7))
+    A = B @ B.T + M * np.eye(M)
+    b = rng.standard_normal(M)
+    H = torch.as_tensor(A, device="cuda")
+    work = torch.empty(engine._lib.lib().rb_cholesky_work_bytes(), dtype=torch.uint8, device="cuda")
+    engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), work.numel(), engine.stream())
+    L = np.tril(H.cpu().numpy())
+    np.testing.assert_allclose(L, np.linalg.cholesky(A), rtol=1e-10, atol=1e-12 * np.abs(L).max())
+    x = torch.as_tensor(b.copy(), device="cuda")
+    engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.stream())
+    np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-12)
+
+
 def test_cholesky_rejects_indefinite():
     A = np.eye(70)
-    with pytest.raises(RedbirdError):
+    with pytest.raises(RedbirdError) as e:
         rbb.reginvunder(A, np.ones(70), -5.0)
+    assert e.value.code == engine._lib.RB_ENOTSPD
 
 
 @pytest.mark.parametrize("gram,tol", [("tf32x3", 2e-4), ("tf32", 1e-2)])
