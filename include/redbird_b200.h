@@ -222,7 +222,11 @@ int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs,
  * Column map: the pairs read nc phi columns cols[0..nc); the ndet detector
  * columns are the slots det0..det0+ndet-1.  Pair k uses source slot
  * pair_src[k] (0..nc-1) and detector pair_det[k] (0..ndet-1).  J is nsd rows
- * of leading dimension ldj >= nn (row k at J + k*ldj).  rmax / emax: the
+ * of leading dimension ldj >= nn (row k at J + k*ldj).  Passing nsd as the
+ * negative of nsrc*ndet declares that the pairs are every (source slot,
+ * detector) combination in detector-major order, k = d*nsrc + s, with nsrc
+ * = det0 and both counts multiples of 4 (sdmap's layout); this selects a
+ * register-blocked path.  rmax / emax: the
  * largest CSR row length and the largest number of tets at one node.
  * phi_kind / out_kind: any real kind with a real kind, complex with complex;
  * out RB_F32/RB_C64 computes in FP32.  evol: ne tet volumes; ddd: the ne x 10

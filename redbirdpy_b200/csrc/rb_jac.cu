@@ -59,6 +59,7 @@ struct JacArgs {
   const int32_t* pdet;  // nsd: 0..ndet-1 index of the detector
   int64_t nsd, ld, ldj;
   int32_t rmax, emax, what;
+  int32_t grid;  // pairs are all (source slot, detector) combinations, detector-major
 };
 
 // smem layout (bytes), TN nodes:
@@ -77,7 +78,7 @@ __host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, i
   return (s + 15) / 16 * 16;
 }
 
-template <typename C, typename In, int TN, bool SPLIT>
+template <typename C, typename In, int TN, bool SPLIT, bool GRID>
 __global__ void __launch_bounds__(kJacThreads)
 jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   typedef typename JacT<C>::real R;
@@ -178,7 +179,54 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     sC[i] = s;
   }
   __syncthreads();
-  // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]; t fastest -> row segments
+  // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]
+  if constexpr (GRID) {
+    // all (source, detector) combinations, k = d * nsrc + s (sdmap's
+    // detector-major order): a thread takes 4 sources x 4 detectors of one
+    // node, so each staged value read from shared memory feeds 4 products
+    const int nsu = a.det0, nsb = nsu / 4, ndb = nd / 4;
+    const int items = nsb * ndb * TN;
+    for (int i = tid; i < items; i += kJacThreads) {
+      const int t = i % TN, pb = i / TN;
+      const int sb = pb % nsb, db = pb / nsb;
+      const int64_t n = n0 + t;
+      if (n >= a.nn) continue;
+      C acc[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = s_zero(C());
+      for (int ia = 0; ia < srn[t]; ++ia) {
+        const C* P = sphi + ((size_t)t * rmax + ia) * nc + sb * 4;
+        const C* Cn = sC + ((size_t)t * rmax + ia) * nd + db * 4;
+        C pv[4], cv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          pv[u] = P[u];
+          cv[u] = Cn[u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = s_fma(pv[u], cv[v], acc[u][v]);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t k = (int64_t)(db * 4 + v) * nsu + sb * 4 + u;
+          if constexpr (SPLIT) {
+            R* Jr = reinterpret_cast<R*>(Jout);
+            Jr[k * a.ldj + n] = acc[u][v].x;
+            Jr[(a.nsd + k) * a.ldj + n] = acc[u][v].y;
+          } else {
+            reinterpret_cast<C*>(Jout)[k * a.ldj + n] = acc[u][v];
+          }
+        }
+    }
+    return;
+  }
+  // general pair list: t fastest -> row segments
   const int64_t total = a.nsd * TN;
   for (int64_t i = tid; i < total; i += kJacThreads) {
     const int t = (int)(i % TN);
@@ -228,8 +276,8 @@ __global__ void jac_elem_kernel(const double* __restrict__ evol, const int32_t* 
   }
 }
 
-template <typename C, typename In, bool SPLIT = false>
-static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
+template <typename C, typename In, bool SPLIT, bool GRID>
+static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   int TN = 8;
   const size_t budget = 110 * 1024;
   while (TN > 1 && jac_smem<C>(TN, a.rmax, a.nc, a.ndet, a.emax) > budget) TN >>= 1;
@@ -238,9 +286,9 @@ static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t s
   const unsigned g = (unsigned)ceil_div(a.nn, TN);
 #define RB_JL(TN_)                                                                                     \
   do {                                                                                                 \
-    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)sm));                                                        \
-    jac_kernel<C, In, TN_, SPLIT><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);                      \
+    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID>,                              \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
+    jac_kernel<C, In, TN_, SPLIT, GRID><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);               \
   } while (0)
   switch (TN) {
     case 8: RB_JL(8); break;
@@ -251,6 +299,12 @@ static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t s
 #undef RB_JL
   RB_LAUNCH_CHECK();
   return RB_OK;
+}
+
+template <typename C, typename In, bool SPLIT = false>
+static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
+  if (a.grid) return launch_jac_t<C, In, SPLIT, true>(a, phi, J, st);
+  return launch_jac_t<C, In, SPLIT, false>(a, phi, J, st);
 }
 
 }  // namespace rb
@@ -266,12 +320,20 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
   if (!mesh || !phi || !cols || !pair_src || !pair_det || !J || !evol) return fail(RB_EARG, "rb_jac: null argument");
   if (what == JAC_D && !ddd) return fail(RB_EARG, "rb_jac: RB_JAC_D needs deldotdel");
   if (what < JAC_MUA_REF || what > JAC_D) return fail(RB_EARG, "rb_jac: bad quantity");
-  if (nc < 1 || ndet < 1 || det0 < 0 || det0 + ndet > nc || nsd < 0 || ldj < mesh->nn)
+  if (nc < 1 || ndet < 1 || det0 < 0 || det0 + ndet > nc || ldj < mesh->nn)
     return fail(RB_EARG, "rb_jac: bad column map");
   if (rmax < 1 || rmax > 64 || emax < 1 || emax > 256) return fail(RB_ESIZE, "rb_jac: rmax/emax out of range");
   if (nsd == 0) return RB_OK;
   JacArgs a{mesh->indptr, mesh->indices, mesh->node_eptr, mesh->node_elist, mesh->elem, evol, ddd, mesh->nn,
-            cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what};
+            cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what, 0};
+  // the blocked path needs the full detector-major grid of sources x detectors
+  // with both counts multiple of 4; the caller flags it through nsd < 0
+  if (nsd < 0) {
+    a.nsd = -nsd;
+    if (a.nsd != (int64_t)det0 * ndet || det0 % 4 || ndet % 4)
+      return fail(RB_EARG, "rb_jac: grid pair layout needs nsd = nsrc * ndet with both multiples of 4");
+    a.grid = 1;
+  }
   cudaStream_t st = as_stream(stream);
   const bool cin = (phi_kind == RB_C128 || phi_kind == RB_C64);
   if (out_kind == RB_JAC_SPLIT_F32 || out_kind == RB_JAC_SPLIT_F64) {

@@ -23,9 +23,8 @@ constexpr int kBlk = 256;
 // register budget (__launch_bounds__) and the single-wave grid size
 template <typename T> struct Bps { static constexpr int value = 4; };
 template <> struct Bps<cdouble> { static constexpr int value = 3; };
-// the SpMM gathers are latency bound: give the FP32 one more resident warps
+// SpMM: same budget (8 gathers in flight need the registers; measured best)
 template <typename T> struct BpsSpmm { static constexpr int value = Bps<T>::value; };
-template <> struct BpsSpmm<float> { static constexpr int value = 5; };
 constexpr int kGridMax = 148 * 8;       // upper bound of any grid (partials arrays)
 
 // ----------------------------------------------------------- vector access
@@ -66,17 +65,10 @@ __device__ __forceinline__ void stv(T* __restrict__ p, const T (&o)[V]) {
   }
 }
 
-// Each block owns one contiguous chunk of rows (better L1 reuse of the x rows
-// that neighbouring matrix rows share); its kBlk/L groups walk the chunk.
-template <int L> __device__ __forceinline__ int64_t row_begin(int64_t n) {
-  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  return blockIdx.x * chunk + threadIdx.x / L;
-}
-template <int L> __device__ __forceinline__ int64_t row_end(int64_t n) {
-  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t e = (int64_t)(blockIdx.x + 1) * chunk;
-  return e < n ? e : n;
-}
+// Rows are dealt to the groups of all blocks in interleaved order: at any
+// moment the whole grid works inside one window of consecutive rows, so the
+// x rows that matrix rows i and i +- (layer size) share are still in L2 when
+// the second one needs them.
 
 template <typename A> __device__ __forceinline__ A acc_zero();
 template <> __device__ __forceinline__ double acc_zero<double>() { return 0.0; }
@@ -136,7 +128,7 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   alignas(16) A acc[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) acc[j] = acc_zero<A>();
-  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     const int32_t b = indptr[row], e = indptr[row + 1];
     alignas(16) T y[V];
 #pragma unroll
@@ -153,20 +145,21 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
           my_v = val[p0 + lane];
         }
         int j = 0;
-        for (; j + 4 <= cnt; j += 4) {
-          int32_t ii[4];
-          T aa[4];
+        constexpr int U = (sizeof(T) <= 4) ? 8 : 4;  // gathers kept in flight
+        for (; j + U <= cnt; j += U) {
+          int32_t ii[U];
+          T aa[U];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < U; ++u) {
             ii[u] = __shfl_sync(0xffffffffu, my_i, j + u);
             aa[u] = shfl_s(my_v, j + u);
           }
           if (on) {
-            alignas(16) T xv[4][V];
+            alignas(16) T xv[U][V];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) ldv<T, V>(X + (int64_t)ii[u] * k + c0, xv[u]);
+            for (int u = 0; u < U; ++u) ldv<T, V>(X + (int64_t)ii[u] * k + c0, xv[u]);
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < U; ++u)
 #pragma unroll
               for (int q = 0; q < V; ++q) y[q] = s_fma(aa[u], xv[u][q], y[q]);
           }
@@ -262,7 +255,7 @@ cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __rest
   alignas(16) double arr[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
-  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     if (!on) continue;
     const T d = dinv[row];
     alignas(16) T r[V], p[V], z[V];
@@ -305,7 +298,7 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
   alignas(16) double arr[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
-  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     if (!on) continue;
     const T d = dinv[row];
     alignas(16) T x[V], r[V], p[V], q[V];
@@ -346,7 +339,7 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
     any |= act[j];
   }
   if (!any) return;
-  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     const T d = dinv[row];
     alignas(16) T r[V], p[V];
     ldv<T, V>(R + row * k + c0, r);
@@ -552,7 +545,7 @@ colnorm_kernel(int64_t n, int64_t k, const double* __restrict__ B, double* __res
   alignas(16) double acc[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) acc[j] = 0.0;
-  for (int64_t row = row_begin<L>(n), row_end_ = row_end<L>(n); row < row_end_; row += kBlk / L) {
+  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     if (!on) continue;
 #pragma unroll
     for (int j = 0; j < V; ++j) {

@@ -385,6 +385,18 @@ def pair_map(sd, nsrc_cols=None):
     return cols, len(s_u), len(d_u), psrc, pdet, act[:, 0], act[:, 1]
 
 
+def _grid_nsd(psrc, pdet, nsu, ndet):
+    """nsd as rb_jac expects it: negative when the pairs are every (source,
+    detector) combination in detector-major order (sdmap's layout) with both
+    counts multiples of 4, which selects the register-blocked kernel path."""
+    nsd = len(psrc)
+    if (nsd == nsu * ndet and nsu % 4 == 0 and ndet % 4 == 0
+            and np.array_equal(psrc, np.tile(np.arange(nsu), ndet))
+            and np.array_equal(pdet, np.repeat(np.arange(ndet), nsu))):
+        return -nsd
+    return nsd
+
+
 def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=None, evol=None, ddd=None):
     """Adjoint Jacobian rows on the device (nsd x nn), see rb_jac.
     what: 'mua' (reference semantics, forward.py:509-569), 'mua_nodal'
@@ -412,7 +424,8 @@ def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=Non
     if len(cols) > 128 or ndet > 64:
         raise ValueError("rb_jac stages at most 128 phi columns and 64 detectors per call")
     call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0, ndet,
-         ptr(ps), ptr(pd), nsd, ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev), ptr(dd), stream())
+         ptr(ps), ptr(pd), _grid_nsd(psrc, pdet, det0, ndet), ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev),
+         ptr(dd), stream())
     return J
 
 
@@ -459,8 +472,8 @@ def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference"):
             raise ValueError(f"unknown parameter {name}")
         sub = J[:, p * nn:]
         call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0,
-             ndet, ptr(ps), ptr(pd), nsd, ptr(sub), ldj, out_kind, mesh.rmax, mesh.emax, ptr(mesh.evol),
-             ptr(mesh.ddd if w == _lib.RB_JAC_D else None), stream())
+             ndet, ptr(ps), ptr(pd), _grid_nsd(psrc, pdet, det0, ndet), ptr(sub), ldj, out_kind, mesh.rmax,
+             mesh.emax, ptr(mesh.evol), ptr(mesh.ddd if w == _lib.RB_JAC_D else None), stream())
     return J, len(params) * nn
 
 
