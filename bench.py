@@ -366,10 +366,7 @@ def run_gn_step(cfg, mesh, world, args):
             engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.stream())
             yv = torch.empty(M, dtype=torch.float64, device=J.device)
             engine.call("rb_vec_mul", engine.ptr(di), engine.ptr(t), engine.ptr(yv), M, engine.stream())
-            out = torch.empty(K, dtype=torch.float64, device=J.device)
-            engine.call("rb_gemv_t", engine.ptr(J), M, K, J.shape[1], engine.ptr(yv), s2, 0.0, engine.ptr(out),
-                        engine.stream())
-            return out.cpu().numpy()
+            return engine.gemv_t(J, K, yv, s2).cpu().numpy()
 
         dmu = timed_stage("solve_jty", solve_apply)
         del J, H

@@ -268,8 +268,9 @@ int rb_reginv_prepare(double* H, int64_t M, int64_t ldh, double lambda, double* 
 size_t rb_cholesky_work_bytes(void);
 int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes, void* stream);
 int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stream);
+size_t rb_gemv_t_work_bytes(int64_t K);
 int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha,
-              double beta, double* out, void* stream);
+              double beta, double* out, void* work, size_t work_bytes, void* stream);
 size_t rb_sumsq_work_bytes(void);
 int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
              size_t work_bytes, void* stream);

@@ -84,7 +84,8 @@ _SIGS = {
     "rb_cholesky_work_bytes": (_sz, []),
     "rb_cholesky": (ctypes.c_int, [_vp, _i64, _i64, _vp, _sz, _vp]),
     "rb_chol_solve": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
-    "rb_gemv_t": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
+    "rb_gemv_t_work_bytes": (_sz, [_i64]),
+    "rb_gemv_t": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
     "rb_sumsq_work_bytes": (_sz, []),
     "rb_sumsq": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "rb_vec_mul": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp]),

@@ -189,19 +189,36 @@ __global__ void bwd_update_kernel(const double* __restrict__ L, int64_t ldh, int
   x[j] -= s;
 }
 
-// out[k] = alpha * sum_m J[m][k] y[m]   (coalesced along k)
-__global__ void gemv_t_kernel(const float* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
-                              const double* __restrict__ y, double alpha, double beta, double* __restrict__ out) {
+// out[k] = alpha * sum_m J[m][k] y[m] + beta out[k]   (coalesced along k).
+// Rows are split over gridDim.y slabs; each slab writes a partial sum and the
+// last kernel adds the slabs in fixed order (deterministic, no atomics).
+constexpr int kGemvSlabs = 16;
+
+__global__ void gemv_t_part_kernel(const float* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+                                   const double* __restrict__ y, double* __restrict__ part) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= K) return;
-  double s0 = 0.0, s1 = 0.0;
-  int64_t m = 0;
-  for (; m + 1 < M; m += 2) {
+  const int64_t rows = (M + gridDim.y - 1) / gridDim.y;
+  const int64_t m0 = blockIdx.y * rows, m1 = min(M, m0 + rows);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int64_t m = m0;
+  for (; m + 3 < m1; m += 4) {
     s0 = fma((double)J[m * ldj + k], y[m], s0);
     s1 = fma((double)J[(m + 1) * ldj + k], y[m + 1], s1);
+    s2 = fma((double)J[(m + 2) * ldj + k], y[m + 2], s2);
+    s3 = fma((double)J[(m + 3) * ldj + k], y[m + 3], s3);
   }
-  if (m < M) s0 = fma((double)J[m * ldj + k], y[m], s0);
-  out[k] = alpha * (s0 + s1) + (beta != 0.0 ? beta * out[k] : 0.0);
+  for (; m < m1; ++m) s0 = fma((double)J[m * ldj + k], y[m], s0);
+  part[blockIdx.y * K + k] = (s0 + s1) + (s2 + s3);
+}
+
+__global__ void gemv_t_sum_kernel(const double* __restrict__ part, int slabs, int64_t K, double alpha, double beta,
+                                  double* __restrict__ out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double s = 0.0;
+  for (int b = 0; b < slabs; ++b) s += part[b * K + k];
+  out[k] = alpha * s + (beta != 0.0 ? beta * out[k] : 0.0);
 }
 
 // per-block partial sums of J^2
@@ -325,26 +342,18 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
   return RB_OK;
 }
 
+size_t rb_gemv_t_work_bytes(int64_t K) { return (size_t)kGemvSlabs * K * sizeof(double) + 256; }
+
 int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
-              double* out, void* stream) {
-  if (!J || !y || !out || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_t: bad arguments");
-  gemv_t_kernel<<<(unsigned)ceil_div(K, 256), 256, 0, as_stream(stream)>>>(J, M, K, ldj, y, alpha, beta, out);
+              double* out, void* work, size_t work_bytes, void* stream) {
+  if (!J || !y || !out || !work || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_t: bad arguments");
+  if (work_bytes < rb_gemv_t_work_bytes(K)) return fail(RB_EARG, "rb_gemv_t: workspace too small");
+  cudaStream_t st = as_stream(stream);
+  const int slabs = (int)std::min<int64_t>(kGemvSlabs, M);
+  double* part = reinterpret_cast<double*>(work);
+  gemv_t_part_kernel<<<dim3((unsigned)ceil_div(K, 256), (unsigned)slabs), 256, 0, st>>>(J, M, K, ldj, y, part);
   RB_LAUNCH_CHECK();
-  return RB_OK;
-}
-
-int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream) {
-  if (!a || !b || !out || n < 0) return fail(RB_EARG, "rb_vec_mul: bad arguments");
-  if (n == 0) return RB_OK;
-  vec_mul_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, as_stream(stream)>>>(a, b, out, n);
-  RB_LAUNCH_CHECK();
-  return RB_OK;
-}
-
-int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* stream) {
-  if (!J || !lo || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_split_tf32: bad arguments");
-  dim3 g((unsigned)std::min<int64_t>(ceil_div(K, 256), 64), (unsigned)std::min<int64_t>(M, 4096));
-  split_tf32_kernel<<<g, 256, 0, as_stream(stream)>>>(J, lo, M, K, ldj);
+  gemv_t_sum_kernel<<<(unsigned)ceil_div(K, 256), 256, 0, st>>>(part, slabs, K, alpha, beta, out);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }

@@ -4,14 +4,16 @@
 // J is M x K FP32, row-major (K contiguous): the Jacobian rows of redbirdpy's
 // jac / matreform layout.  Both MMA operands are row blocks of the same J and
 // are "K-major", so one TMA tensor map (box 32 x 128, 128-byte swizzle)
-// serves A (128 rows) and B (256 rows as two boxes).  One CTA computes one
-// 128 x 256 tile of H; only tiles that touch the upper triangle are launched
-// and a second kernel mirrors the upper triangle into the lower one.
+// serves every load.  One CTA computes one 256 x 256 tile of H as two
+// M = 128, N = 256 MMAs that share the B operand (two accumulators filling
+// all 512 TMEM columns), which halves the operand bytes per FLOP against a
+// single 128 x 256 tile.  Only tiles on or above the diagonal are launched;
+// a second kernel mirrors the upper triangle into the lower one.
 //
 // Warp roles (192 threads): warp 0 = TMA producer (one lane), warp 1 = TMEM
 // allocator + MMA issuer (one lane), warps 2..5 = epilogue (each reads the
 // 32 TMEM lanes of its quarter with tcgen05.ld and writes FP64 rows of H).
-// A 4-stage shared-memory ring (48 KB per stage) is synchronised with
+// A 3-stage shared-memory ring (64 KB per stage) is synchronised with
 // mbarriers; every wait is bounded and reports a timeout through an error
 // word instead of hanging.
 #include <cuda.h>
@@ -22,16 +24,18 @@
 
 namespace rb {
 
-constexpr int kGM = 128;   // tile rows (A)
+constexpr int kGM = 256;   // tile rows (A, two MMA halves of 128)
+constexpr int kGMH = 128;  // rows per MMA / per TMA box
 constexpr int kGN = 256;   // tile columns (B rows)
 constexpr int kGK = 32;    // FP32 elements per 128-byte row of a stage
-constexpr int kGStages = 4;
-constexpr int kGABytes = kGM * kGK * 4;  // 16 KB
+constexpr int kGStages = 3;
+constexpr int kGABytes = kGM * kGK * 4;  // 32 KB
 constexpr int kGBBytes = kGN * kGK * 4;  // 32 KB
+constexpr int kGBoxBytes = kGMH * kGK * 4;  // 16 KB
 constexpr int kGStageBytes = kGABytes + kGBBytes;
 constexpr int kGSmem = kGStages * kGStageBytes + 1024 + 256;  // ring + alignment + barriers
 constexpr int kGThreads = 192;
-constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators
+constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators (rows 0-127, 128-255)
 // K-blocks per accumulation chunk: the tensor cores' FP32 accumulator is
 // drained into the FP64 output every kGChunk * 32 K-elements, so that its
 // rounding never builds up over the (up to ~10^6 long) K dimension
@@ -89,7 +93,7 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
 
 // instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 256
 constexpr uint32_t kGIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kGN >> 3) << 17) |
-                             ((uint32_t)(kGM >> 4) << 24);
+                             ((uint32_t)(kGMH >> 4) << 24);
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -117,9 +121,9 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kGStages * kGStageBytes);
   uint64_t* empty = full + kGStages;
-  uint64_t* tfull = empty + kGStages;  // [2] accumulator ready for the epilogue
-  uint64_t* tempty = tfull + 2;        // [2] accumulator drained by the epilogue
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  uint64_t* tfull = empty + kGStages;  // accumulators ready for the epilogue
+  uint64_t* tempty = tfull + 1;        // accumulators drained by the epilogue
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
 
   // tile (bi, bj): walk the tile columns until this block's index falls inside
   const int64_t nbi = (M + kGM - 1) / kGM, nbj = (M + kGN - 1) / kGN;
@@ -135,10 +139,8 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(smem_u32(&tfull[b]), 1);
-      mbar_init(smem_u32(&tempty[b]), 4 * 32);
-    }
+    mbar_init(smem_u32(tfull), 1);
+    mbar_init(smem_u32(tempty), 4 * 32);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -167,70 +169,77 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
         mbar_expect_tx(bar, kGStageBytes);
         tma_load_2d(a, ma, bar, kx, i0);
+        tma_load_2d(a + kGBoxBytes, ma, bar, kx, i0 + kGMH);
         tma_load_2d(b, mb, bar, kx, j0);
-        tma_load_2d(b + kGABytes, mb, bar, kx, j0 + kGM);
+        tma_load_2d(b + kGBoxBytes, mb, bar, kx, j0 + kGMH);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       for (int kb = 0; kb < nk; ++kb) {
         const int s = kb % kGStages;
-        const int c = kb / kGChunk, acc = c & 1;
+        const int c = kb / kGChunk;
         const bool first = (kb % kGChunk) == 0;
         const bool last = (kb % kGChunk) == kGChunk - 1 || kb == nk - 1;
-        // reuse of an accumulator waits until the epilogue drained it
-        if (first && c >= 2 && !mbar_wait(smem_u32(&tempty[acc]), ((c >> 1) - 1) & 1, err, 4)) break;
+        // a new chunk waits until the epilogue drained the previous one
+        if (first && c >= 1 && !mbar_wait(smem_u32(tempty), (c - 1) & 1, err, 4)) break;
         if (!mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a = smem_u32(sm + s * kGStageBytes);
         const uint32_t b = a + kGABytes;
-        const uint32_t d = tmem + (uint32_t)(acc * kGN);
 #pragma unroll
-        for (int k = 0; k < kGK / 8; ++k)  // kind::tf32 consumes K = 8 (32 bytes) per MMA
-          umma_tf32(d, umma_desc_sw128(a + 32 * k), umma_desc_sw128(b + 32 * k), !(first && k == 0));
+        for (int k = 0; k < kGK / 8; ++k) {  // kind::tf32 consumes K = 8 (32 bytes) per MMA
+          const uint64_t bd = umma_desc_sw128(b + 32 * k);
+          const uint32_t acc = !(first && k == 0);
+          umma_tf32(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
+          umma_tf32(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+        }
         umma_commit(smem_u32(&empty[s]));
-        if (last) umma_commit(smem_u32(&tfull[acc]));
+        if (last) umma_commit(smem_u32(tfull));
       }
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 = tile rows and adds
-    // each chunk's FP32 partial sums into the FP64 output row
+    // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 of both accumulators
+    // (tile rows r and r + 128) and adds each chunk's FP32 partial sums into
+    // the FP64 output rows
     const int q = warp & 3;
     const int row = 32 * q + lane;
-    const int64_t gi = (int64_t)i0 + row;
     const int nchunk = (nk + kGChunk - 1) / kGChunk;
     for (int c = 0; c < nchunk; ++c) {
-      const int acc = c & 1;
       // warp-uniform outcome: tcgen05.ld below needs the whole warp
-      const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[acc]), (c >> 1) & 1, err, 3));
+      const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(tfull), c & 1, err, 3));
       if (!got) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-      for (int c0 = 0; c0 < kGN; c0 += 32) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kGN + c0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (gi < M) {
-          double* dst = H + gi * ldh + j0 + c0;
+      for (int h = 0; h < 2; ++h) {
+        const int64_t gi = (int64_t)i0 + h * kGMH + row;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kGN; c0 += 32) {
+          uint32_t v[32];
+          const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * kGN + c0);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (gi < M) {
+            double* dst = H + gi * ldh + j0 + c0;
 #pragma unroll
-          for (int u = 0; u < 32; ++u)
-            if ((int64_t)j0 + c0 + u < M) {
-              const double x = alpha * (double)__uint_as_float(v[u]);
-              dst[u] = (c == 0) ? x : dst[u] + x;
-            }
+            for (int u = 0; u < 32; ++u)
+              if ((int64_t)j0 + c0 + u < M) {
+                const double x = alpha * (double)__uint_as_float(v[u]);
+                dst[u] = (c == 0) ? x : dst[u] + x;
+              }
+          }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[acc])) : "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(tempty)) : "memory");
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -278,7 +287,7 @@ static int make_map(CUtensorMap* map, const float* J, int64_t M, int64_t K, int6
   if (!enc) return fail(RB_ECUDA, "rb_gram: cuTensorMapEncodeTiled unavailable");
   cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)M};
   cuuint64_t gstride[1] = {(cuuint64_t)ldj * sizeof(float)};
-  cuuint32_t box[2] = {(cuuint32_t)kGK, (cuuint32_t)kGM};
+  cuuint32_t box[2] = {(cuuint32_t)kGK, (cuuint32_t)kGMH};
   cuuint32_t estride[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(J), gdim, gstride, box, estride,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

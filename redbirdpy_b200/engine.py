@@ -523,8 +523,19 @@ def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None)
     call("rb_chol_solve", ptr(H), M, M, ptr(t), stream())
     y = torch.empty(M, dtype=torch.float64, device=dev)
     call("rb_vec_mul", ptr(di), ptr(t), ptr(y), M, stream())
-    out = torch.empty(K, dtype=torch.float64, device=dev)
-    call("rb_gemv_t", ptr(J), M, K, ldj, ptr(y), float(alpha), 0.0, ptr(out), stream())
+    return gemv_t(J, K, y, alpha, lo=lo)
+
+
+def gemv_t(J, K, y, alpha=1.0, beta=0.0, out=None, lo=None):
+    """out = alpha J^T y + beta out on the device (J FP32 rows, y FP64); with
+    ``lo`` the split remainder of J is added as well."""
+    M, ldj = J.shape
+    dev = J.device
+    if out is None:
+        out = torch.empty(K, dtype=torch.float64, device=dev)
+    wb = _lib.lib().rb_gemv_t_work_bytes(K)
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    call("rb_gemv_t", ptr(J), M, K, ldj, ptr(y), float(alpha), float(beta), ptr(out), ptr(work), wb, stream())
     if lo is not None:  # J = hi + lo
-        call("rb_gemv_t", ptr(lo), M, K, ldj, ptr(y), float(alpha), 1.0, ptr(out), stream())
+        call("rb_gemv_t", ptr(lo), M, K, ldj, ptr(y), float(alpha), 1.0, ptr(out), ptr(work), wb, stream())
     return out

@@ -105,9 +105,7 @@ def reginvover(Amat, rhs, lambda_, LTL=None, blocks=None, precision="tf32x3", **
     # J^T r through the same GEMV kernel, then the Gram of J^T
     Jr, Kr = _device_rows(A)
     r = torch.as_tensor(np.ascontiguousarray(np.ravel(rhs), dtype=np.float64), device=Jr.device)
-    proj = torch.empty(Kr, dtype=torch.float64, device=Jr.device)
-    engine.call("rb_gemv_t", engine.ptr(Jr), Jr.shape[0], Kr, Jr.shape[1], engine.ptr(r), 1.0, 0.0,
-                engine.ptr(proj), engine.stream())
+    proj = engine.gemv_t(Jr, Kr, r)
     JT, K = _device_rows(A.T)
     M = JT.shape[0]
     H, lo = engine.gram(JT, K, 1.0, precision)
