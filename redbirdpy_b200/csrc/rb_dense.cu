@@ -358,6 +358,22 @@ int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y
   return RB_OK;
 }
 
+int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream) {
+  if (!a || !b || !out || n < 0) return fail(RB_EARG, "rb_vec_mul: bad arguments");
+  if (n == 0) return RB_OK;
+  vec_mul_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, as_stream(stream)>>>(a, b, out, n);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* stream) {
+  if (!J || !lo || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_split_tf32: bad arguments");
+  dim3 g((unsigned)std::min<int64_t>(ceil_div(K, 256), 64), (unsigned)std::min<int64_t>(M, 4096));
+  split_tf32_kernel<<<g, 256, 0, as_stream(stream)>>>(J, lo, M, K, ldj);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
 size_t rb_sumsq_work_bytes(void) { return 148 * 8 * sizeof(double) + 256; }
 
 int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
