@@ -428,9 +428,9 @@ def run_gn_step(cfg, mesh, world, args):
         ms64 = max_over_ranks(f0.elapsed_time(f1), world)
         err = float(np.linalg.norm(dmu_mixed - dmu64) / np.linalg.norm(dmu64))
     M, K = 8192, 2 * mesh.nn
-    nbi, nbj = M // 128, M // 256
-    tiles = sum(min(nbi, (bj * 256 + 255) // 128 + 1) for bj in range(nbj))
-    gram_flop = tiles * 128 * 256 * K * 2
+    nbt = (M + 255) // 256
+    tiles = nbt * (nbt + 1) // 2  # 256 x 256 tiles on or above the diagonal
+    gram_flop = tiles * 256 * 256 * K * 2
     gram_ms = mixed_stages.get("gram_tf32")
     tflops = gram_flop / (gram_ms * 1e-3) / 1e12 if gram_ms else None
     pk = None
@@ -444,12 +444,42 @@ def run_gn_step(cfg, mesh, world, args):
         "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,
         "speedup_vs_fp64": round(ms64 / ms, 3) if ms64 else None,
         "dmu_rel_err_vs_fp64": err,
-        "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel (tcgen05 kind::tf32, 128x256 tiles)",
+        "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel (tcgen05 kind::tf32, 256x256 tiles)",
                           "achieved": round(tflops, 1) if tflops else None, "unit": "TFLOP/s",
                           "algorithmic_flop": gram_flop, "peak_bf16_measured": pk,
                           "frac_of_bf16_measured": round(tflops / pk, 4) if (tflops and pk) else None,
                           "note": "TF32 dense peak is half the BF16 one"},
     }
+
+
+def run_profile(args):
+    """A short, fixed workload for ncu captures (``--profile-run``): the
+    forward step ``--warmup + --steps`` times on the box meshed at
+    ``--spacing`` mm, then (``--with-gn``) one mixed-precision GN iteration
+    of the frequency-domain problem on the same mesh."""
+    import torch
+
+    import redbirdpy_b200 as rbb
+    from redbirdpy_b200 import engine
+
+    torch.cuda.set_device(0)
+    cfg = workload_cfg(spacing=args.spacing)
+    cfg, sd = rbb.meshprep(cfg)
+    mesh = engine.mesh_of(cfg)
+    optics = engine.Optics.from_cfg(mesh, cfg)
+    for _ in range(args.warmup + args.steps):
+        opt = engine.locate_optodes(mesh, cfg)
+        B = opt.rhs(mesh)
+        mat = engine.assemble(mesh, optics)
+        X, info = engine.solve(mat, B)
+        det = engine.getdet(mesh, opt, X)
+    torch.cuda.synchronize()
+    out = {"profile_run": True, "nn": mesh.nn, "ne": mesh.ne, "iters": info["iters"]}
+    if args.with_gn:
+        class A:  # one timed GN iteration, no FP64 comparison
+            steps, no_fp64_gn = 1, True
+        out["gn"] = run_gn_step(cfg, mesh, 1, A)
+    print(json.dumps(out))
 
 
 def _ref_worker(args):
@@ -523,9 +553,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration measurement")
     ap.add_argument("--no-fp64-gn", action="store_true", help="skip the plain-FP64 GN comparison")
+    ap.add_argument("--profile-run", action="store_true", help="short fixed workload for ncu captures")
+    ap.add_argument("--spacing", type=float, default=1.0, help="mesh pitch (mm) of --profile-run")
+    ap.add_argument("--with-gn", action="store_true", help="--profile-run: add one GN iteration")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.profile_run:
+        run_profile(args)
     else:
         run_b200(args)
 
