@@ -438,7 +438,8 @@ def run_gn_step(cfg, mesh, world, args):
     if os.path.exists(p):
         pk = json.load(open(p)).get("bf16_tflops")
     return {
-        "workload": "3M tets, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, mua+D nodal (K=1040502)",
+        "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
+                    f"mua+D nodal (K={2 * mesh.nn})",
         "iters_per_s": round(1e3 / ms, 4) * world, "ms_per_iter": round(ms, 1), "breakdown_ms": mixed_stages,
         "fp64_iters_per_s": round(1e3 / ms64, 4) * world if ms64 else None,
         "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,
