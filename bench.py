@@ -118,7 +118,8 @@ def max_over_ranks(x, world):
 
     if world == 1:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -491,7 +492,8 @@ def _ref_worker(args):
 
     z = np.load(path)
     A = sparse.csr_matrix((z["data"], z["indices"], z["indptr"]))
-    b = z["rhs"][:, col]
+    R = sparse.csc_matrix((z["rdata"], z["rindices"], z["rindptr"]), shape=tuple(z["rshape"]))
+    b = R[:, col].toarray().ravel()
     t0 = time.perf_counter()
     x, info = cg(A, b, rtol=tol, maxiter=maxiter)
     return time.perf_counter() - t0, info
@@ -517,7 +519,9 @@ def run_reference(args):
     rhs, _, _, _ = fo.femrhs(ocfg)
     ncore = os.cpu_count() or 1
     tmp = os.path.join(tempfile.gettempdir(), f"rb_ref_{os.getpid()}.npz")
-    np.savez(tmp, data=A.data, indices=A.indices, indptr=A.indptr, rhs=rhs.toarray())
+    rc = rhs.tocsc()
+    np.savez(tmp, data=A.data, indices=A.indices, indptr=A.indptr, rdata=rc.data, rindices=rc.indices,
+             rindptr=rc.indptr, rshape=np.array(rc.shape))
     ctx = mp.get_context("spawn")
     times = []
     with ctx.Pool(ncore) as pool:

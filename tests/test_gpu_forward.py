@@ -204,3 +204,24 @@ def test_large_pattern_vs_scipy():
     assert A.nnz == 972876
     assert np.array_equal(A.indptr, R.indptr) and np.array_equal(A.indices, R.indices)
     assert np.abs(A.data - R.data).max() / np.abs(R.data).max() <= 1e-12
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_femsolve_breakdown_is_a_flag_not_a_hang(cplx):
+    """(p, A p) = 0 on the first step (indefinite / complex-symmetric
+    D^-1 A): the column stops with the breakdown flag 2, like the reference's
+    non-zero iterative-solver flags, and the call returns."""
+    from scipy import sparse
+
+    dt = complex if cplx else float
+    A = sparse.diags(np.array([1.0, -1.0], dtype=dt)).tocsr()
+    x, flag = rbb.femsolve(A, np.array([1.0, 1.0]), maxiter=50)
+    assert flag == 2
+
+
+def test_femsolve_nan_matrix_flags_breakdown():
+    from scipy import sparse
+
+    A = sparse.diags(np.array([2.0, np.nan, 3.0])).tocsr()
+    x, flag = rbb.femsolve(A, np.ones(3), maxiter=50)
+    assert flag == 2
