@@ -11,6 +11,7 @@
 // device; the host only polls a counter of active columns every few
 // iterations.  Columns are frozen individually when they converge.
 #include <algorithm>
+#include <cmath>
 #include <type_traits>
 #include <vector>
 
@@ -308,8 +309,10 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
     ldv<T, V>(Q + row * k + c0, q);
 #pragma unroll
     for (int j = 0; j < V; ++j) {
-      x[j] = s_fma(al[j], p[j], x[j]);
-      r[j] = s_sub(r[j], s_mul(al[j], q[j]));
+      if (act[j]) {  // frozen columns keep x and r untouched (p may hold NaN after a breakdown)
+        x[j] = s_fma(al[j], p[j], x[j]);
+        r[j] = s_sub(r[j], s_mul(al[j], q[j]));
+      }
       const T z = s_mul(d, r[j]);
       arz[j] = acc_fma(r[j], z, arz[j]);
       arr[j] += s_abs2(r[j]);
@@ -456,7 +459,7 @@ struct OuterState {
   double prev;
   double scale;
   int32_t active;
-  int32_t done;  // 1 converged, 2 stagnated
+  int32_t done;  // 1 converged, 2 stagnated, 3 non-finite residual
 };
 
 __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterState* os) {
@@ -484,7 +487,10 @@ __global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterSta
   const double rel = sqrt(s) / o.bnorm;
   o.prev = o.relres;
   o.relres = rel;
-  if (!(rel > tol)) {
+  if (!isfinite(rel)) {  // NaN/Inf in the matrix, the data or a correction
+    o.active = 0;
+    o.done = 3;
+  } else if (!(rel > tol)) {
     o.active = 0;
     o.done = 1;
   } else if (rel > stall * o.prev) {
@@ -808,9 +814,9 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   double worst = 0.0;
   int flag = 0;
   for (int64_t c = 0; c < k; ++c) {
-    worst = std::max(worst, hos[c].relres);
+    worst = std::isfinite(hos[c].relres) ? std::max(worst, hos[c].relres) : hos[c].relres;
     if (hos[c].done == 0 || (hos[c].done == 2 && hos[c].relres > 1e-10)) flag = std::max(flag, 1);
-    if (hcs[c].status == 2 && hos[c].relres > 1e-10) flag = 2;
+    if ((hcs[c].status == 2 && hos[c].relres > 1e-10) || hos[c].done == 3) flag = 2;
   }
   if (flag == 1 && sweep_flag == 0 && worst <= o.tol) flag = 0;
   info.iters += total_iters;
