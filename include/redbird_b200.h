@@ -193,7 +193,7 @@ typedef struct rb_solve_info {
  * unconjugated bilinear form).  B is nn x nrhs real FP64; X is nn x nrhs of
  * the matrix's FP64 kind.  All-zero columns of B give exactly zero columns
  * (the reference skips them, solver.py:568-581). */
-size_t rb_femsolve_work_bytes(int64_t n, int64_t nrhs, int32_t is_complex, int32_t precision);
+size_t rb_femsolve_work_bytes(int64_t n, int64_t nnz, int64_t nrhs, int32_t is_complex, int32_t precision);
 int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs,
                 const rb_solve_opts* opts, rb_solve_info* info /* host */, void* work,
                 size_t work_bytes, void* stream);

@@ -353,7 +353,7 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
         kb = min(128, k - c0)
         Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
         Xb = torch.empty((n, kb), dtype=xdt, device=B.device) if (c0 or kb != k) else X
-        wb = _lib.lib().rb_femsolve_work_bytes(n, kb, int(mat.is_complex), prec)
+        wb = _lib.lib().rb_femsolve_work_bytes(n, mat.struct.nnz, kb, int(mat.is_complex), prec)
         work = torch.empty(wb, dtype=torch.uint8, device=B.device)
         inf = _lib.RbSolveInfo()
         call("rb_femsolve", ctypes.byref(mat.struct), ptr(Bb), ptr(Xb), kb, ctypes.byref(opts), ctypes.byref(inf),

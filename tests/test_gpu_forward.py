@@ -225,3 +225,42 @@ def test_femsolve_nan_matrix_flags_breakdown():
     A = sparse.diags(np.array([2.0, np.nan, 3.0])).tocsr()
     x, flag = rbb.femsolve(A, np.ones(3), maxiter=50)
     assert flag == 2
+
+
+def _spd_dense_row(n, seed):
+    """SPD matrix whose row/column 7 is full (a row group of more than 256
+    values), n not a multiple of the 8-row groups."""
+    from scipy import sparse
+
+    rng = np.random.default_rng(seed)
+    M = sparse.random(n, n, density=0.03, random_state=rng).tolil()
+    M[7, :] = rng.uniform(0.1, 0.2, n)
+    M = M.tocsr()
+    return (M @ M.T + 20 * sparse.eye(n)).tocsr()
+
+
+@pytest.mark.parametrize("k", [32, 64, 128])
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_femsolve_row_group_spmm(golden, k, precision):
+    """32, 64 and 128 columns: the FP64 solves take the row-group SpMM (bulk
+    copies of each neighbour row once per 4-row group), the mixed ones the
+    per-row SpMM (padded gather batches at 128 columns).  FEM matrices (real
+    and complex symmetric) and a ragged SPD matrix with a dense row (a group of
+    more than 256 values), against SuperLU."""
+    from scipy import sparse
+    from scipy.sparse.linalg import splu
+
+    rng = np.random.default_rng(k)
+    mats = []
+    for case in ("c1_cw", "nodal_fd"):
+        g = golden(case)
+        mats.append(sparse.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"])))
+    mats.append(_spd_dense_row(301, k))
+    for A in mats:
+        b = rng.standard_normal((A.shape[0], k))
+        b[:, 3] = 0.0
+        x, flag = rbb.femsolve(A, b, precision=precision)
+        ref = splu(A.tocsc()).solve(b.astype(A.dtype))
+        assert flag == 0
+        assert np.all(x[:, 3] == 0)
+        assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-11
