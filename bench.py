@@ -237,8 +237,10 @@ def run_b200(args):
 
     # end to end through the public API (host arrays in, numpy out)
     host_cfg = cfg
-    for _ in range(1):
-        rbb.runforward(host_cfg)
+    # warm-up: two results held at once, the steady state of a loop that
+    # keeps the previous phi while the next call runs (fills the pinned pool)
+    warm = [rbb.runforward(host_cfg) for _ in range(2)]
+    del warm
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()

@@ -97,6 +97,14 @@ typedef struct rb_optics {
   double reff;         /* effective reflection coefficient of the boundary */
 } rb_optics;
 
+/* Per-tet mua and musp from a label table (the label branch of femlhs,
+ * redbirdpy/forward.py:244-252: prop[seg]): mua_out[e] = tab[l][0],
+ * musp_out[e] = tab[l][1] * (1 - tab[l][2]) with l = seg[e] clipped to
+ * [0, nlabel).  tab is nlabel x ncol (ncol >= 2; g is taken as 0 when
+ * ncol == 2), all on the device. */
+int rb_prop_from_labels(const int32_t* seg, int64_t ne, const double* tab, int64_t nlabel, int32_t ncol,
+                        double* mua_out, double* musp_out, void* stream);
+
 /* femlhs (redbirdpy/forward.py:90-256): A = K*D + M*mua (+ i*omega/c*n*M)
  * + Robin boundary terms, written into the fixed CSR pattern of `mesh`.
  * Like the reference it combines the precomputed deldotdel rows `ddd`

@@ -329,3 +329,28 @@ extern "C" int rb_femlhs_noalloc(const rb_mesh* mesh, const rb_optics* optics, c
              ? launch_femlhs<false, RB_PROP_NODE>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st)
              : launch_femlhs<false, RB_PROP_ELEM>(m, o, evol, ddd, dco, val64, val32, dinv64, dinv32, st);
 }
+
+namespace rb {
+// label table -> per-tet mua, musp (seg clipped like np.clip(seg, 0, nlabel - 1))
+__global__ void prop_labels_kernel(const int32_t* __restrict__ seg, int64_t ne, const double* __restrict__ tab,
+                                   int64_t nlabel, int ncol, double* __restrict__ mua, double* __restrict__ musp) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t l = seg[e];
+    l = l < 0 ? 0 : (l >= nlabel ? nlabel - 1 : l);
+    const double* t = tab + l * ncol;
+    mua[e] = t[0];
+    musp[e] = ncol >= 3 ? t[1] * (1.0 - t[2]) : t[1];
+  }
+}
+}  // namespace rb
+
+extern "C" int rb_prop_from_labels(const int32_t* seg, int64_t ne, const double* tab, int64_t nlabel, int32_t ncol,
+                                   double* mua_out, double* musp_out, void* stream) {
+  if (!seg || !tab || !mua_out || !musp_out || ne < 0 || nlabel < 1 || ncol < 2)
+    return fail(RB_EARG, "rb_prop_from_labels: bad arguments");
+  if (ne == 0) return RB_OK;
+  prop_labels_kernel<<<(unsigned)std::min<int64_t>(ceil_div(ne, 256), 148 * 16), 256, 0, as_stream(stream)>>>(
+      seg, ne, tab, nlabel, ncol, mua_out, musp_out);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}

@@ -11,6 +11,7 @@ here computes on the CPU; every numerical step is a call into
 """
 
 import ctypes
+import weakref
 
 import numpy as np
 import torch
@@ -71,6 +72,7 @@ class DeviceMesh:
         self.evol_host = evol
         self._ddd = None
         self._evol = None
+        self._labels = (None, None)
         self.struct = _lib.RbMesh(
             self.nn, self.ne, self.nf, self.nnz, self.node.data_ptr(), self.elem.data_ptr(),
             self.face.data_ptr(), self.area.data_ptr(), self.eptr.data_ptr(), self.elist.data_ptr(),
@@ -106,6 +108,13 @@ class DeviceMesh:
             else:
                 self._geometry()
         return self._evol
+
+    def labels(self, seg):
+        """Device int32 copy of a per-tet label array, cached per array."""
+        key = (id(seg), np.shape(seg))
+        if self._labels[0] != key:
+            self._labels = (key, _i32(np.asarray(seg).ravel(), self.device))
+        return self._labels[1]
 
     def deldotdel_host(self):
         return self.ddd.cpu().numpy()
@@ -156,6 +165,40 @@ def mesh_of(cfg):
     return m
 
 
+# ------------------------------------------------------------ host results
+class PinnedPool:
+    """Page-locked host buffers for large results copied off the device.  A
+    buffer is handed out again only once the numpy array made from it (and
+    every view of that array) has been released, so an array returned to the
+    caller is never overwritten.  Fresh pageable arrays cost a page fault per
+    4 KB on first touch (~2 GB/s); a reused pinned buffer takes the copy at
+    PCIe speed."""
+
+    def __init__(self, per_shape=3, min_bytes=1 << 20):
+        self.per_shape = per_shape
+        self.min_bytes = min_bytes
+        self._slots = {}
+
+    def to_numpy(self, t):
+        if t.numel() * t.element_size() < self.min_bytes:
+            return t.cpu().numpy()
+        slots = self._slots.setdefault((tuple(t.shape), t.dtype), [])
+        slot = next((s for s in slots if s[1] is None or s[1]() is None), None)
+        if slot is None:
+            if len(slots) >= self.per_shape:  # every pooled buffer is still referenced
+                return t.cpu().numpy()
+            slot = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True), None]
+            slots.append(slot)
+        slot[0].copy_(t, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+        arr = slot[0].numpy()
+        slot[1] = weakref.ref(arr)
+        return arr
+
+
+host_pool = PinnedPool()
+
+
 # ------------------------------------------------------------------ optics
 class Optics:
     """Per-node or per-tet optical properties on the device, as femlhs reads
@@ -163,15 +206,16 @@ class Optics:
 
     def __init__(self, mesh, mua, musp, nref, omega, reff):
         dev = mesh.device
-        mua = np.asarray(mua, dtype=np.float64)
+        if not isinstance(mua, torch.Tensor):
+            mua = np.asarray(mua, dtype=np.float64)
         if len(mua) == mesh.ne:
             self.kind = _lib.RB_PROP_ELEM
         elif len(mua) == mesh.nn:
             self.kind = _lib.RB_PROP_NODE
         else:
             raise ValueError("Property format not recognized")
-        self.mua = _f64(mua, dev)
-        self.musp = _f64(musp, dev)
+        self.mua = mua if isinstance(mua, torch.Tensor) else _f64(mua, dev)
+        self.musp = musp if isinstance(musp, torch.Tensor) else _f64(musp, dev)
         if np.ndim(nref) > 0 and len(nref) == len(mua):
             self.nref = _f64(nref, dev)
             self.nref_scalar = 0.0
@@ -193,10 +237,17 @@ class Optics:
             musp = props[:, 1] * (1 - props[:, 2]) if props.shape[1] >= 3 else props[:, 1]
             nref = props[:, 3] if props.shape[1] >= 4 else 1.37
         elif cfg.get("seg") is not None:
-            idx = np.clip(np.asarray(cfg["seg"]).astype(np.int32), 0, props.shape[0] - 1)
-            mua = props[idx, 0]
-            musp = props[idx, 1] * (1 - props[idx, 2]) if props.shape[1] >= 3 else props[idx, 1]
-            nref = props[idx[0], 3] if props.shape[1] >= 4 else 1.37
+            # label table expanded per tet on the device (prop[seg]); the
+            # labels themselves are uploaded once per seg array
+            seg = mesh.labels(cfg["seg"])
+            nseg = int(seg.numel())
+            tab = _f64(props[:, :3] if props.shape[1] >= 3 else props[:, :2], mesh.device)
+            mua = torch.empty(nseg, dtype=torch.float64, device=mesh.device)
+            musp = torch.empty(nseg, dtype=torch.float64, device=mesh.device)
+            call("rb_prop_from_labels", ptr(seg), nseg, ptr(tab), props.shape[0], tab.shape[1], ptr(mua), ptr(musp),
+                 stream())
+            l0 = int(np.clip(int(np.asarray(cfg["seg"]).ravel()[0]), 0, props.shape[0] - 1))
+            nref = props[l0, 3] if props.shape[1] >= 4 else 1.37
         else:
             raise ValueError("Property format not recognized")
         omega = 0.0 if mode == 2 else float(cfg.get("omega", 0) or 0)

@@ -54,7 +54,7 @@ def runforward(cfg, **kwargs):
     for md in rfcw:
         det, phi, _, _, info = forward_device(cfg, mode=md, **kwargs)
         det_out[md] = {"detphi": det.cpu().numpy()}
-        phi_out[md] = {"phi": phi.cpu().numpy()}
+        phi_out[md] = {"phi": engine.host_pool.to_numpy(phi)}
     if len(rfcw) == 1:
         return det_out[rfcw[0]]["detphi"], phi_out[rfcw[0]]["phi"]
     return det_out, phi_out

@@ -87,6 +87,21 @@ def getreff(n_in, n_out=1.0):
     return (r_phi + r_j) / (2 - r_phi + r_j)
 
 
+def _first_elem_with_node(cfg, v):
+    """Index of the first tet that has (1-based) node v, or None; cached in
+    cfg['_b200'] per elem array (a full scan of elem otherwise)."""
+    elem = cfg["elem"]
+    key = (id(elem), np.shape(elem), int(v))
+    cache = cfg.get("_b200")
+    if isinstance(cache, dict) and cache.get("first_elem_key") == key:
+        return cache["first_elem"]
+    hit = np.nonzero(np.any(elem[:, :4] == v, axis=1))[0]
+    r = int(hit[0]) if len(hit) else None
+    if isinstance(cache, dict):
+        cache["first_elem_key"], cache["first_elem"] = key, r
+    return r
+
+
 def getbulk(cfg):
     """Bulk [mua, mus, g, n] at the air interface (property.py:216-332)."""
     default = np.array([0.0, 0.0, 0.0, 1.37])
@@ -121,8 +136,8 @@ def getbulk(cfg):
         if face is not None and len(seg) == nn:
             label = seg[face[0, 0] - 1]
         elif face is not None and len(seg) == ne:
-            hit = np.nonzero(np.any(cfg["elem"][:, :4] == face[0, 0], axis=1))[0]
-            label = seg[hit[0]] if len(hit) else 0
+            hit = _first_elem_with_node(cfg, face[0, 0])
+            label = seg[hit] if hit is not None else 0
         else:
             label = seg[0]
         label = int(label)
@@ -133,9 +148,9 @@ def getbulk(cfg):
         return prop[face[0, 0] - 1] if face is not None else prop[0]
     if prop.shape[0] == ne:
         if face is not None:
-            hit = np.nonzero(np.any(cfg["elem"][:, :4] == face[0, 0], axis=1))[0]
-            if len(hit):
-                return prop[hit[0]]
+            hit = _first_elem_with_node(cfg, face[0, 0])
+            if hit is not None:
+                return prop[hit]
         return prop[0]
     return default
 

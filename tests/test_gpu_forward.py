@@ -264,3 +264,37 @@ def test_femsolve_row_group_spmm(golden, k, precision):
         assert flag == 0
         assert np.all(x[:, 3] == 0)
         assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-11
+
+
+def test_pinned_result_pool_never_overwrites_live_arrays():
+    """runforward copies phi into reused page-locked buffers: a buffer comes
+    back only after the array from it, and every view of it, is gone."""
+    pool = engine.PinnedPool(per_shape=2, min_bytes=0)
+    t = torch.arange(8, dtype=torch.float64, device="cuda")
+    a = pool.to_numpy(t)
+    b = pool.to_numpy(t + 100)
+    assert a[0] == 0 and b[0] == 100  # two live arrays, two buffers
+    c = pool.to_numpy(t + 200)  # both pooled buffers in use: a plain copy
+    assert a[0] == 0 and b[0] == 100 and c[0] == 200
+    view = b[2:]
+    del a, b
+    d = pool.to_numpy(t + 300)  # reuses a's buffer, never b's (view alive)
+    e = pool.to_numpy(t + 400)
+    assert view[0] == 102 and d[0] == 300 and e[0] == 400
+    assert not np.shares_memory(d, view) and not np.shares_memory(e, view)
+
+
+def test_label_properties_expand_on_device(golden):
+    """prop[seg] on the device (rb_prop_from_labels) gives the reference's
+    matrix for the labelled workload, including labels out of range (clipped)."""
+    g = golden("c1_cw")
+    cfg = cfg_from(g)
+    A = rbb.femlhs(cfg, g["deldotdel"])
+    assert np.abs(A.data - g["A_data"]).max() / np.abs(g["A_data"]).max() <= 1e-12
+    mesh = engine.mesh_of(cfg)
+    seg = np.array([-3, 0, 1, 7] * (mesh.ne // 4) + [1] * (mesh.ne % 4))
+    cfg2 = dict(cfg, seg=seg, prop=np.array([[0.02, 2.0, 0.5, 1.37], [0.01, 1.0, 0.0, 1.37]]))
+    o = engine.Optics.from_cfg(mesh, cfg2)
+    idx = np.clip(seg, 0, 1)
+    np.testing.assert_array_equal(o.mua.cpu().numpy(), cfg2["prop"][idx, 0])
+    np.testing.assert_array_equal(o.musp.cpu().numpy(), cfg2["prop"][idx, 1] * (1 - cfg2["prop"][idx, 2]))
