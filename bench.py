@@ -283,6 +283,10 @@ def run_b200(args):
     }
     if not args.no_gn:
         out["gn"] = run_gn_step(cfg, mesh, world, args)
+    if not args.no_adjoint:
+        out["adjoint"] = run_adjoint(world, args)
+    if not args.no_batch:
+        out["batch"] = run_batch(world, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         v, dt = cpu_sample_port(cfg, ncol=1)
         out["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": "port",
@@ -486,6 +490,170 @@ def run_profile(args):
     print(json.dumps(out))
 
 
+def _log_amp_loss(parts, targets):
+    import torch
+
+    return sum(0.5 * torch.sum((torch.log(torch.abs(p)) - torch.log(torch.abs(t))) ** 2)
+               for p, t in zip(parts, targets))
+
+
+def run_adjoint(world, args):
+    """Adjoint gradient and Jacobian rows on the 375k-tet box (51 x 51 x 26
+    nodes at 2 mm), per-node mua ~ U[0.008, 0.012], mus ~ U[0.9, 1.1]
+    (seed 0), 32 sources (8 x 4 grid) and 32 detectors (offset 5 mm) on z = 0,
+    CW.  One step = forward + autograd backward of
+    0.5 ||log|det| - log|target|||^2 (target: +10% mua) through the
+    hand-written adjoint; beside it the full FP32 Jmua and JD rows
+    (1024 x 67,626 each) and their HBM write rate."""
+    import torch
+
+    import redbirdpy_b200 as rbb
+    from redbirdpy_b200 import engine
+    from redbirdpy_b200.adjoint import DeviceModel, detector_values
+    from redbirdpy_b200.meshgen import kuhn_box
+
+    node, elem = kuhn_box([100, 100, 50], 2.0)
+    nn = node.shape[0]
+    rng = np.random.default_rng(0)
+    prop = np.column_stack([rng.uniform(0.008, 0.012, nn), rng.uniform(0.9, 1.1, nn), np.zeros(nn),
+                            np.full(nn, 1.37)])
+    src = np.column_stack([np.repeat(np.linspace(15, 85, 8), 4), np.tile(np.linspace(30, 70, 4), 8), np.zeros(32)])
+    cfg = dict(node=node, elem=elem, prop=prop, srcpos=src, srcdir=np.array([[0, 0, 1.0]]), detpos=src + [5, 5, 0],
+               detdir=np.array([[0, 0, 1.0]]), omega=0.0)
+    cfg, sd = rbb.meshprep(cfg)
+    out = {"workload": f"{elem.shape[0]} tets / {nn} nodes, 32 src x 32 det, CW, per-node mua and D"}
+    mua0 = torch.as_tensor(prop[:, 0].copy(), device="cuda")
+    d0 = torch.as_tensor(1.0 / (3.0 * (prop[:, 0] + prop[:, 1])), device="cuda")
+    grads = {}
+    for prec in ("mixed", "fp64"):
+        model = DeviceModel(cfg, precision=prec)
+        with torch.no_grad():
+            target = detector_values(model, mua0 * 1.1, d0)
+
+        def step():
+            mua = mua0.clone().requires_grad_(True)
+            dco = d0.clone().requires_grad_(True)
+            loss = _log_amp_loss([detector_values(model, mua, dco)], [target])
+            loss.backward()
+            return mua.grad, dco.grad
+
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ks = max(1, min(args.steps, 3))
+        e0.record()
+        for _ in range(ks):
+            gm, gd = step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
+        grads[prec] = (gm, gd)
+        out[f"{prec}_ms_per_gradient"] = round(ms, 2)
+    gm, gd = grads["mixed"]
+    rm, rd = grads["fp64"]
+    out["grad_rel_err_vs_fp64"] = float(max((torch.abs(gm - rm).max() / torch.abs(rm).max()).item(),
+                                            (torch.abs(gd - rd).max() / torch.abs(rd).max()).item()))
+    out["gradients_per_s"] = round(world * 1e3 / out["mixed_ms_per_gradient"], 3)
+    # full FP32 Jacobian rows (mua and D), as the GN step builds them
+    model = DeviceModel(cfg)
+    phi, _ = model.fields(mua0, d0)
+    mesh = model.mesh
+    ns = model.opt.nsrc
+    sdj = np.column_stack([np.tile(np.arange(ns), ns), ns + np.repeat(np.arange(ns), ns), np.ones(ns * ns)])
+    for _ in range(2):
+        J, K = engine.jacobian_matrix(mesh, phi, sdj, ("mua", "D"), "exact")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        J, K = engine.jacobian_matrix(mesh, phi, sdj, ("mua", "D"), "exact")
+    e1.record()
+    torch.cuda.synchronize()
+    jms = e0.elapsed_time(e1) / 3
+    jbytes = J.shape[0] * K * 4
+    peak, _ = peaks()
+    out["jacobian"] = {"rows": int(J.shape[0]), "cols": int(K), "ms": round(jms, 3),
+                       "write_gbs": round(jbytes / (jms * 1e-3) / 1e9, 1),
+                       "frac_of_hbm": round(jbytes / (jms * 1e-3) / 1e9 / peak, 4),
+                       "note": "includes the zero fill of J (torch) and both parameter launches"}
+    return out
+
+
+def run_batch(world, args):
+    """256 uneven box instances (seed 2; extents ~ U[30, 80] mm per axis,
+    spacing in {2, 3, 4} mm, per-node mua ~ U[0.005, 0.03], mus ~ U[0.5, 2],
+    4-16 top-surface sources and 4-16 detectors each, CW): forward + adjoint
+    gradient of a log-amplitude misfit (target: +10% mua) for all instances
+    as one block-diagonal system (one assembly, one mixed-precision solve,
+    one adjoint contraction), against a loop over the instances' own models
+    (timed on the first 32)."""
+    import torch
+
+    import redbirdpy_b200 as rbb
+    from redbirdpy_b200.adjoint import BatchModel, DeviceModel, detector_values
+    from redbirdpy_b200.meshgen import batch_boxes
+
+    cfgs = [rbb.meshprep(c)[0] for c in batch_boxes(256, seed=2)]
+    nn = sum(c["node"].shape[0] for c in cfgs)
+    ne = sum(c["elem"].shape[0] for c in cfgs)
+    bm = BatchModel(cfgs)
+    mua0 = torch.as_tensor(np.concatenate([c["prop"][:, 0] for c in cfgs]), device="cuda")
+    d0 = torch.as_tensor(np.concatenate([1.0 / (3.0 * (c["prop"][:, 0] + c["prop"][:, 1])) for c in cfgs]),
+                         device="cuda")
+    with torch.no_grad():
+        targets = bm.split(detector_values(bm, mua0 * 1.1, d0))
+
+    def step():
+        mua = mua0.clone().requires_grad_(True)
+        dco = d0.clone().requires_grad_(True)
+        _log_amp_loss(bm.split(detector_values(bm, mua, dco)), targets).backward()
+        return mua.grad
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ks = max(1, min(args.steps, 3))
+    e0.record()
+    for _ in range(ks):
+        g = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
+    # accuracy: detector values against the FP64 form of the same batch
+    with torch.no_grad():
+        dm = detector_values(bm, mua0, d0)
+        d64 = detector_values(BatchModel(cfgs, precision="fp64"), mua0, d0)
+    mask = torch.abs(d64) > 0
+    err = float((torch.abs(dm - d64)[mask] / torch.abs(d64)[mask]).max().item())
+    # loop over per-instance models (first 32 instances)
+    nloop = 32
+    models = [DeviceModel(c) for c in cfgs[:nloop]]
+    tl = []
+    for i, m in enumerate(models):
+        mu0 = mua0[bm.node_off[i]:bm.node_off[i + 1]]
+        dd0 = d0[bm.node_off[i]:bm.node_off[i + 1]]
+        mu = mu0.clone().requires_grad_(True)
+        dc = dd0.clone().requires_grad_(True)
+        _log_amp_loss([detector_values(m, mu, dc)], [targets[i]]).backward()  # warm-up
+    torch.cuda.synchronize()
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0.record()
+    for i, m in enumerate(models):
+        mu = mua0[bm.node_off[i]:bm.node_off[i + 1]].clone().requires_grad_(True)
+        dc = d0[bm.node_off[i]:bm.node_off[i + 1]].clone().requires_grad_(True)
+        _log_amp_loss([detector_values(m, mu, dc)], [targets[i]]).backward()
+    l1.record()
+    torch.cuda.synchronize()
+    loop_ms = l0.elapsed_time(l1) / nloop
+    return {"workload": f"256 instances, {nn} nodes / {ne} tets in total, {bm.S} source + {bm.D} detector columns",
+            "instances_per_s": round(world * 256 / (ms * 1e-3), 2), "ms_per_batch": round(ms, 2),
+            "loop_instances_per_s": round(world * 1e3 / loop_ms, 2),
+            "loop_sample": f"first {nloop} instances, one model each (same kernels, launch-bound)",
+            "speedup_vs_loop": round(loop_ms * 256 / ms, 2), "det_max_rel_err_vs_fp64": err}
+
+
 def _ref_worker(args):
     path, col, tol, maxiter = args
     import numpy as np
@@ -560,6 +728,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration measurement")
     ap.add_argument("--no-fp64-gn", action="store_true", help="skip the plain-FP64 GN comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient / Jacobian measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances measurement")
     ap.add_argument("--profile-run", action="store_true", help="short fixed workload for ncu captures")
     ap.add_argument("--spacing", type=float, default=1.0, help="mesh pitch (mm) of --profile-run")
     ap.add_argument("--with-gn", action="store_true", help="--profile-run: add one GN iteration")

@@ -255,6 +255,17 @@ int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_
                 const int32_t* src_col, const int32_t* det_col, int64_t nsd, void* je,
                 void* stream);
 
+/* Adjoint fields of the backward pass (no counterpart in the reference, which
+ * has no autograd): for the instance i that owns row r (rows
+ * [row0[i], row0[i+1]), detector rows [det0[i], det0[i+1]) of g),
+ *   lam[r][s] = sum_d phi[r][dcol0 + d] * conj(g[det0[i] + d][s]),  s < ns
+ * i.e. lambda_s = A^-1 sum_d conj(g[d, s]) b_d from the detector columns of
+ * the forward solve.  phi: nn x ld, g: ndet_total x ns, lam: nn x ns, all
+ * RB_F64 or all RB_C128 (kind).  ninst = 1 for a single mesh. */
+int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, const void* g, int64_t ns,
+                      const int64_t* row0, const int64_t* det0, int64_t ninst, int32_t kind, void* lam,
+                      void* stream);
+
 /* ------------------------------------------------------ Gauss-Newton step
  * reginvunder (redbirdpy/recon.py:429-509) on the device:
  *   H = alpha J J^T            rb_gram: tcgen05 tensor cores, TF32 inputs,

@@ -11,7 +11,8 @@ numerical work runs in hand-written CUDA kernels (``librbb200.so``, C ABI in
 
 __version__ = "0.1.0"
 
-from . import forward, solver, utility, meshgen  # noqa: F401
+from . import adjoint, forward, solver, utility, meshgen  # noqa: F401
+from .adjoint import DeviceModel, detector_values  # noqa: F401
 from .forward import *  # noqa: F401,F403
 from .solver import *  # noqa: F401,F403
 from .utility import *  # noqa: F401,F403

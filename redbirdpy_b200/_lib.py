@@ -69,6 +69,7 @@ _SIGS = {
     "rb_tsearch": (ctypes.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "rb_point_rhs": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),
     "rb_prop_from_labels": (ctypes.c_int, [_vp, _i64, _vp, _i64, _i32, _vp, _vp, _vp]),
+    "rb_adjoint_fields": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _vp, _vp]),
     "rb_femgetdet": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i64, _i64, _i32, _vp, _vp]),
     "rb_femsolve_work_bytes": (_sz, [_i64, _i64, _i64, _i32, _i32]),
     "rb_femsolve": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _vp, _i64, ctypes.POINTER(RbSolveOpts),

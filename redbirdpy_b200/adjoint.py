@@ -1,0 +1,218 @@
+"""Differentiable forward model: per-node (mua, D) -> detector values, with a
+hand-written adjoint backward (a ``torch.autograd.Function``).
+
+The forward pass is runforward's pipeline on the device (femrhs, femlhs with
+node-based properties, femsolve, femgetdet; redbirdpy/forward.py:152-199).
+Sources and detectors are solved as one block of right-hand sides, so the
+detector fields phi_d - the adjoint fields that redbirdpy's jac contracts
+with the source fields (redbirdpy/forward.py:621-681) - come out of the same
+solve.  For a real loss L of detval[d, s] with upstream gradient g (PyTorch's
+convention: g = dL/dRe + i dL/dIm for complex detector values):
+
+    dL/dp_n = Re sum_s phi_s^T (-dA/dp_n) lambda_s,
+    lambda_s = sum_d conj(g[d, s]) phi_d = A^-1 sum_d conj(g[d, s]) b_d
+
+(A is symmetric, complex-symmetric in the frequency domain).  lambda is the
+transposed solve of the backward, formed from the detector columns already in
+hand; ``resolve=True`` solves A lambda_s = sum_d conj(g[d, s]) b_d afresh
+instead.  The contraction is rb_jac's per-node bilinear form evaluated on the
+(source, lambda) column pairs, with the exact derivatives of the node-based
+assembly: 'mua_nodal' (mua at fixed D) and 'D' (the nodal D whose element
+mean femlhs uses, redbirdpy/forward.py:289-340).
+"""
+
+import numpy as np
+import torch
+
+from . import engine
+from .solver import solver_options
+
+__all__ = ["DeviceModel", "BatchModel", "detector_values"]
+
+
+class DeviceModel:
+    """Mesh, optodes and solver settings of one differentiable forward model.
+
+    Right-hand-side columns are [sources | detectors] (``S`` and ``D`` of
+    them); ``getdet`` gives the detector values as (detector rows) x S, and
+    ``row0``/``det0`` delimit the instances (one here, many in BatchModel)."""
+
+    def __init__(self, cfg, precision="mixed", **solver_kw):
+        props = np.atleast_2d(np.asarray(cfg["prop"], dtype=np.float64))
+        self.mesh = engine.mesh_of(cfg)
+        if props.shape[0] != self.mesh.nn:
+            raise ValueError("detector_values needs node-based properties (one prop row per node)")
+        self.nref = props[:, 3] if props.shape[1] >= 4 else 1.37
+        self.omega = float(cfg.get("omega", 0) or 0)
+        self.reff = cfg.get("reff", 0.493)
+        self.opt = engine.locate_optodes(self.mesh, cfg)
+        if self.opt.nsrc < 1 or self.opt.ndet < 1:
+            raise ValueError("Must define at least one source and detector")
+        if self.opt.nsrc > 64 or self.opt.ndet > 64:
+            raise ValueError("detector_values handles at most 64 sources and 64 detectors")
+        self.S, self.D = self.opt.nsrc, self.opt.ndet
+        self.B = self.opt.rhs(self.mesh)
+        dev = self.mesh.device
+        self.row0 = torch.tensor([0, self.mesh.nn], dtype=torch.int64, device=dev)
+        self.det0 = torch.tensor([0, self.D], dtype=torch.int64, device=dev)
+        self.ninst = 1
+        self.solve_kw = dict(solver_options(solver_kw), precision=precision)
+
+    def optics(self, mua, dcoef):
+        """Optics with node mua and D (musp = 1/(3D) - mua, so that femlhs's
+        D = 1/(3(mua + musp)) returns the given D)."""
+        musp = 1.0 / (3.0 * dcoef) - mua
+        return engine.Optics(self.mesh, mua.contiguous(), musp.contiguous(), self.nref, self.omega, self.reff)
+
+    def fields(self, mua, dcoef):
+        mat = engine.assemble(self.mesh, self.optics(mua, dcoef))
+        phi, info = engine.solve(mat, self.B, **self.solve_kw)
+        if info["flag"] != 0:
+            raise RuntimeError(f"forward solve did not converge (flag {info['flag']})")
+        return phi, mat
+
+    def getdet(self, phi):
+        return engine.getdet(self.mesh, self.opt, phi)
+
+
+class BatchModel(DeviceModel):
+    """Many independent meshes as one block-diagonal system: one assembly,
+    one multi-RHS solve and one adjoint contraction for all of them.
+
+    Instance i's nodes, tets and faces follow those of instance i-1 (indices
+    offset, coordinates untouched, so every element's geometry is its own).
+    Right-hand-side column j < S is source j of every instance that has one
+    (zero elsewhere), column S + j detector j: the solve needs
+    max(sources) + max(detectors) columns however many instances there are,
+    and the block-diagonal matrix keeps the instances' fields apart.  All
+    instances share omega and the boundary reflection coefficient."""
+
+    def __init__(self, cfgs, precision="mixed", **solver_kw):
+        from .utility import getoptodes
+
+        if not cfgs:
+            raise ValueError("BatchModel needs at least one instance")
+        nns = [c["node"].shape[0] for c in cfgs]
+        nes = [c["elem"].shape[0] for c in cfgs]
+        self.node_off = np.concatenate([[0], np.cumsum(nns)])
+        self.elem_off = np.concatenate([[0], np.cumsum(nes)])
+        node = np.vstack([np.asarray(c["node"], dtype=np.float64)[:, :3] for c in cfgs])
+        elem = np.vstack([np.asarray(c["elem"])[:, :4].astype(np.int64) + o for c, o in zip(cfgs, self.node_off)])
+        face = np.vstack([np.asarray(c["face"])[:, :3].astype(np.int64) + o for c, o in zip(cfgs, self.node_off)])
+        area = np.concatenate([np.asarray(c["area"], dtype=np.float64) for c in cfgs])
+        evol = np.concatenate([np.asarray(c["evol"], dtype=np.float64) for c in cfgs])
+        omegas = {float(c.get("omega", 0) or 0) for c in cfgs}
+        reffs = {float(c.get("reff", 0.493)) for c in cfgs}
+        if len(omegas) != 1 or len(reffs) != 1:
+            raise ValueError("batched instances must share omega and reff")
+        self.omega, self.reff = omegas.pop(), reffs.pop()
+        props = [np.atleast_2d(np.asarray(c["prop"], dtype=np.float64)) for c in cfgs]
+        if any(p.shape[0] != n for p, n in zip(props, nns)):
+            raise ValueError("detector_values needs node-based properties (one prop row per node)")
+        nref = np.concatenate([p[:, 3] if p.shape[1] >= 4 else np.full(p.shape[0], 1.37) for p in props])
+        self.nref = nref if np.ptp(nref) > 0 else float(nref[0])
+        self.mesh = engine.DeviceMesh(node, elem, face, area, evol)
+        dev = self.mesh.device
+        # optodes: located among each instance's own tets
+        self.ns, self.nd = [], []
+        locs, barys = [], []
+        for i, c in enumerate(cfgs):
+            src, det, _, _ = getoptodes(c)
+            pts = np.vstack([src, det])
+            self.ns.append(src.shape[0])
+            self.nd.append(det.shape[0])
+            pt = torch.as_tensor(pts, dtype=torch.float64, device=dev)
+            loc = torch.empty(pts.shape[0], dtype=torch.int32, device=dev)
+            bary = torch.empty((pts.shape[0], 4), dtype=torch.float64, device=dev)
+            e0, e1 = int(self.elem_off[i]), int(self.elem_off[i + 1])
+            engine.call("rb_tsearch", engine.ptr(self.mesh.node), engine.ptr(self.mesh.elem[e0:e1]), e1 - e0,
+                        engine.ptr(pt), pts.shape[0], engine.ptr(loc), engine.ptr(bary), engine.stream())
+            locs.append(torch.where(loc >= 0, loc + e0, loc))
+            barys.append(bary)
+        self.S, self.D = max(self.ns), max(self.nd)
+        if self.S + self.D > 128:
+            raise ValueError("batched instances: at most 128 source + detector columns")
+        self.B = torch.zeros((self.mesh.nn, self.S + self.D), dtype=torch.float64, device=dev)
+        for i in range(len(cfgs)):
+            ns, nd = self.ns[i], self.nd[i]
+            for lo, cnt, col0 in ((0, ns, 0), (ns, nd, self.S)):
+                engine.call("rb_point_rhs", engine.ptr(self.mesh.elem), engine.ptr(locs[i][lo:lo + cnt]),
+                            engine.ptr(barys[i][lo:lo + cnt]), cnt, self.mesh.nn, self.S + self.D, col0,
+                            engine.ptr(self.B), engine.stream())
+        self.loc_det = torch.cat([l[n:] for l, n in zip(locs, self.ns)]).contiguous()
+        self.bary_det = torch.cat([b[n:] for b, n in zip(barys, self.ns)]).contiguous()
+        self.row0 = torch.as_tensor(self.node_off, dtype=torch.int64, device=dev)
+        self.det0 = torch.as_tensor(np.concatenate([[0], np.cumsum(self.nd)]), dtype=torch.int64, device=dev)
+        self.ninst = len(cfgs)
+        self.solve_kw = dict(solver_options(solver_kw), precision=precision)
+
+    def getdet(self, phi):
+        """All instances' detector values: row det0[i] + d, column s."""
+        kind = engine._lib.RB_C128 if phi.is_complex() else engine._lib.RB_F64
+        nd = int(self.det0[-1].item())
+        out = torch.empty((nd, self.S), dtype=phi.dtype, device=phi.device)
+        engine.call("rb_femgetdet", engine.ptr(self.mesh.elem), engine.ptr(self.loc_det), engine.ptr(self.bary_det),
+                    nd, engine.ptr(phi), phi.shape[1], self.S, kind, engine.ptr(out), engine.stream())
+        return out
+
+    def split(self, det):
+        """Per-instance (ndet_i x nsrc_i) views of getdet's output."""
+        d0 = self.det0.cpu().numpy()
+        return [det[d0[i]:d0[i + 1], :self.ns[i]] for i in range(self.ninst)]
+
+    def node_slices(self, v):
+        return [v[self.node_off[i]:self.node_off[i + 1]] for i in range(self.ninst)]
+
+
+class _DetectorValues(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, mua, dcoef, model, resolve):
+        phi, mat = model.fields(mua.detach(), dcoef.detach())
+        det = model.getdet(phi)
+        ctx.model, ctx.resolve, ctx.mat = model, resolve, mat
+        ctx.save_for_backward(phi)
+        return det
+
+    @staticmethod
+    def backward(ctx, g):
+        (phi,) = ctx.saved_tensors
+        model = ctx.model
+        S, D = model.S, model.D
+        g = g.to(phi.dtype).contiguous()
+        if ctx.resolve:
+            # transposed solve: A lambda_s = sum_d conj(g[d, s]) b_d; the
+            # solver takes real right-hand sides, so complex ones go as Re, Im
+            gc = g.conj() if phi.is_complex() else g
+            bd = model.B[:, S:S + D]
+            if phi.is_complex():
+                lr, _ = engine.solve(ctx.mat, (bd @ gc.real).contiguous(), **model.solve_kw)
+                li, _ = engine.solve(ctx.mat, (bd @ gc.imag).contiguous(), **model.solve_kw)
+                lam = lr + 1j * li
+            else:
+                lam, _ = engine.solve(ctx.mat, (bd @ gc).contiguous(), **model.solve_kw)
+        else:
+            # the detector columns are A^-1 b_d already
+            lam = torch.empty((phi.shape[0], S), dtype=phi.dtype, device=phi.device)
+            kind = engine._lib.RB_C128 if phi.is_complex() else engine._lib.RB_F64
+            engine.call("rb_adjoint_fields", engine.ptr(phi), phi.shape[0], phi.shape[1], S, engine.ptr(g), S,
+                        engine.ptr(model.row0), engine.ptr(model.det0), model.ninst, kind, engine.ptr(lam),
+                        engine.stream())
+        fields = torch.cat([phi[:, :S], lam], dim=1).contiguous()
+        pairs = np.column_stack([np.arange(S), S + np.arange(S), np.ones(S, dtype=np.int64)])
+        grads = []
+        for what, need in (("mua_nodal", ctx.needs_input_grad[0]), ("D", ctx.needs_input_grad[1])):
+            if not need:
+                grads.append(None)
+                continue
+            J = engine.jacobian(model.mesh, fields, pairs, what, out_dtype=torch.float64)
+            grads.append((J.real if J.is_complex() else J).sum(dim=0))
+        return grads[0], grads[1], None, None
+
+
+def detector_values(model, mua, dcoef, resolve=False):
+    """Detector values of the node-based forward model at per-node ``mua``
+    and ``dcoef`` (D, mm), differentiable in both through the adjoint
+    backward: (ndet x nsrc) for a DeviceModel, all instances' detector rows x
+    max(nsrc) for a BatchModel (``split`` gives the per-instance blocks).
+    Real for CW, complex in the frequency domain."""
+    return _DetectorValues.apply(mua, dcoef, model, resolve)

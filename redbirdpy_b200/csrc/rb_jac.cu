@@ -307,11 +307,56 @@ static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t s
   return launch_jac_t<C, In, SPLIT, false>(a, phi, J, st);
 }
 
+// lam[r][s] = sum_d phi[r][dcol0 + d] conj(g[det0_i + d][s]) for the instance i of row r
+template <typename T>
+__global__ void adjoint_fields_kernel(const T* __restrict__ phi, int64_t nn, int64_t ld, int64_t dcol0,
+                                      const T* __restrict__ g, int64_t ns, const int64_t* __restrict__ row0,
+                                      const int64_t* __restrict__ det0, int64_t ninst, T* __restrict__ lam) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn * ns;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / ns, s = t - r * ns;
+    int64_t lo = 0, hi = ninst - 1;  // instance of row r: row0[i] <= r < row0[i + 1]
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (row0[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    const int64_t d0 = det0[lo], nd = det0[lo + 1] - d0;
+    T acc = s_zero(T());
+    for (int64_t d = 0; d < nd; ++d) {
+      T gv = g[(d0 + d) * ns + s];
+      if constexpr (Scalar<T>::is_complex) gv.y = -gv.y;
+      acc = s_fma(phi[r * ld + dcol0 + d], gv, acc);
+    }
+    lam[r * ns + s] = acc;
+  }
+}
+
 }  // namespace rb
 
 using namespace rb;
 
 extern "C" {
+
+int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, const void* g, int64_t ns,
+                      const int64_t* row0, const int64_t* det0, int64_t ninst, int32_t kind, void* lam,
+                      void* stream) {
+  if (!phi || !g || !row0 || !det0 || !lam || nn < 0 || ns < 0 || ninst < 1 || dcol0 < 0 || dcol0 > ld)
+    return fail(RB_EARG, "rb_adjoint_fields: bad arguments");
+  if (nn * ns == 0) return RB_OK;
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(nn * ns, 256), 148 * 32);
+  cudaStream_t st = as_stream(stream);
+  if (kind == RB_F64)
+    adjoint_fields_kernel<double><<<grid, 256, 0, st>>>((const double*)phi, nn, ld, dcol0, (const double*)g, ns, row0,
+                                                        det0, ninst, (double*)lam);
+  else if (kind == RB_C128)
+    adjoint_fields_kernel<cdouble><<<grid, 256, 0, st>>>((const cdouble*)phi, nn, ld, dcol0, (const cdouble*)g, ns,
+                                                         row0, det0, ninst, (cdouble*)lam);
+  else
+    return fail(RB_EARG, "rb_adjoint_fields: kind must be RB_F64 or RB_C128");
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
 
 int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
             const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,

@@ -15,7 +15,7 @@ tetrahedra come out with negative signed volume and ``meshprep`` swaps nodes
 
 import numpy as np
 
-__all__ = ["kuhn_box", "grid_optodes"]
+__all__ = ["kuhn_box", "grid_optodes", "batch_boxes"]
 
 
 def kuhn_box(size, spacing, origin=(0.0, 0.0, 0.0)):
@@ -59,3 +59,31 @@ def grid_optodes(x_range, y_range, n_per_side, z=0.0, offset=(0.0, 0.0)):
     ys = np.linspace(y_range[0], y_range[1], n_per_side) + offset[1]
     yy, xx = np.meshgrid(ys, xs, indexing="ij")
     return np.column_stack([xx.ravel(), yy.ravel(), np.full(xx.size, float(z))])
+
+
+def batch_boxes(count=256, seed=2, dims=(30.0, 80.0), spacings=(2.0, 3.0, 4.0), nopt=(4, 16),
+                mua=(0.005, 0.03), mus=(0.5, 2.0), nref=1.37):
+    """Independent box workloads of uneven size (unprepared cfg dicts).
+
+    Per instance: extents ~ U[dims] mm per axis rounded to a multiple of a
+    spacing drawn from ``spacings``; per-node mua ~ U[mua], mus ~ U[mus],
+    g = 0, n = ``nref``; ``nopt`` ranges the number of sources and, separately,
+    of detectors, placed at random on the top face (z = 0, pointing +z) at
+    least one cell from its edges.  CW (omega = 0)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        h = float(rng.choice(spacings))
+        size = np.maximum(np.rint(rng.uniform(dims[0], dims[1], 3) / h), 2) * h
+        node, elem = kuhn_box(size, h)
+        nn = node.shape[0]
+        prop = np.column_stack([rng.uniform(mua[0], mua[1], nn), rng.uniform(mus[0], mus[1], nn), np.zeros(nn),
+                                np.full(nn, nref)])
+        ns, nd = rng.integers(nopt[0], nopt[1] + 1, 2)
+
+        def top(k):
+            return np.column_stack([rng.uniform(h, size[0] - h, k), rng.uniform(h, size[1] - h, k), np.zeros(k)])
+
+        out.append(dict(node=node, elem=elem, prop=prop, srcpos=top(ns), srcdir=np.array([[0, 0, 1.0]]),
+                        detpos=top(nd), detdir=np.array([[0, 0, 1.0]]), omega=0.0))
+    return out
