@@ -62,20 +62,42 @@ struct JacArgs {
   int32_t grid;  // pairs are all (source slot, detector) combinations, detector-major
 };
 
-// smem layout (bytes), TN nodes:
-//   phi [TN][rmax][nc] C | Bm [TN][rmax][rmax] R | Cm [TN][rmax][ndet] C |
-//   W [TN][emax][16] R | EN [TN][emax] int4 | nb [TN][rmax] int | rn [TN] int
+// Per-node strides of the staged phi and C blocks, padded so that the TN
+// nodes a warp covers land in different shared-memory banks: with E
+// elements per 128-byte bank row, the phi stride is 1 (mod E) and the C
+// stride E/4 (mod E).
+template <typename C> __host__ __device__ inline int jac_phi_stride(int rmax, int nc) {
+  constexpr int E = 128 / (int)sizeof(C);
+  return (rmax * nc + E - 1) / E * E + 1;
+}
+template <typename C> __host__ __device__ inline int jac_c_stride(int rmax, int nd) {
+  constexpr int E = 128 / (int)sizeof(C);
+  return (rmax * nd + E - 1) / E * E + E / 4;
+}
+
+// smem layout, TN nodes, each region starting on a 16-byte boundary:
+//   phi [TN][phi stride] C | Bm [TN][rmax][rmax] R | Cm [TN][C stride] C |
+//   W [TN][emax][16] R | EN [TN][emax] int4 | nb [TN][rmax] int | rn, ek [TN] int
+__host__ __device__ inline size_t al16(size_t b) { return (b + 15) / 16 * 16; }
+struct JacSmem {
+  size_t phi, B, C, W, EN, nb, total;
+};
+template <typename C>
+__host__ __device__ inline JacSmem jac_layout(int TN, int rmax, int nc, int ndet, int emax) {
+  typedef typename JacT<C>::real R;
+  JacSmem L;
+  L.phi = 0;
+  L.B = L.phi + al16((size_t)TN * jac_phi_stride<C>(rmax, nc) * sizeof(C));
+  L.C = L.B + al16((size_t)TN * rmax * rmax * sizeof(R));
+  L.W = L.C + al16((size_t)TN * jac_c_stride<C>(rmax, ndet) * sizeof(C));
+  L.EN = L.W + al16((size_t)TN * emax * 16 * sizeof(R));
+  L.nb = L.EN + al16((size_t)TN * emax * sizeof(int4));
+  L.total = L.nb + al16((size_t)TN * rmax * sizeof(int) + TN * sizeof(int) * 2);
+  return L;
+}
 template <typename C>
 __host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, int emax) {
-  typedef typename JacT<C>::real R;
-  size_t s = 0;
-  s += (size_t)TN * rmax * nc * sizeof(C);
-  s += (size_t)TN * rmax * rmax * sizeof(R);
-  s += (size_t)TN * rmax * ndet * sizeof(C);
-  s += (size_t)TN * emax * 16 * sizeof(R);
-  s += (size_t)TN * emax * sizeof(int4);
-  s += (size_t)TN * rmax * sizeof(int) + TN * sizeof(int) * 2;
-  return (s + 15) / 16 * 16;
+  return jac_layout<C>(TN, rmax, nc, ndet, emax).total;
 }
 
 template <typename C, typename In, int TN, bool SPLIT, bool GRID>
@@ -84,12 +106,14 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   typedef typename JacT<C>::real R;
   extern __shared__ __align__(16) unsigned char smem[];
   const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax;
-  C* sphi = reinterpret_cast<C*>(smem);
-  R* sB = reinterpret_cast<R*>(sphi + (size_t)TN * rmax * nc);
-  C* sC = reinterpret_cast<C*>(sB + (size_t)TN * rmax * rmax);
-  R* sW = reinterpret_cast<R*>(sC + (size_t)TN * rmax * nd);
-  int4* sEN = reinterpret_cast<int4*>(sW + (size_t)TN * emax * 16);
-  int* snb = reinterpret_cast<int*>(sEN + (size_t)TN * emax);
+  const int SP = jac_phi_stride<C>(rmax, nc), SC = jac_c_stride<C>(rmax, nd);
+  const JacSmem L = jac_layout<C>(TN, rmax, nc, nd, emax);
+  C* sphi = reinterpret_cast<C*>(smem + L.phi);
+  R* sB = reinterpret_cast<R*>(smem + L.B);
+  C* sC = reinterpret_cast<C*>(smem + L.C);
+  R* sW = reinterpret_cast<R*>(smem + L.W);
+  int4* sEN = reinterpret_cast<int4*>(smem + L.EN);
+  int* snb = reinterpret_cast<int*>(smem + L.nb);
   int* srn = snb + TN * rmax;
   int* sek = srn + TN;
 
@@ -142,7 +166,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     C v;
     if (nb >= 0) v = cvt<C, In>(phi[(int64_t)nb * a.ld + a.cols[c]]);
     else v = s_zero(C());
-    sphi[i] = v;
+    sphi[(size_t)(slot / rmax) * SP + (size_t)(slot % rmax) * nc + c] = v;
   }
   // 2. B_n[a][b] = sum over the node's tets of w_e at the local positions
   for (int i = tid; i < TN * rmax * rmax; i += kJacThreads) {
@@ -173,10 +197,10 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     C s = s_zero(C());
     if (ia < srn[t]) {
       const R* Brow = sB + ((size_t)t * rmax + ia) * rmax;
-      const C* P = sphi + (size_t)t * rmax * nc + a.det0 + d;
+      const C* P = sphi + (size_t)t * SP + a.det0 + d;
       for (int b = 0; b < srn[t]; ++b) s = s_add(s, scale_r(Brow[b], P[(size_t)b * nc]));
     }
-    sC[i] = s;
+    sC[(size_t)t * SC + r] = s;
   }
   __syncthreads();
   // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]
@@ -197,8 +221,8 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) acc[u][v] = s_zero(C());
       for (int ia = 0; ia < srn[t]; ++ia) {
-        const C* P = sphi + ((size_t)t * rmax + ia) * nc + sb * 4;
-        const C* Cn = sC + ((size_t)t * rmax + ia) * nd + db * 4;
+        const C* P = sphi + (size_t)t * SP + (size_t)ia * nc + sb * 4;
+        const C* Cn = sC + (size_t)t * SC + (size_t)ia * nd + db * 4;
         C pv[4], cv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -234,8 +258,8 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     const int64_t n = n0 + t;
     if (n >= a.nn) continue;
     const int ps = a.psrc[k], pd = a.pdet[k];
-    const C* P = sphi + (size_t)t * rmax * nc + ps;
-    const C* Cn = sC + (size_t)t * rmax * nd + pd;
+    const C* P = sphi + (size_t)t * SP + ps;
+    const C* Cn = sC + (size_t)t * SC + pd;
     C s = s_zero(C());
     for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
     if constexpr (SPLIT) {
