@@ -98,7 +98,7 @@ typedef struct rb_optics {
 } rb_optics;
 
 /* Per-tet mua and musp from a label table (the label branch of femlhs,
- * redbirdpy/forward.py:244-252: prop[seg]): mua_out[e] = tab[l][0],
+ * redbirdpy/forward.py:127-140: prop[seg]): mua_out[e] = tab[l][0],
  * musp_out[e] = tab[l][1] * (1 - tab[l][2]) with l = seg[e] clipped to
  * [0, nlabel).  tab is nlabel x ncol (ncol >= 2; g is taken as 0 when
  * ncol == 2), all on the device. */

@@ -2,10 +2,10 @@
 hand-written adjoint backward (a ``torch.autograd.Function``).
 
 The forward pass is runforward's pipeline on the device (femrhs, femlhs with
-node-based properties, femsolve, femgetdet; redbirdpy/forward.py:152-199).
+node-based properties, femsolve, femgetdet; redbirdpy/forward.py:40-87).
 Sources and detectors are solved as one block of right-hand sides, so the
 detector fields phi_d - the adjoint fields that redbirdpy's jac contracts
-with the source fields (redbirdpy/forward.py:621-681) - come out of the same
+with the source fields (redbirdpy/forward.py:509-569) - come out of the same
 solve.  For a real loss L of detval[d, s] with upstream gradient g (PyTorch's
 convention: g = dL/dRe + i dL/dIm for complex detector values):
 
@@ -18,7 +18,7 @@ hand; ``resolve=True`` solves A lambda_s = sum_d conj(g[d, s]) b_d afresh
 instead.  The contraction is rb_jac's per-node bilinear form evaluated on the
 (source, lambda) column pairs, with the exact derivatives of the node-based
 assembly: 'mua_nodal' (mua at fixed D) and 'D' (the nodal D whose element
-mean femlhs uses, redbirdpy/forward.py:289-340).
+mean femlhs uses, redbirdpy/forward.py:177-228).
 """
 
 import numpy as np

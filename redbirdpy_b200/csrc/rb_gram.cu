@@ -37,9 +37,14 @@ constexpr int kGSmem = kGStages * kGStageBytes + 1024 + 256;  // ring + alignmen
 constexpr int kGThreads = 192;
 constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators (rows 0-127, 128-255)
 // K-blocks per accumulation chunk: the tensor cores' FP32 accumulator is
-// drained into the FP64 output every kGChunk * 32 K-elements, so that its
-// rounding never builds up over the (up to ~10^6 long) K dimension
+// drained into the FP64 output every chunk * 32 K-elements, because its
+// rounding error grows linearly with the chunk length (measured ~2e-5
+// relative per 4096 K; ~8e-3 after one undrained sweep of K = 10^6).  The
+// split form (tf32x3) drains every 4096 K; the plain TF32 form every 16384 K
+// (~1e-4, below what its rounded inputs allow), so that its MMAs wait on
+// four times fewer drains.
 constexpr int kGChunk = 128;
+constexpr int kGChunkTf32 = 512;
 constexpr long long kGWaitLimit = 1LL << 24;  // polls before a wait gives up (seconds)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -155,6 +160,7 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   // H = hi hi^T + hi lo^T + lo hi^T, one K sweep per product, one accumulator
   const int nk1 = (int)((K + kGK - 1) / kGK);
   const int nk = nk1 * segs;
+  const int chunk = (segs == 1) ? kGChunkTf32 : kGChunk;  // K-blocks between drains
 
   if (warp == 0) {
     if (lane == 0) {
@@ -178,9 +184,9 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     if (lane == 0) {
       for (int kb = 0; kb < nk; ++kb) {
         const int s = kb % kGStages;
-        const int c = kb / kGChunk;
-        const bool first = (kb % kGChunk) == 0;
-        const bool last = (kb % kGChunk) == kGChunk - 1 || kb == nk - 1;
+        const int c = kb / chunk;
+        const bool first = (kb % chunk) == 0;
+        const bool last = (kb % chunk) == chunk - 1 || kb == nk - 1;
         // a new chunk waits until the epilogue drained the previous one
         if (first && c >= 1 && !mbar_wait(smem_u32(tempty), (c - 1) & 1, err, 4)) break;
         if (!mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2)) break;
@@ -204,7 +210,7 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     // the FP64 output rows
     const int q = warp & 3;
     const int row = 32 * q + lane;
-    const int nchunk = (nk + kGChunk - 1) / kGChunk;
+    const int nchunk = (nk + chunk - 1) / chunk;
     for (int c = 0; c < nchunk; ++c) {
       // warp-uniform outcome: tcgen05.ld below needs the whole warp
       const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(tfull), c & 1, err, 3));
