@@ -252,6 +252,10 @@ def run_b200(args):
     h2d = (2 * mesh.ne * 8) + 128 * 3 * 8
     d2h = det_h.nbytes + phi_h.nbytes
 
+    traffic = {}
+    tp = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp))
     it = infos[-1]
     out = {
         "metric": METRIC, "value": round(world * nrhs / (ms_mixed * 1e-3), 3), "unit": UNIT,
@@ -270,13 +274,16 @@ def run_b200(args):
         "roofline": {"bound": "hbm", "kernel": "spmm_kernel<float> (CSR SpMM, 128 RHS, fused p.Ap)",
                      "achieved": round(sp_gbs, 1) if sp_gbs else None, "peak": peak, "unit": "GB/s",
                      "frac": round(sp_gbs / peak, 4) if sp_gbs else None, "peak_source": peak_kind,
-                     "algorithmic_bytes": spmm_bytes, "launch_ms": round(sp_ms, 4), "traffic": None},
+                     "algorithmic_bytes": spmm_bytes, "launch_ms": round(sp_ms, 4),
+                     "traffic": traffic.get("spmm_kernel<float,32,4,EPI_PQDOT>"),
+                     "traffic_source": "ncu capture, profiles/forward_3Mtet_128rhs_launches_and_kernels.md"},
         "roofline_update": {"kernel": "cg_update_kernel<float>", "achieved": round(up_gbs, 1) if up_gbs else None,
                             "unit": "GB/s", "frac": round(up_gbs / peak, 4) if up_gbs else None,
-                            "algorithmic_bytes": upd_bytes, "launch_ms": round(up_ms, 4)},
+                            "algorithmic_bytes": upd_bytes, "launch_ms": round(up_ms, 4),
+                            "traffic": traffic.get("cg_update_kernel<float,32,4>")},
         "roofline_assembly": {"kernel": "femlhs_rows_kernel (+ dcoeff prologue)", "achieved": round(asm_gbs, 1),
                               "unit": "GB/s", "frac": round(asm_gbs / peak, 4), "algorithmic_bytes": asm_bytes,
-                              "launch_ms": round(asm_ms, 4)},
+                              "launch_ms": round(asm_ms, 4), "traffic": traffic.get("femlhs_rows_kernel<real,per-tet>")},
         "e2e": {"value": round(world * nrhs / e2e_s, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,
