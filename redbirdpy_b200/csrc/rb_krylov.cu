@@ -513,6 +513,17 @@ constexpr size_t grp_smem_bytes() {
 }
 
 // ------------------------------------------------------- CG vector kernels
+// relres, stagnation and the per-column scale of the next correction
+struct OuterState {
+  double bnorm;
+  double relres;
+  double prev;
+  double scale;
+  double itol2;  // squared inner tolerance of the next sweep
+  int32_t active;
+  int32_t done;  // 1 converged, 2 stagnated, 3 non-finite residual
+};
+
 // Per-column state of the inner Krylov iteration (device).
 struct ColState {
   cdouble rz;      // (r, z) unconjugated (real solves use .x)
@@ -521,6 +532,7 @@ struct ColState {
   cdouble beta;
   double rr;       // ||r||^2
   double rr0;      // ||r_0||^2
+  double tol2;     // squared relative tolerance of this column's sweep (< 0: the solve's own)
   int32_t active;  // column still iterating
   int32_t status;  // 0 running/converged, 2 breakdown
   int32_t iters;
@@ -683,7 +695,7 @@ __device__ __forceinline__ cdouble sum_part(const A* __restrict__ part, int nb, 
 // after init: rz, rr0; a column is active iff its rhs is nonzero and enabled
 template <typename A>
 __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
-                                const int32_t* __restrict__ enable) {
+                                const int32_t* __restrict__ enable, const OuterState* __restrict__ os) {
   RB_FIN_WARP();
   const cdouble rz = sum_part<A>(part_rz, nb, k, c, lane);
   const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
@@ -695,6 +707,7 @@ __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const doubl
   s.active = (enable == nullptr || enable[c]) && s.rr > 0.0;
   s.status = 0;
   s.iters = 0;
+  s.tol2 = os ? os[c].itol2 : -1.0;
   s.alpha = make_double2(0, 0);
   s.beta = make_double2(0, 0);
   cs[c] = s;
@@ -733,7 +746,7 @@ __global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const doubl
   if (!finite_c(rzn) || !isfinite(rr)) {
     s.active = 0;
     s.status = 2;
-  } else if (rr <= tol2 * s.rr0) {
+  } else if (rr <= (s.tol2 >= 0.0 ? s.tol2 : tol2) * s.rr0) {
     s.active = 0;
   } else if (s.rz.x == 0.0 && s.rz.y == 0.0) {
     s.active = 0;
@@ -747,15 +760,6 @@ __global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const doubl
 }
 
 // --------------------------------------------------- refinement kernels
-// relres, stagnation and the per-column scale of the next correction
-struct OuterState {
-  double bnorm;
-  double relres;
-  double prev;
-  double scale;
-  int32_t active;
-  int32_t done;  // 1 converged, 2 stagnated, 3 non-finite residual
-};
 
 __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterState* os) {
   RB_FIN_WARP();
@@ -767,13 +771,19 @@ __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterSta
   o.relres = (s > 0.0) ? 1e300 : 0.0;
   o.prev = 1e300;
   o.scale = 0.0;
+  o.itol2 = -1.0;
   o.active = s > 0.0;
   o.done = (s > 0.0) ? 0 : 1;
   os[c] = o;
 }
 
+// A sweep normally solves its correction to inner_tol.  The sweep that will
+// bring a column to the target solves to 1e-2 * tol / relres instead (not
+// below itol_min, the inner precision's reach): it over-solves past the FP64
+// floor, so that small far-field entries of the solution, which a global
+// residual norm barely sees, converge as well.
 __global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterState* os, double tol,
-                                 double stall, int32_t* nactive) {
+                                 double stall, double inner_tol, double itol_min, int32_t* nactive) {
   RB_FIN_WARP();
   if (!os[c].active) return;
   const double s = sum_part<double>(part, nb, k, c, lane).x;
@@ -793,6 +803,9 @@ __global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterSta
     o.done = 2;
   } else {
     o.scale = 1.0 / sqrt(s);
+    double it = inner_tol;
+    if (rel * inner_tol < 10.0 * tol) it = fmax(fmin(inner_tol, 1e-2 * tol / rel), itol_min);
+    o.itol2 = it * it;
   }
   os[c] = o;
   if (o.active) atomicAdd(nactive, 1);
@@ -1069,7 +1082,8 @@ template <typename T>
 static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, const Shape& sh, const Shape& shs,
                        void* part_a,
                        double* part_b, T* Xs, T* R, T* P, T* Q, ColState* cs, const int32_t* enable,
-                       int32_t* counter, double tol, int maxiter, int check_every, int* iters_out,
+                       const OuterState* os, int32_t* counter, double tol, int maxiter, int check_every,
+                       int* iters_out,
                        int* launches, KernelTimer& tm, const GroupPlan* gp, cudaStream_t st) {
   typedef typename Scalar<T>::acc Acc;
   const int64_t n = A.n;
@@ -1079,7 +1093,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
   RB_DISPATCH_LV(sh, RB_INIT);
 #undef RB_INIT
   RB_LAUNCH_CHECK();
-  fin_init_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable);
+  fin_init_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable, os);
   RB_LAUNCH_CHECK();
   *launches += 2;
   int it = 0;
@@ -1150,7 +1164,9 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     // R64 = B - A X (FP64)
     RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh64, st)));
     RB_CUDA_TRY(cudaMemsetAsync(b.counter + 1, 0, sizeof(int32_t), st));
-    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os, o.tol, stall, b.counter + 1);
+    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os, o.tol, stall, o.inner_tol,
+                                         sizeof(T) == sizeof(T64) ? o.inner_tol : std::min(o.inner_tol, 1e-6),
+                                         b.counter + 1);
     RB_LAUNCH_CHECK();
     launches += 2;
     int32_t nact = 0;
@@ -1162,7 +1178,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     launches += 1;
     int it = 0;
     RB_TRY(inner_solve<T>(A, val, dinv, k, sh, shs, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
-                          b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, st));
+                          b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, st));
     total_iters += it;
     if (it >= o.maxiter) sweep_flag = 1;
     correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, b.os, X);
