@@ -28,14 +28,33 @@ __global__ void prep_scale_kernel(double* __restrict__ H, int64_t M, int64_t ldh
   H[i * ldh + j] *= di[i] * di[j];
 }
 
+// Stage the lower triangle of the nb x nb block at (r0, c0) of H into
+// shared memory (zeros above the diagonal), all loads issued before the
+// stores so that they overlap (the block is read once from L2/HBM).
+template <int LD>
+__device__ __forceinline__ void load_lower(const double* __restrict__ H, int64_t ldh, int64_t r0, int64_t c0, int nb,
+                                           double (*A)[LD]) {
+  constexpr int kPer = 16;
+  for (int e0 = threadIdx.x; e0 < kNB * kNB; e0 += kPer * blockDim.x) {
+    double v[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = e0 + u * blockDim.x, i = e / kNB, j = e % kNB;
+      v[u] = (e < kNB * kNB && i < nb && j <= i) ? H[(r0 + i) * ldh + c0 + j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < kNB * kNB) A[e / kNB][e % kNB] = v[u];
+    }
+  }
+}
+
 // factor the nb x nb diagonal block at (j0, j0) in shared memory (lower)
 __global__ void potrf_diag_kernel(double* __restrict__ H, int64_t ldh, int64_t j0, int nb, int* __restrict__ err) {
   __shared__ double A[kNB][kNB + 1];
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < nb * nb; e += nt) {
-    const int i = e / nb, j = e % nb;
-    A[i][j] = (j <= i) ? H[(j0 + i) * ldh + j0 + j] : 0.0;
-  }
+  load_lower<kNB + 1>(H, ldh, j0, j0, nb, A);
   __syncthreads();
   for (int c = 0; c < nb; ++c) {
     __shared__ double piv;
@@ -71,28 +90,30 @@ __global__ void trsm_panel_kernel(double* __restrict__ H, int64_t ldh, int64_t M
   __shared__ double L[kNB][kNB + 1];
   extern __shared__ double xs[];  // [kNB][blockDim.x]
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < nb * nb; e += nt) {
-    const int i = e / nb, j = e % nb;
-    L[i][j] = (j <= i) ? H[(j0 + i) * ldh + j0 + j] : 0.0;
-  }
+  load_lower<kNB + 1>(H, ldh, j0, j0, nb, L);
   __syncthreads();
   const int64_t r = j0 + nb + blockIdx.x * (int64_t)nt + tid;
   if (r >= M) return;
   double* row = H + r * ldh + j0;
+  // the row itself, loaded up front
+  for (int c = 0; c < nb; ++c) xs[c * nt + tid] = row[c];
   for (int c = 0; c < nb; ++c) {
-    double s = row[c];
+    double s = xs[c * nt + tid];
     for (int t = 0; t < c; ++t) s -= xs[t * nt + tid] * L[c][t];
     xs[c * nt + tid] = s / L[c][c];
   }
   for (int c = 0; c < nb; ++c) row[c] = xs[c * nt + tid];
 }
 
-// trailing update A22 -= L21 L21^T on 64 x 64 tiles of the lower triangle;
-// the 64-wide panel is staged in two 32-column halves (static smem < 48 KB)
-__global__ void __launch_bounds__(256) syrk_update_kernel(double* __restrict__ H, int64_t ldh, int64_t M, int64_t j0,
-                                                          int nb) {
-  __shared__ double Ai[kNB][33];
-  __shared__ double Aj[kNB][33];
+// trailing update A22 -= L21 L21^T on 64 x 64 tiles of the lower triangle.
+// 128 threads, 8 x 4 outputs each; the panel is staged k-major in two
+// 32-column halves so that a thread's 8 (and 4) operands are consecutive in
+// shared memory (16-byte loads; rows padded to 66 doubles).
+constexpr int kSyrkThreads = 128;
+__global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __restrict__ H, int64_t ldh, int64_t M,
+                                                                   int64_t j0, int nb) {
+  __shared__ __align__(16) double As[32][kNB + 2];
+  __shared__ __align__(16) double Bs[32][kNB + 2];
   const int64_t s0 = j0 + nb;  // first trailing row
   // blockIdx.x enumerates lower tiles (ti >= tj) in row-major order
   int64_t t = blockIdx.x, ti = 0;
@@ -103,32 +124,46 @@ __global__ void __launch_bounds__(256) syrk_update_kernel(double* __restrict__ H
   const int64_t tj = t;
   const int64_t r0 = s0 + ti * kNB, c0 = s0 + tj * kNB;
   const int tid = threadIdx.x;
-  const int tr = (tid / 16) * 4, tc = (tid % 16) * 4;
-  double acc[4][4] = {};
+  const int tr = (tid >> 4) * 8, tc = (tid & 15) * 4;
+  double acc[8][4];
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
   for (int k0 = 0; k0 < nb; k0 += 32) {
     const int kc = min(32, nb - k0);
     __syncthreads();
-    for (int e = tid; e < kNB * 32; e += 256) {
-      const int i = e / 32, k = e % 32;
-      Ai[i][k] = (r0 + i < M && k < kc) ? H[(r0 + i) * ldh + j0 + k0 + k] : 0.0;
-      Aj[i][k] = (c0 + i < M && k < kc) ? H[(c0 + i) * ldh + j0 + k0 + k] : 0.0;
+#pragma unroll 4
+    for (int e = tid; e < kNB * 32; e += kSyrkThreads) {
+      const int i = e >> 5, k = e & 31;
+      As[k][i] = (r0 + i < M && k < kc) ? H[(r0 + i) * ldh + j0 + k0 + k] : 0.0;
+      Bs[k][i] = (c0 + i < M && k < kc) ? H[(c0 + i) * ldh + j0 + k0 + k] : 0.0;
     }
     __syncthreads();
     for (int k = 0; k < kc; ++k) {
-      double a[4], b[4];
+      double a[8], b[4];
+      const double2* pa = reinterpret_cast<const double2*>(&As[k][tr]);
+      const double2* pb = reinterpret_cast<const double2*>(&Bs[k][tc]);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        a[u] = Ai[tr + u][k];
-        b[u] = Aj[tc + u][k];
+        const double2 x = pa[u];
+        a[2 * u] = x.x;
+        a[2 * u + 1] = x.y;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 2; ++u) {
+        const double2 x = pb[u];
+        b[2 * u] = x.x;
+        b[2 * u + 1] = x.y;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
     }
   }
 #pragma unroll
-  for (int u = 0; u < 4; ++u)
+  for (int u = 0; u < 8; ++u)
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int64_t i = r0 + tr + u, j = c0 + tc + v;
@@ -143,24 +178,26 @@ __global__ void tri_block_kernel(const double* __restrict__ L, int64_t ldh, int6
   __shared__ double Lb[kNB][kNB + 1];
   __shared__ double v[kNB];
   const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e % nb;
-    Lb[i][j] = (j <= i) ? L[(k0 + i) * ldh + k0 + j] : 0.0;
-  }
+  load_lower<kNB + 1>(L, ldh, k0, k0, nb, Lb);
   if (tid < nb) v[tid] = x[k0 + tid];
   __syncthreads();
-  if (tid == 0) {
+  if (tid < 32) {  // one warp: each step's dot product across the lanes
+    const int lane = tid;
     if (mode == 0) {
       for (int c = 0; c < nb; ++c) {
-        double s = v[c];
-        for (int t = 0; t < c; ++t) s -= Lb[c][t] * v[t];
-        v[c] = s / Lb[c][c];
+        double s = 0.0;
+        for (int t = lane; t < c; t += 32) s += Lb[c][t] * v[t];
+        s = warp_sum(s);
+        if (lane == 0) v[c] = (v[c] - s) / Lb[c][c];
+        __syncwarp();
       }
     } else {
       for (int c = nb - 1; c >= 0; --c) {
-        double s = v[c];
-        for (int t = c + 1; t < nb; ++t) s -= Lb[t][c] * v[t];
-        v[c] = s / Lb[c][c];
+        double s = 0.0;
+        for (int t = c + 1 + lane; t < nb; t += 32) s += Lb[t][c] * v[t];
+        s = warp_sum(s);
+        if (lane == 0) v[c] = (v[c] - s) / Lb[c][c];
+        __syncwarp();
       }
     }
   }
@@ -313,7 +350,7 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
         H, ldh, M, j0, nb);
     RB_LAUNCH_CHECK();
     const int64_t T = ceil_div(rest, kNB);
-    syrk_update_kernel<<<(unsigned)(T * (T + 1) / 2), 256, 0, st>>>(H, ldh, M, j0, nb);
+    syrk_update_kernel<<<(unsigned)(T * (T + 1) / 2), kSyrkThreads, 0, st>>>(H, ldh, M, j0, nb);
     RB_LAUNCH_CHECK();
   }
   int herr = 0;
@@ -328,14 +365,14 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
   cudaStream_t st = as_stream(stream);
   for (int64_t k0 = 0; k0 < M; k0 += kNB) {  // L y = b
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
-    tri_block_kernel<<<1, 64, 0, st>>>(L, ldh, k0, nb, x, 0);
+    tri_block_kernel<<<1, 256, 0, st>>>(L, ldh, k0, nb, x, 0);
     const int64_t rest = M - k0 - nb;
     if (rest > 0) fwd_update_kernel<<<(unsigned)ceil_div(rest, 8), 256, 0, st>>>(L, ldh, M, k0, nb, x);
     RB_LAUNCH_CHECK();
   }
   for (int64_t k0 = ((M - 1) / kNB) * kNB; k0 >= 0; k0 -= kNB) {  // L^T x = y
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
-    tri_block_kernel<<<1, 64, 0, st>>>(L, ldh, k0, nb, x, 1);
+    tri_block_kernel<<<1, 256, 0, st>>>(L, ldh, k0, nb, x, 1);
     if (k0 > 0) bwd_update_kernel<<<(unsigned)ceil_div(k0, 256), 256, 0, st>>>(L, ldh, k0, nb, x);
     RB_LAUNCH_CHECK();
   }
