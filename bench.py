@@ -353,8 +353,19 @@ def run_gn_step(cfg, mesh, world, args):
         stages[name] = stages.get(name, 0.0) + e0.elapsed_time(e1)
         return r
 
+    def apply_update(prop, dmu):
+        """runrecon's update (mua, and D through musp: D = 1/(3(mua+musp)))."""
+        nn = prop.shape[0]
+        d_old = 1.0 / (3.0 * (prop[:, 0] + prop[:, 1]))
+        prop[:, 0] += dmu[:nn]
+        prop[:, 1] = 1.0 / (3.0 * (d_old + dmu[nn:2 * nn])) - prop[:, 0]
+
+    state = {"phi": None}
+
     def step_mixed():
-        det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg))
+        # one iteration of the GN loop: the forward solve starts from the
+        # previous iterate's fields, and the update is applied at the end
+        det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg, x0=state["phi"]))
         J, K = timed_stage("jacobian", lambda: engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact"))
         y = det.cpu().numpy().ravel()
         mis = data - y
@@ -384,25 +395,32 @@ def run_gn_step(cfg, mesh, world, args):
 
         dmu = timed_stage("solve_jty", solve_apply)
         del J, H
+        apply_update(gcfg["prop"], dmu)
+        state["phi"] = phi
         return dmu
 
-    # warm-up, then timed steps (device time, CUDA events around each stage)
+    # warm-up (GN iteration 1, from zero fields), then timed iterations 2..
+    # (device time, CUDA events around each stage); the state before the last
+    # timed iteration is kept for the FP64 form
     step_mixed()
     torch.cuda.synchronize()
     stages.clear()
     ks = max(1, min(args.steps, 2))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(ks):
+    for i in range(ks):
+        if i == ks - 1:
+            snap = (gcfg["prop"].copy(), state["phi"])
         dmu_mixed = step_mixed()
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
     mixed_stages = {k: round(v / ks, 2) for k, v in stages.items()}
 
-    # plain FP64 form
+    # plain FP64 form of the same GN iteration (same state, same warm start)
     def step_fp64():
-        det, phi, _, _, _ = forward_device(gcfg, precision="fp64")
+        gcfg["prop"] = snap[0].copy()
+        det, phi, _, _, _ = forward_device(gcfg, precision="fp64", x0=snap[1])
         cols, det0, ndet, psrc, pdet, _, _ = engine.pair_map(sd)
         nn = mesh.nn
         K = 2 * nn
@@ -453,7 +471,8 @@ def run_gn_step(cfg, mesh, world, args):
         pk = json.load(open(p)).get("bf16_tflops")
     return {
         "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
-                    f"mua+D nodal (K={2 * mesh.nn})",
+                    f"mua+D nodal (K={2 * mesh.nn}); GN iterations 2..{ks + 1} of the loop (forward warm-started "
+                    f"from the previous iterate's fields), iteration 1 untimed",
         "iters_per_s": round(1e3 / ms, 4) * world, "ms_per_iter": round(ms, 1), "breakdown_ms": mixed_stages,
         "fp64_iters_per_s": round(1e3 / ms64, 4) * world if ms64 else None,
         "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,

@@ -182,6 +182,8 @@ typedef struct rb_solve_opts {
   double tol;          /* target max relative residual ||b-Ax||/||b|| */
   double inner_tol;    /* relative residual of each FP32 correction solve */
   int32_t profile;     /* nonzero: time the Krylov kernels with CUDA events */
+  int32_t use_x0;      /* nonzero: X holds an initial guess (e.g. the previous
+                          Gauss-Newton iterate's fields); zero: start from 0 */
 } rb_solve_opts;
 
 typedef struct rb_solve_info {

@@ -1153,7 +1153,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
 #undef RB_CN
   RB_LAUNCH_CHECK();
   fin_bnorm_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os);
-  RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
+  if (!o.use_x0) RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
   launches += 2;
   const double stall = 0.25;
   KernelTimer tm;

@@ -383,27 +383,36 @@ DEFAULT_TOL = 1e-15
 
 
 def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=2000, max_outer=10,
-          check_every=10, profile=False):
+          check_every=10, profile=False, x0=None):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
     Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
     corrections inside FP64 iterative refinement; ``'fp64'``: the same loop
     entirely in FP64.  Up to 128 columns per library call; wider B is solved
-    in column blocks."""
+    in column blocks.  ``x0`` (nn x k, the solution's dtype) is an initial
+    guess: the refinement starts from its FP64 residual instead of from zero."""
     prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
     n, k = B.shape
     xdt = torch.complex128 if mat.is_complex else torch.float64
-    X = torch.empty((n, k), dtype=xdt, device=B.device)
+    if x0 is not None:
+        if tuple(x0.shape) != (n, k):
+            raise ValueError("x0 must have the shape of B")
+        X = x0.to(device=B.device, dtype=xdt).contiguous().clone()
+    else:
+        X = torch.empty((n, k), dtype=xdt, device=B.device)
     info = {"iters": 0, "outer": 0, "flag": 0, "launches": 0, "relres": 0.0, "spmm_ms": 0.0, "update_ms": 0.0,
             "spmm_launches": 0, "update_launches": 0}
     if prec == _lib.RB_FP64 and inner_tol > 1e-6:
         inner_tol = max(tol, 1e-15)
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
-                            int(bool(profile)))
+                            int(bool(profile)), int(x0 is not None))
     for c0 in range(0, k, 128):
         kb = min(128, k - c0)
         Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
-        Xb = torch.empty((n, kb), dtype=xdt, device=B.device) if (c0 or kb != k) else X
+        if c0 or kb != k:
+            Xb = X[:, c0:c0 + kb].contiguous() if x0 is not None else torch.empty((n, kb), dtype=xdt, device=B.device)
+        else:
+            Xb = X
         wb = _lib.lib().rb_femsolve_work_bytes(n, mat.struct.nnz, kb, int(mat.is_complex), prec)
         work = torch.empty(wb, dtype=torch.uint8, device=B.device)
         inf = _lib.RbSolveInfo()

@@ -25,7 +25,7 @@ def _check_single_wavelength(cfg):
         raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
 
 
-def forward_device(cfg, mode=1, **kwargs):
+def forward_device(cfg, mode=1, x0=None, **kwargs):
     """One forward pass kept on the device: returns (detval, phi, optodes,
     matrix, solve-info) with detval (ndet x nsrc) and phi (nn x (nsrc+ndet))
     as CUDA tensors.  The order matches runforward: femrhs, femlhs, femsolve,
@@ -35,7 +35,7 @@ def forward_device(cfg, mode=1, **kwargs):
     opt = engine.locate_optodes(mesh, cfg)
     B = opt.rhs(mesh)
     mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode))
-    phi, info = engine.solve(mat, B, **solver_options(kwargs))
+    phi, info = engine.solve(mat, B, x0=x0, **solver_options(kwargs))
     det = engine.getdet(mesh, opt, phi)
     return det, phi, opt, mat, info
 

@@ -162,6 +162,9 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     jac_mode = kwargs.get("jac_mode", "reference" if param == "mua" else "exact")
     gram_prec = kwargs.get("gram", "tf32")
     lambda_rule = kwargs.get("lambda_rule", "fixed")
+    # each forward solve starts from the previous iterate's fields (the
+    # refinement then only removes what the property update changed)
+    warm_start = kwargs.get("warm_start", True)
     if kwargs.get("prior") or "lmat" in kwargs or "ltl" in kwargs:
         raise NotImplementedError("structural priors are outside this engine's scope")
     if "param" in recon or isinstance(recon.get("prop"), dict):
@@ -185,7 +188,8 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     for it in range(maxiter):
         t0 = time.time()
         cfg, recon = syncprop(cfg, recon)
-        det, phi, _, _, _ = forward_device(cfg, **solverflag)
+        det, phi, _, _, _ = forward_device(cfg, x0=phi if (warm_start and phi is not None) else None,
+                                           **solverflag)
         mesh = engine.mesh_of(cfg)
         J, K = engine.jacobian_matrix(mesh, phi, sd, params, jac_mode)
         y = det.cpu().numpy().ravel()
