@@ -97,7 +97,8 @@ __device__ __forceinline__ cdouble acc_add(cdouble a, cdouble b) { return make_d
 
 // Block-reduce per-lane column accumulators acc[V] (lane l owns columns
 // l*V..) into part[blockIdx.x * k + c].
-template <typename A, int L, int V>
+// With S column slices, group g of the block owns slice g % S.
+template <typename A, int L, int V, int S = 1>
 __device__ __forceinline__ void block_colreduce(const A (&acc)[V], A* __restrict__ part, int64_t k,
                                                 A* sm /* kBlk * V */) {
   const int lane = threadIdx.x % L, grp = threadIdx.x / L;
@@ -105,11 +106,11 @@ __device__ __forceinline__ void block_colreduce(const A (&acc)[V], A* __restrict
 #pragma unroll
   for (int j = 0; j < V; ++j) sm[(grp * L + lane) * V + j] = acc[j];
   __syncthreads();
-  for (int c = threadIdx.x; c < L * V; c += kBlk) {
+  for (int c = threadIdx.x; c < S * L * V; c += kBlk) {
     if (c < k) {
-      const int l = c / V, j = c % V;
+      const int sl = c / (L * V), l = (c % (L * V)) / V, j = c % V;
       A s = acc_zero<A>();
-      for (int g = 0; g < G; ++g) s = acc_add(s, sm[(g * L + l) * V + j]);
+      for (int g = sl; g < G; g += S) s = acc_add(s, sm[(g * L + l) * V + j]);
       part[(int64_t)blockIdx.x * k + c] = s;
     }
   }
@@ -131,7 +132,11 @@ enum { EPI_STORE = 0, EPI_PQDOT = 1, EPI_RESID = 2 };
 
 // y_row = A_row x; EPI_STORE: Y = y; EPI_PQDOT: Y = y, acc += x_row*y (unconj);
 // EPI_RESID: Y = B - y, acc += |B - y|^2   (B real FP64)
-template <typename T, int L, int V, int EPI>
+// S column slices (S = 1, or 2 for complex64 at 128 columns): a lane group
+// takes (row, slice) tasks, slice = task % S, so that a lane keeps 16 bytes
+// per gathered row and 8 gathers in flight; the group count is a multiple of
+// S, so a group always sees the same slice (and its column sums stay put).
+template <typename T, int L, int V, int EPI, int S = 1>
 __global__ void __launch_bounds__(kBlk, BpsSpmm<T>::value)
 spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
             const T* __restrict__ val, const T* __restrict__ X, T* __restrict__ Y,
@@ -141,13 +146,15 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   A* part = reinterpret_cast<A*>(part_);
   __shared__ A sm[(EPI == EPI_STORE) ? 1 : kBlk * V];
   const int lane = threadIdx.x % L;
-  const int64_t c0 = (int64_t)lane * V;
+  const int64_t task0 = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L;
+  const int64_t c0 = (task0 % S) * (int64_t)(L * V) + (int64_t)lane * V;
   const bool on = c0 < k;
   const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
   alignas(16) A acc[V];
 #pragma unroll
   for (int j = 0; j < V; ++j) acc[j] = acc_zero<A>();
-  for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
+  for (int64_t task = task0; task < n * S; task += groups) {
+    const int64_t row = task / S;
     const int32_t b = indptr[row], e = indptr[row + 1];
     alignas(16) T y[V];
 #pragma unroll
@@ -167,7 +174,7 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
         // with copies of the row's last entry taken with coefficient 0 (same
         // NaN behaviour as the exact product) rather than falling back to
         // one dependent load at a time.
-        constexpr int U = (sizeof(T) <= 4) ? 8 : 4;
+        constexpr int U = (V * sizeof(T) <= 16) ? 8 : 4;
         for (int j = 0; j < cnt; j += U) {
           int32_t ii[U];
           T aa[U];
@@ -228,7 +235,7 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
       stv<T, V>(Y + row * k + c0, y);
     }
   }
-  if (EPI != EPI_STORE) block_colreduce<A, L, V>(acc, part, k, sm);
+  if (EPI != EPI_STORE) block_colreduce<A, L, V, S>(acc, part, k, sm);
 }
 
 // ------------------------------------------------ row-group SpMM (k = 32 V)
@@ -874,6 +881,7 @@ colnorm_kernel(int64_t n, int64_t k, const double* __restrict__ B, double* __res
 struct Shape {
   int L, V;
   unsigned grid;
+  int S = 1;  // column slices of the SpMM (see spmm_kernel)
 };
 
 static int64_t num_sms() {
@@ -897,6 +905,23 @@ static Shape pick_shape(int64_t n, int64_t k, int bps) {
   return s;
 }
 
+// SpMM shape: complex64 at 128 columns takes two 64-column slices (2 values
+// of 8 bytes per lane, 8 gathers in flight), measured 23% faster per launch
+// than one slice of 4 values with 4 gathers in flight
+template <typename T>
+static Shape pick_spmm_shape(int64_t n, int64_t k) {
+  if (std::is_same<T, cfloat>::value && k == 128) {
+    Shape s;
+    s.L = 32;
+    s.V = 2;
+    s.S = 2;
+    s.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(num_sms() * BpsSpmm<T>::value,
+                                                               ceil_div(2 * n, kBlk / s.L)));
+    return s;
+  }
+  return pick_shape(n, k, BpsSpmm<T>::value);
+}
+
 #define RB_DISPATCH_LV(sh, FN)                       \
   switch (sh.L * 8 + sh.V) {                         \
     case 4 * 8 + 1: FN(4, 1); break;                 \
@@ -917,6 +942,12 @@ static Shape pick_shape(int64_t n, int64_t k, int bps) {
 template <typename T, int EPI>
 int spmm_t(const rb_csr& A, const T* val, const T* X, T* Y, const double* B, void* part, int64_t k,
            const Shape& sh, cudaStream_t st) {
+  if (sh.S == 2) {
+    if (sh.L != 32 || sh.V != 2 || k != 128) return fail(RB_EARG, "bad sliced SpMM shape");
+    spmm_kernel<T, 32, 2, EPI, 2><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+    RB_LAUNCH_CHECK();
+    return RB_OK;
+  }
 #define RB_SPMM(L_, V_) \
   spmm_kernel<T, L_, V_, EPI><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part)
   RB_DISPATCH_LV(sh, RB_SPMM);
@@ -1141,7 +1172,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
                        const GroupPlan* gp, cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
-  const Shape shs = pick_shape(n, k, BpsSpmm<T>::value); // inner SpMM
+  const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
   const Shape sh64 = pick_shape(n, k, Bps<T64>::value);  // FP64 residual kernels
   const unsigned fg = (unsigned)ceil_div(k, 8);
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
