@@ -245,7 +245,9 @@ enum rb_jac_what { RB_JAC_MUA_REF = 0, RB_JAC_MUA_NODAL = 1, RB_JAC_D = 2 };
 /* extra out_kind values for complex phi: real FP32 / FP64 output with the
  * real parts in rows 0..nsd-1 and the imaginary parts in rows nsd..2nsd-1
  * (matreform 'real' stacking, redbirdpy/recon.py:532-546) */
-enum rb_jac_split { RB_JAC_SPLIT_F32 = 4, RB_JAC_SPLIT_F64 = 5 };
+enum rb_jac_split { RB_JAC_SPLIT_F32 = 4, RB_JAC_SPLIT_F64 = 5,
+                    RB_JAC_SPLIT_BF16 = 6, /* split rows rounded to BF16 (GN step in BF16) */
+                    RB_JAC_BF16 = 7 /* real rows rounded to BF16 */ };
 int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
@@ -276,6 +278,9 @@ int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, co
  *                              rb_split_tf32) H = hi hi^T + hi lo^T + lo hi^T,
  *                              close to FP32-input accuracy at 3x the work.
  *                              J: M x K FP32 rows, ldj % 4 == 0, 16-B aligned.
+ *                              rb_gram_bf16: J stored as BF16 (kind::f16 with
+ *                              BF16 A and B), ldj % 8 == 0: half the bytes and
+ *                              twice the tensor rate of TF32.
  *   H += lambda I, normalise   rb_reginv_prepare (_normalize_diag, recon.py:784-789)
  *   H = L L^T                  rb_cholesky (FP64, in place, lower)
  *   L L^T x = b                rb_chol_solve (in place on x)
@@ -284,6 +289,8 @@ int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, co
 size_t rb_gram_work_bytes(void);
 int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha,
             double* H, int64_t ldh, void* work, size_t work_bytes, void* stream);
+int rb_gram_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
+                 void* work, size_t work_bytes, void* stream);
 int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* stream);
 int rb_reginv_prepare(double* H, int64_t M, int64_t ldh, double lambda, double* di, void* stream);
 size_t rb_cholesky_work_bytes(void);
@@ -292,9 +299,13 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
 size_t rb_gemv_t_work_bytes(int64_t K);
 int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha,
               double beta, double* out, void* work, size_t work_bytes, void* stream);
+int rb_gemv_t_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha,
+                   double beta, double* out, void* work, size_t work_bytes, void* stream);
 size_t rb_sumsq_work_bytes(void);
 int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
              size_t work_bytes, void* stream);
+int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
+                  size_t work_bytes, void* stream);
 int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream);
 
 #ifdef __cplusplus

@@ -20,7 +20,7 @@ RB_F64, RB_C128, RB_F32, RB_C64 = range(4)
 RB_PROP_NODE, RB_PROP_ELEM = 0, 1
 RB_MIXED, RB_FP64 = 0, 1
 RB_JAC_MUA_REF, RB_JAC_MUA_NODAL, RB_JAC_D = 0, 1, 2
-RB_JAC_SPLIT_F32, RB_JAC_SPLIT_F64 = 4, 5
+RB_JAC_SPLIT_F32, RB_JAC_SPLIT_F64, RB_JAC_SPLIT_BF16, RB_JAC_BF16 = 4, 5, 6, 7
 
 _i64, _i32, _vp, _dbl, _sz = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_double, ctypes.c_size_t
 
@@ -81,6 +81,7 @@ _SIGS = {
     "rb_jac_elem": (ctypes.c_int, [ctypes.POINTER(RbMesh), _vp, _vp, _i32, _i64, _vp, _vp, _i64, _vp, _vp]),
     "rb_gram_work_bytes": (_sz, []),
     "rb_gram": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp]),
+    "rb_gram_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp]),
     "rb_split_tf32": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
     "rb_reginv_prepare": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _vp, _vp]),
     "rb_cholesky_work_bytes": (_sz, []),
@@ -88,8 +89,10 @@ _SIGS = {
     "rb_chol_solve": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
     "rb_gemv_t_work_bytes": (_sz, [_i64]),
     "rb_gemv_t": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
+    "rb_gemv_t_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
     "rb_sumsq_work_bytes": (_sz, []),
     "rb_sumsq": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
+    "rb_sumsq_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "rb_vec_mul": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp]),
 }
 

@@ -7,6 +7,8 @@
 //   sum(J^2)              (Frobenius block scaling, recon.py:235)   (sumsq)
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "rb_common.cuh"
 
 namespace rb {
@@ -231,7 +233,12 @@ __global__ void bwd_update_kernel(const double* __restrict__ L, int64_t ldh, int
 // last kernel adds the slabs in fixed order (deterministic, no atomics).
 constexpr int kGemvSlabs = 16;
 
-__global__ void gemv_t_part_kernel(const float* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+__device__ __forceinline__ double jval(float v) { return v; }
+__device__ __forceinline__ double jval(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// J stored as FP32 or BF16 (JT)
+template <typename JT>
+__global__ void gemv_t_part_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
                                    const double* __restrict__ y, double* __restrict__ part) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= K) return;
@@ -240,12 +247,12 @@ __global__ void gemv_t_part_kernel(const float* __restrict__ J, int64_t M, int64
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int64_t m = m0;
   for (; m + 3 < m1; m += 4) {
-    s0 = fma((double)J[m * ldj + k], y[m], s0);
-    s1 = fma((double)J[(m + 1) * ldj + k], y[m + 1], s1);
-    s2 = fma((double)J[(m + 2) * ldj + k], y[m + 2], s2);
-    s3 = fma((double)J[(m + 3) * ldj + k], y[m + 3], s3);
+    s0 = fma(jval(J[m * ldj + k]), y[m], s0);
+    s1 = fma(jval(J[(m + 1) * ldj + k]), y[m + 1], s1);
+    s2 = fma(jval(J[(m + 2) * ldj + k]), y[m + 2], s2);
+    s3 = fma(jval(J[(m + 3) * ldj + k]), y[m + 3], s3);
   }
-  for (; m < m1; ++m) s0 = fma((double)J[m * ldj + k], y[m], s0);
+  for (; m < m1; ++m) s0 = fma(jval(J[m * ldj + k]), y[m], s0);
   part[blockIdx.y * K + k] = (s0 + s1) + (s2 + s3);
 }
 
@@ -259,13 +266,14 @@ __global__ void gemv_t_sum_kernel(const double* __restrict__ part, int slabs, in
 }
 
 // per-block partial sums of J^2
-__global__ void sumsq_kernel(const float* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+template <typename JT>
+__global__ void sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
                              double* __restrict__ part) {
   __shared__ double red[32];
   double s = 0.0;
   for (int64_t m = blockIdx.x; m < M; m += gridDim.x)
     for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-      const double v = J[m * ldj + k];
+      const double v = jval(J[m * ldj + k]);
       s += v * v;
     }
   s = warp_sum(s);
@@ -381,18 +389,35 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
 
 size_t rb_gemv_t_work_bytes(int64_t K) { return (size_t)kGemvSlabs * K * sizeof(double) + 256; }
 
-int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
-              double* out, void* work, size_t work_bytes, void* stream) {
+}  // extern "C"
+
+template <typename JT>
+static int gemv_t_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
+                      double* out, void* work, size_t work_bytes, void* stream) {
   if (!J || !y || !out || !work || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_t: bad arguments");
   if (work_bytes < rb_gemv_t_work_bytes(K)) return fail(RB_EARG, "rb_gemv_t: workspace too small");
   cudaStream_t st = as_stream(stream);
   const int slabs = (int)std::min<int64_t>(kGemvSlabs, M);
   double* part = reinterpret_cast<double*>(work);
-  gemv_t_part_kernel<<<dim3((unsigned)ceil_div(K, 256), (unsigned)slabs), 256, 0, st>>>(J, M, K, ldj, y, part);
+  gemv_t_part_kernel<JT><<<dim3((unsigned)ceil_div(K, 256), (unsigned)slabs), 256, 0, st>>>(J, M, K, ldj, y, part);
   RB_LAUNCH_CHECK();
   gemv_t_sum_kernel<<<(unsigned)ceil_div(K, 256), 256, 0, st>>>(part, slabs, K, alpha, beta, out);
   RB_LAUNCH_CHECK();
   return RB_OK;
+}
+
+extern "C" {
+
+
+int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
+              double* out, void* work, size_t work_bytes, void* stream) {
+  return gemv_t_run(J, M, K, ldj, y, alpha, beta, out, work, work_bytes, stream);
+}
+
+int rb_gemv_t_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
+                   double* out, void* work, size_t work_bytes, void* stream) {
+  return gemv_t_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, y, alpha, beta, out, work, work_bytes,
+                    stream);
 }
 
 int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream) {
@@ -413,18 +438,34 @@ int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* 
 
 size_t rb_sumsq_work_bytes(void) { return 148 * 8 * sizeof(double) + 256; }
 
-int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
-             void* stream) {
+}  // extern "C"
+
+template <typename JT>
+static int sumsq_run(const JT* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
+                     void* stream) {
   if (!J || !out || !work || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_sumsq: bad arguments");
   if (work_bytes < rb_sumsq_work_bytes()) return fail(RB_EARG, "rb_sumsq: workspace too small");
   cudaStream_t st = as_stream(stream);
   const int nb = 148 * 8;
   double* part = reinterpret_cast<double*>(work);
-  sumsq_kernel<<<nb, 256, 0, st>>>(J, M, K, ldj, part);
+  sumsq_kernel<JT><<<nb, 256, 0, st>>>(J, M, K, ldj, part);
   RB_LAUNCH_CHECK();
   sum_parts_kernel<<<1, 1024, 0, st>>>(part, nb, out);
   RB_LAUNCH_CHECK();
   return RB_OK;
+}
+
+extern "C" {
+
+
+int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
+             void* stream) {
+  return sumsq_run(J, M, K, ldj, out, work, work_bytes, stream);
+}
+
+int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
+                  void* stream) {
+  return sumsq_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, out, work, work_bytes, stream);
 }
 
 }  // extern "C"

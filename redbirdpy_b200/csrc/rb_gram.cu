@@ -27,7 +27,7 @@ namespace rb {
 constexpr int kGM = 256;   // tile rows (A, two MMA halves of 128)
 constexpr int kGMH = 128;  // rows per MMA / per TMA box
 constexpr int kGN = 256;   // tile columns (B rows)
-constexpr int kGK = 32;    // FP32 elements per 128-byte row of a stage
+constexpr int kGK = 32;    // FP32 elements per 128-byte row of a stage (64 for BF16)
 constexpr int kGStages = 3;
 constexpr int kGABytes = kGM * kGK * 4;  // 32 KB
 constexpr int kGBBytes = kGN * kGK * 4;  // 32 KB
@@ -45,6 +45,7 @@ constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators (rows 0
 // four times fewer drains.
 constexpr int kGChunk = 128;
 constexpr int kGChunkTf32 = 512;
+constexpr int kGChunkBf16 = 256;  // the same 16384 K with 64 BF16 elements per K-block
 constexpr long long kGWaitLimit = 1LL << 24;  // polls before a wait gives up (seconds)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -96,9 +97,12 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   return d;
 }
 
-// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 256
+// instruction descriptor: D = F32, both operands K-major, M = 128, N = 256;
+// A = B = TF32 (kind::tf32, format 2) or A = B = BF16 (kind::f16, format 1)
 constexpr uint32_t kGIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kGN >> 3) << 17) |
                              ((uint32_t)(kGMH >> 4) << 24);
+constexpr uint32_t kGIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGN >> 3) << 17) |
+                                 ((uint32_t)(kGMH >> 4) << 24);
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -106,6 +110,16 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t 
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
       "l"(a), "l"(b), "r"(kGIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+// both operands BF16 (one type for A and B, as kind::f16 requires)
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kGIdescBf16), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
       : "memory");
 }
 
@@ -119,6 +133,8 @@ __device__ __host__ __forceinline__ int64_t gram_col_tiles(int64_t bj, int64_t n
   return need < nbi ? need : nbi;
 }
 
+// BF16: J stored as BF16 (64 elements per 128-byte stage row), one pass
+template <bool BF16>
 __global__ void __launch_bounds__(kGThreads, 1)
 gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_lo, int segs,
                  int64_t M, int64_t K, double* __restrict__ H, int64_t ldh, double alpha, int* __restrict__ err) {
@@ -158,9 +174,10 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   const uint32_t tmem = *tmem_slot;
   // segs == 1: H = J J^T.  segs == 3 (split precision, J = hi + lo):
   // H = hi hi^T + hi lo^T + lo hi^T, one K sweep per product, one accumulator
-  const int nk1 = (int)((K + kGK - 1) / kGK);
+  constexpr int kE = BF16 ? 2 * kGK : kGK;  // elements per 128-byte stage row
+  const int nk1 = (int)((K + kE - 1) / kE);
   const int nk = nk1 * segs;
-  const int chunk = (segs == 1) ? kGChunkTf32 : kGChunk;  // K-blocks between drains
+  const int chunk = BF16 ? kGChunkBf16 : (segs == 1) ? kGChunkTf32 : kGChunk;  // K-blocks between drains
 
   if (warp == 0) {
     if (lane == 0) {
@@ -170,7 +187,7 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         const uint32_t a = smem_u32(sm + s * kGStageBytes);
         const uint32_t b = a + kGABytes;
         const uint32_t bar = smem_u32(&full[s]);
-        const int seg = kb / nk1, kx = (kb - seg * nk1) * kGK;
+        const int seg = kb / nk1, kx = (kb - seg * nk1) * kE;
         const CUtensorMap* ma = (seg == 2) ? &tmap_lo : &tmap;
         const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
         mbar_expect_tx(bar, kGStageBytes);
@@ -194,11 +211,16 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         const uint32_t a = smem_u32(sm + s * kGStageBytes);
         const uint32_t b = a + kGABytes;
 #pragma unroll
-        for (int k = 0; k < kGK / 8; ++k) {  // kind::tf32 consumes K = 8 (32 bytes) per MMA
+        for (int k = 0; k < 4; ++k) {  // 32 bytes of K per MMA: 8 TF32 or 16 BF16 elements
           const uint64_t bd = umma_desc_sw128(b + 32 * k);
           const uint32_t acc = !(first && k == 0);
-          umma_tf32(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
-          umma_tf32(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+          if constexpr (BF16) {
+            umma_bf16(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
+            umma_bf16(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+          } else {
+            umma_tf32(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
+            umma_tf32(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+          }
         }
         umma_commit(smem_u32(&empty[s]));
         if (last) umma_commit(smem_u32(tfull));
@@ -288,14 +310,15 @@ static EncodeTiledFn encode_fn() {
 
 using namespace rb;
 
-static int make_map(CUtensorMap* map, const float* J, int64_t M, int64_t K, int64_t ldj) {
+static int make_map(CUtensorMap* map, const void* J, int64_t M, int64_t K, int64_t ldj, bool bf16 = false) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fail(RB_ECUDA, "rb_gram: cuTensorMapEncodeTiled unavailable");
   cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)M};
-  cuuint64_t gstride[1] = {(cuuint64_t)ldj * sizeof(float)};
-  cuuint32_t box[2] = {(cuuint32_t)kGK, (cuuint32_t)kGMH};
+  cuuint64_t gstride[1] = {(cuuint64_t)ldj * (bf16 ? 2 : 4)};
+  cuuint32_t box[2] = {(cuuint32_t)(bf16 ? 2 * kGK : kGK), (cuuint32_t)kGMH};
   cuuint32_t estride[2] = {1, 1};
-  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(J), gdim, gstride, box, estride,
+  CUresult r = enc(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                   const_cast<void*>(J), gdim, gstride, box, estride,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RB_ECUDA, "rb_gram: cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -306,17 +329,18 @@ extern "C" {
 
 size_t rb_gram_work_bytes(void) { return 256; }
 
-int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
-            void* work, size_t work_bytes, void* stream) {
+static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_t K, int64_t ldj, double alpha,
+                    double* H, int64_t ldh, void* work, size_t work_bytes, void* stream) {
   if (!J || !H || !work || M < 1 || K < 1 || ldj < K || ldh < M)
     return fail(RB_EARG, "rb_gram: bad arguments");
   if (work_bytes < rb_gram_work_bytes()) return fail(RB_EARG, "rb_gram: workspace too small");
-  if ((reinterpret_cast<uintptr_t>(J) & 15) || (Jlo && (reinterpret_cast<uintptr_t>(Jlo) & 15)) || (ldj % 4))
-    return fail(RB_EARG, "rb_gram: J must be 16-byte aligned with a row stride that is a multiple of 4 floats");
+  const int64_t lda = bf16 ? 8 : 4;  // elements per 16 bytes
+  if ((reinterpret_cast<uintptr_t>(J) & 15) || (Jlo && (reinterpret_cast<uintptr_t>(Jlo) & 15)) || (ldj % lda))
+    return fail(RB_EARG, "rb_gram: J must be 16-byte aligned with a row stride that is a multiple of 16 bytes");
   if (M > (int64_t)1 << 30 || K > (int64_t)1 << 30) return fail(RB_ESIZE, "rb_gram: matrix too large");
   CUtensorMap map, map_lo;
-  RB_TRY(make_map(&map, J, M, K, ldj));
-  RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj));
+  RB_TRY(make_map(&map, J, M, K, ldj, bf16));
+  RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj, bf16));
   const int segs = Jlo ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   int* err = reinterpret_cast<int*>(work);
@@ -324,8 +348,13 @@ int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj,
   const int64_t nbi = ceil_div(M, kGM), nbj = ceil_div(M, kGN);
   int64_t tiles = 0;
   for (int64_t bj = 0; bj < nbj; ++bj) tiles += gram_col_tiles(bj, nbi);
-  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-  gram_tf32_kernel<<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, K, H, ldh, alpha, err);
+  if (bf16) {
+    RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+    gram_tf32_kernel<true><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, K, H, ldh, alpha, err);
+  } else {
+    RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+    gram_tf32_kernel<false><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, K, H, ldh, alpha, err);
+  }
   RB_LAUNCH_CHECK();
   dim3 mg((unsigned)ceil_div(M, 32), (unsigned)ceil_div(M, 32));
   mirror_upper_kernel<<<mg, dim3(32, 8), 0, st>>>(H, M, ldh);
@@ -335,6 +364,16 @@ int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj,
   RB_CUDA_TRY(cudaStreamSynchronize(st));
   if (herr) return fail(RB_ECUDA, "rb_gram: pipeline wait timed out (stage %d)", herr);
   return RB_OK;
+}
+
+int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
+            void* work, size_t work_bytes, void* stream) {
+  return gram_run(J, Jlo, false, M, K, ldj, alpha, H, ldh, work, work_bytes, stream);
+}
+
+int rb_gram_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh, void* work,
+                 size_t work_bytes, void* stream) {
+  return gram_run(J, nullptr, true, M, K, ldj, alpha, H, ldh, work, work_bytes, stream);
 }
 
 }  // extern "C"

@@ -14,6 +14,8 @@
 // multiply-adds: J[k][n] = sum_a phi_s(k)[a] C_n[a][d(k)].  Threads that
 // write one row segment are consecutive, so the nsd x nn output (the
 // dominant HBM traffic) is written in full sectors.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 #include "rb_common.cuh"
@@ -100,7 +102,29 @@ __host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, i
   return jac_layout<C>(TN, rmax, nc, ndet, emax).total;
 }
 
-template <typename C, typename In, int TN, bool SPLIT, bool GRID>
+// one Jacobian entry: complex values split into a real-part and an
+// imaginary-part row block (SPLIT), optionally rounded to BF16 (BF)
+template <typename C, bool SPLIT, bool BF>
+__device__ __forceinline__ void jac_store(void* Jout, int64_t nsd, int64_t ldj, int64_t k, int64_t n, C v) {
+  typedef typename JacT<C>::real R;
+  if constexpr (SPLIT) {
+    if constexpr (BF) {
+      __nv_bfloat16* Jb = reinterpret_cast<__nv_bfloat16*>(Jout);
+      Jb[k * ldj + n] = __float2bfloat16_rn(v.x);
+      Jb[(nsd + k) * ldj + n] = __float2bfloat16_rn(v.y);
+    } else {
+      R* Jr = reinterpret_cast<R*>(Jout);
+      Jr[k * ldj + n] = v.x;
+      Jr[(nsd + k) * ldj + n] = v.y;
+    }
+  } else if constexpr (BF) {
+    reinterpret_cast<__nv_bfloat16*>(Jout)[k * ldj + n] = __float2bfloat16_rn(v);
+  } else {
+    reinterpret_cast<C*>(Jout)[k * ldj + n] = v;
+  }
+}
+
+template <typename C, typename In, int TN, bool SPLIT, bool GRID, bool BF>
 __global__ void __launch_bounds__(kJacThreads)
 jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   typedef typename JacT<C>::real R;
@@ -239,13 +263,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int64_t k = (int64_t)(db * 4 + v) * nsu + sb * 4 + u;
-          if constexpr (SPLIT) {
-            R* Jr = reinterpret_cast<R*>(Jout);
-            Jr[k * a.ldj + n] = acc[u][v].x;
-            Jr[(a.nsd + k) * a.ldj + n] = acc[u][v].y;
-          } else {
-            reinterpret_cast<C*>(Jout)[k * a.ldj + n] = acc[u][v];
-          }
+          jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n, acc[u][v]);
         }
     }
     return;
@@ -262,15 +280,9 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     const C* Cn = sC + (size_t)t * SC + pd;
     C s = s_zero(C());
     for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
-    if constexpr (SPLIT) {
-      // complex rows split into a block of real parts and a block of
-      // imaginary parts (matreform 'real', recon.py:532-546)
-      R* Jr = reinterpret_cast<R*>(Jout);
-      Jr[k * a.ldj + n] = s.x;
-      Jr[(a.nsd + k) * a.ldj + n] = s.y;
-    } else {
-      reinterpret_cast<C*>(Jout)[k * a.ldj + n] = s;
-    }
+    // complex rows are split into a block of real parts and a block of
+    // imaginary parts (matreform 'real', recon.py:532-546)
+    jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n, s);
   }
 }
 
@@ -300,7 +312,7 @@ __global__ void jac_elem_kernel(const double* __restrict__ evol, const int32_t* 
   }
 }
 
-template <typename C, typename In, bool SPLIT, bool GRID>
+template <typename C, typename In, bool SPLIT, bool GRID, bool BF>
 static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   int TN = 8;
   const size_t budget = 110 * 1024;
@@ -310,9 +322,9 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
   const unsigned g = (unsigned)ceil_div(a.nn, TN);
 #define RB_JL(TN_)                                                                                     \
   do {                                                                                                 \
-    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID>,                              \
+    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID, BF>,                          \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
-    jac_kernel<C, In, TN_, SPLIT, GRID><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);               \
+    jac_kernel<C, In, TN_, SPLIT, GRID, BF><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);           \
   } while (0)
   switch (TN) {
     case 8: RB_JL(8); break;
@@ -325,10 +337,10 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
   return RB_OK;
 }
 
-template <typename C, typename In, bool SPLIT = false>
+template <typename C, typename In, bool SPLIT = false, bool BF = false>
 static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
-  if (a.grid) return launch_jac_t<C, In, SPLIT, true>(a, phi, J, st);
-  return launch_jac_t<C, In, SPLIT, false>(a, phi, J, st);
+  if (a.grid) return launch_jac_t<C, In, SPLIT, true, BF>(a, phi, J, st);
+  return launch_jac_t<C, In, SPLIT, false, BF>(a, phi, J, st);
 }
 
 // lam[r][s] = sum_d phi[r][dcol0 + d] conj(g[det0_i + d][s]) for the instance i of row r
@@ -405,6 +417,16 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
   }
   cudaStream_t st = as_stream(stream);
   const bool cin = (phi_kind == RB_C128 || phi_kind == RB_C64);
+  if (out_kind == RB_JAC_SPLIT_BF16) {
+    if (!cin) return fail(RB_EARG, "rb_jac: split output needs complex phi");
+    return phi_kind == RB_C64 ? launch_jac<cfloat, cfloat, true, true>(a, phi, J, st)
+                              : launch_jac<cfloat, cdouble, true, true>(a, phi, J, st);
+  }
+  if (out_kind == RB_JAC_BF16) {
+    if (cin) return fail(RB_EARG, "rb_jac: BF16 rows need real phi (complex phi: RB_JAC_SPLIT_BF16)");
+    return phi_kind == RB_F32 ? launch_jac<float, float, false, true>(a, phi, J, st)
+                              : launch_jac<float, double, false, true>(a, phi, J, st);
+  }
   if (out_kind == RB_JAC_SPLIT_F32 || out_kind == RB_JAC_SPLIT_F64) {
     if (!cin) return fail(RB_EARG, "rb_jac: split output needs complex phi");
     if (out_kind == RB_JAC_SPLIT_F32)

@@ -506,9 +506,14 @@ def _pad4(n):
     return (n + 3) // 4 * 4
 
 
-def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference"):
-    """The real FP32 Jacobian of the GN step, rows x columns = (nsd or 2 nsd)
-    x (len(params) * nn), stored with a row stride padded to 4 floats.
+def _pad8(n):
+    return (n + 7) // 8 * 8
+
+
+def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torch.float32):
+    """The real Jacobian of the GN step (FP32, or BF16 with ``dtype``), rows x
+    columns = (nsd or 2 nsd) x (len(params) * nn), stored with a row stride
+    padded to 16 bytes.
     Complex fields give matreform 'real' stacking [Re; Im] (recon.py:532-546).
     mode 'reference' = redbirdpy's jac for mua (forward.py:509-569);
     'exact' = derivatives of the node-based assembly ('mua' at fixed D, 'D')."""
@@ -517,9 +522,13 @@ def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference"):
     cplx = phi.is_complex()
     rows = 2 * nsd if cplx else nsd
     nn = mesh.nn
-    ldj = _pad4(len(params) * nn)
-    J = torch.zeros((rows, ldj), dtype=torch.float32, device=phi.device)
-    out_kind = _lib.RB_JAC_SPLIT_F32 if cplx else _lib.RB_F32
+    bf = dtype == torch.bfloat16
+    ldj = _pad8(len(params) * nn) if bf else _pad4(len(params) * nn)
+    J = torch.zeros((rows, ldj), dtype=dtype, device=phi.device)
+    if bf:
+        out_kind = _lib.RB_JAC_SPLIT_BF16 if cplx else _lib.RB_JAC_BF16
+    else:
+        out_kind = _lib.RB_JAC_SPLIT_F32 if cplx else _lib.RB_F32
     phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
                 torch.complex64: _lib.RB_C64}[phi.dtype]
     colsd, ps, pd = _i32(cols, phi.device), _i32(psrc, phi.device), _i32(pdet, phi.device)
@@ -541,17 +550,23 @@ def sumsq(J, K):
     out = torch.empty(1, dtype=torch.float64, device=J.device)
     wb = _lib.lib().rb_sumsq_work_bytes()
     work = torch.empty(wb, dtype=torch.uint8, device=J.device)
-    call("rb_sumsq", ptr(J), J.shape[0], K, J.shape[1], ptr(out), ptr(work), wb, stream())
+    fn = "rb_sumsq_bf16" if J.dtype == torch.bfloat16 else "rb_sumsq"
+    call(fn, ptr(J), J.shape[0], K, J.shape[1], ptr(out), ptr(work), wb, stream())
     return out
 
 
 def gram(J, K, alpha=1.0, precision="tf32"):
     """H = alpha J J^T (M x M FP64) on the tensor cores.  precision 'tf32'
     (one pass) or 'tf32x3' (split hi/lo, three passes; J is left as hi and
-    the returned lo completes it)."""
+    the returned lo completes it); a BF16 J takes the BF16 MMA."""
     M, ldj = J.shape
     H = torch.empty((M, M), dtype=torch.float64, device=J.device)
     lo = None
+    if J.dtype == torch.bfloat16:
+        wb = _lib.lib().rb_gram_work_bytes()
+        work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+        call("rb_gram_bf16", ptr(J), M, K, ldj, float(alpha), ptr(H), M, ptr(work), wb, stream())
+        return H, None
     if precision == "tf32x3":
         lo = torch.empty_like(J)
         call("rb_split_tf32", ptr(J), ptr(lo), M, K, ldj, stream())
@@ -595,7 +610,8 @@ def gemv_t(J, K, y, alpha=1.0, beta=0.0, out=None, lo=None):
         out = torch.empty(K, dtype=torch.float64, device=dev)
     wb = _lib.lib().rb_gemv_t_work_bytes(K)
     work = torch.empty(wb, dtype=torch.uint8, device=dev)
-    call("rb_gemv_t", ptr(J), M, K, ldj, ptr(y), float(alpha), float(beta), ptr(out), ptr(work), wb, stream())
+    fn = "rb_gemv_t_bf16" if J.dtype == torch.bfloat16 else "rb_gemv_t"
+    call(fn, ptr(J), M, K, ldj, ptr(y), float(alpha), float(beta), ptr(out), ptr(work), wb, stream())
     if lo is not None:  # J = hi + lo
         call("rb_gemv_t", ptr(lo), M, K, ldj, ptr(y), float(alpha), 1.0, ptr(out), ptr(work), wb, stream())
     return out

@@ -191,7 +191,8 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
         det, phi, _, _, _ = forward_device(cfg, x0=phi if (warm_start and phi is not None) else None,
                                            **solverflag)
         mesh = engine.mesh_of(cfg)
-        J, K = engine.jacobian_matrix(mesh, phi, sd, params, jac_mode)
+        J, K = engine.jacobian_matrix(mesh, phi, sd, params, jac_mode,
+                                      dtype=torch.bfloat16 if gram_prec == "bf16" else torch.float32)
         y = det.cpu().numpy().ravel()
         misfit = y0 - y
         if np.iscomplexobj(misfit) or np.iscomplexobj(y0):
@@ -228,5 +229,6 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
             break
     recon["lambda"] = lambda_
     Jout = J[:, :K]
-    Jout = Jout.cpu().numpy() if Jout.numel() * 4 < 2 ** 31 else Jout
+    if Jout.numel() * 4 < 2 ** 31:
+        Jout = Jout.float().cpu().numpy()
     return recon, resid, cfg, updates, {"mua": Jout}, det.cpu().numpy(), phi.cpu().numpy()

@@ -71,3 +71,25 @@ def test_kuhn_box_counts():
     node, elem = kuhn_box([100, 100, 50], 1)
     assert node.shape == (520251, 3) and elem.shape == (3000000, 4)
     assert elem.min() == 1 and elem.max() == 520251
+
+
+def test_batch_boxes_workload():
+    """The uneven-instance workload generator: seeded, extents multiples of
+    the spacing, optode counts and properties in their ranges."""
+    from redbirdpy_b200.meshgen import batch_boxes
+
+    a = batch_boxes(12, seed=2)
+    b = batch_boxes(12, seed=2)
+    for x, y in zip(a, b):
+        assert np.array_equal(x["node"], y["node"]) and np.array_equal(x["prop"], y["prop"])
+    for c in a:
+        node, elem = c["node"], c["elem"]
+        ext = node.max(axis=0) - node.min(axis=0)
+        h = np.diff(np.unique(node[:, 0]))[0]
+        assert h in (2.0, 3.0, 4.0)
+        assert np.allclose(ext / h, np.rint(ext / h)) and np.all(ext >= 2 * h)
+        assert elem.min() == 1 and elem.max() == node.shape[0]
+        assert 4 <= c["srcpos"].shape[0] <= 16 and 4 <= c["detpos"].shape[0] <= 16
+        assert np.all((c["prop"][:, 0] >= 0.005) & (c["prop"][:, 0] <= 0.03))
+        assert np.all((c["prop"][:, 1] >= 0.5) & (c["prop"][:, 1] <= 2.0))
+        assert np.all(c["srcpos"][:, 2] == 0) and np.all(c["srcpos"][:, :2] >= h)

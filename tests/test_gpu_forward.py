@@ -298,3 +298,26 @@ def test_label_properties_expand_on_device(golden):
     idx = np.clip(seg, 0, 1)
     np.testing.assert_array_equal(o.mua.cpu().numpy(), cfg2["prop"][idx, 0])
     np.testing.assert_array_equal(o.musp.cpu().numpy(), cfg2["prop"][idx, 1] * (1 - cfg2["prop"][idx, 2]))
+
+
+def test_femsolve_warm_start(golden):
+    """An initial guess (the Gauss-Newton warm start) changes the iteration
+    count, not the answer: from the solution itself the solve ends at once."""
+    from redbirdpy_b200 import engine as eng
+
+    g = golden("nodal_fd")
+    cfg = cfg_from(g)
+    mesh = eng.mesh_of(cfg)
+    opt = eng.locate_optodes(mesh, cfg)
+    B = opt.rhs(mesh)
+    mat = eng.assemble(mesh, eng.Optics.from_cfg(mesh, cfg))
+    x_cold, i_cold = eng.solve(mat, B)
+    x_same, i_same = eng.solve(mat, B, x0=x_cold)
+    assert i_same["iters"] == 0 and i_same["flag"] == 0
+    assert torch.equal(x_same, x_cold)
+    x_pert = x_cold * (1 + 0.01 * torch.rand_like(x_cold.real))
+    x_warm, i_warm = eng.solve(mat, B, x0=x_pert)
+    assert i_warm["flag"] == 0 and i_warm["iters"] < i_cold["iters"]
+    assert (torch.abs(x_warm - x_cold).max() / torch.abs(x_cold).max()).item() < 1e-12
+    with pytest.raises(ValueError):
+        eng.solve(mat, B, x0=x_cold[:, :3])

@@ -138,3 +138,59 @@ def test_runrecon_residual_decreases_fd_mua_and_d(golden):
                                                   param="mua+D", lambda_rule="maxdiag")
     assert resid[-1] < 0.5 * resid[0], resid
     assert "dcoeff" in upd[0] and upd[0]["mua"].shape == (nn,)
+
+
+def _bf16_rows(A):
+    """A (numpy) as BF16 device rows with a 16-byte row stride, and the
+    FP64 values of the rounded entries."""
+    M, K = A.shape
+    ldj = (K + 7) // 8 * 8
+    J = torch.zeros((M, ldj), dtype=torch.bfloat16, device="cuda")
+    J[:, :K] = torch.as_tensor(A, dtype=torch.float32, device="cuda").to(torch.bfloat16)
+    return J, K, J[:, :K].double().cpu().numpy()
+
+
+@pytest.mark.parametrize("M,K", [(8, 40), (300, 1000), (513, 2048), (1024, 40000)])
+def test_gram_bf16_tensor_cores(M, K):
+    """BF16 rows through the kind::f16 MMA: against FP64 products of the same
+    rounded entries (what remains is the FP32 accumulation)."""
+    rng = np.random.default_rng(M + K)
+    J, Kc, Ar = _bf16_rows(rng.standard_normal((M, K)))
+    H, _ = engine.gram(J, Kc, 0.5)
+    H = H.cpu().numpy()
+    ref = 0.5 * (Ar @ Ar.T)
+    assert np.abs(H - ref).max() / np.abs(ref).max() < 1e-3
+    assert np.array_equal(H, H.T)
+    # the other BF16 pieces of the GN step
+    s = engine.sumsq(J, Kc).item()
+    assert abs(s - (Ar ** 2).sum()) <= 1e-12 * (Ar ** 2).sum()
+    y = rng.standard_normal(M)
+    out = engine.gemv_t(J, Kc, torch.as_tensor(y, device="cuda"), 2.0).cpu().numpy()
+    np.testing.assert_allclose(out, 2.0 * (Ar.T @ y), rtol=1e-10, atol=1e-12 * np.abs(Ar.T @ y).max())
+
+
+@pytest.mark.parametrize("case", ["nodal_cw", "nodal_fd"])
+def test_jacobian_bf16_rows(golden, case):
+    g = golden(case)
+    cfg = cfg_from(g)
+    mesh = engine.mesh_of(cfg)
+    phi = torch.as_tensor(g["phi"], device="cuda")
+    sd = g["sd"]
+    J32, K = engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact")
+    J16, K16 = engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact", dtype=torch.bfloat16)
+    assert K16 == K and J16.shape[1] % 8 == 0
+    a, b = J32[:, :K].double(), J16[:, :K].double()
+    assert (torch.abs(a - b) <= 2.0 ** -8 * torch.abs(a) + 1e-30).all()
+
+
+def test_runrecon_bf16_matches_reference(golden):
+    g, m = golden("nodal_gn"), golden("nodal_cw")
+    cfg = cfg_from(m)
+    cfg["prop"] = g["prop0"].copy()
+    recon = {"prop": g["prop0"].copy()}
+    recon, resid, cfg, upd, J, det, phi = rbb.run(cfg, recon, g["detphi0"], m["sd"], maxiter=2, lambda_=0.05,
+                                                  report=False, gram="bf16")
+    np.testing.assert_allclose(resid, g["resid"], rtol=1e-2)
+    for k, key in enumerate(("dmu0", "dmu1")):
+        ref = g[key]
+        assert np.abs(upd[k]["mua"] - ref).max() / np.abs(ref).max() < 3e-2, key
