@@ -229,8 +229,19 @@ class Optics:
                                     self.nref_scalar, self.omega, self.reff)
 
     @staticmethod
-    def from_cfg(mesh, cfg, mode=1):
-        props = np.atleast_2d(np.asarray(cfg["prop"], dtype=np.float64))
+    def from_cfg(mesh, cfg, mode=1, wv=""):
+        """femlhs's property selection (forward.py:105-144): with dicts keyed
+        by wavelength, ``prop``, ``reff`` and ``omega`` of wavelength ``wv``."""
+        prop = cfg["prop"]
+        reff = cfg.get("reff", 0.493)
+        omega = cfg.get("omega", 0)
+        if isinstance(prop, dict):
+            if not wv:
+                raise ValueError("per-wavelength properties need a wavelength")
+            prop = prop[wv]
+            reff = reff[wv] if isinstance(reff, dict) else reff
+            omega = omega.get(wv, 0) if isinstance(omega, dict) else omega
+        props = np.atleast_2d(np.asarray(prop, dtype=np.float64))
         nn, ne = mesh.nn, mesh.ne
         if props.shape[0] in (nn, ne):
             mua = props[:, 0]
@@ -250,8 +261,7 @@ class Optics:
             nref = props[l0, 3] if props.shape[1] >= 4 else 1.37
         else:
             raise ValueError("Property format not recognized")
-        omega = 0.0 if mode == 2 else float(cfg.get("omega", 0) or 0)
-        reff = cfg.get("reff", 0.493)
+        omega = 0.0 if mode == 2 else float(omega or 0)
         return Optics(mesh, mua, musp, nref, omega, reff)
 
 
@@ -357,10 +367,10 @@ class Optodes:
         return loc, bary
 
 
-def locate_optodes(mesh, cfg):
+def locate_optodes(mesh, cfg, wv=""):
     from .utility import getoptodes
 
-    src, det, wsrc, wdet = getoptodes(cfg)
+    src, det, wsrc, wdet = getoptodes(cfg, wv)
     if (wsrc is not None and np.size(wsrc)) or (wdet is not None and np.size(wdet)):
         raise NotImplementedError("wide-field sources/detectors are outside this engine's scope")
     parts = [p for p in (src, det) if p is not None]

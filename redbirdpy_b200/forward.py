@@ -20,21 +20,22 @@ __all__ = ["runforward", "femlhs", "femrhs", "femgetdet", "jac", "C0", "forward_
 C0 = engine.C0
 
 
-def _check_single_wavelength(cfg):
-    if isinstance(cfg.get("prop"), dict):
-        raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
+def _wavelengths(cfg):
+    """The wavelength keys of per-wavelength properties, or [''] (forward.py:52-54)."""
+    prop = cfg.get("prop")
+    return list(prop.keys()) if isinstance(prop, dict) else [""]
 
 
-def forward_device(cfg, mode=1, x0=None, **kwargs):
+def forward_device(cfg, mode=1, x0=None, wv="", **kwargs):
     """One forward pass kept on the device: returns (detval, phi, optodes,
     matrix, solve-info) with detval (ndet x nsrc) and phi (nn x (nsrc+ndet))
     as CUDA tensors.  The order matches runforward: femrhs, femlhs, femsolve,
-    femgetdet (redbirdpy/forward.py:66-75)."""
-    _check_single_wavelength(cfg)
+    femgetdet (redbirdpy/forward.py:66-75); ``wv`` selects the wavelength of
+    per-wavelength properties."""
     mesh = engine.mesh_of(cfg)
-    opt = engine.locate_optodes(mesh, cfg)
+    opt = engine.locate_optodes(mesh, cfg, wv)
     B = opt.rhs(mesh)
-    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode))
+    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode, wv))
     phi, info = engine.solve(mat, B, x0=x0, **solver_options(kwargs))
     det = engine.getdet(mesh, opt, phi)
     return det, phi, opt, mat, info
@@ -50,11 +51,19 @@ def runforward(cfg, **kwargs):
         rfcw = [rfcw]
     if cfg.get("deldotdel") is None:
         cfg["deldotdel"] = engine.mesh_of(cfg).deldotdel_host()
-    det_out, phi_out = {}, {}
-    for md in rfcw:
-        det, phi, _, _, info = forward_device(cfg, mode=md, **kwargs)
-        det_out[md] = {"detphi": det.cpu().numpy()}
-        phi_out[md] = {"phi": engine.host_pool.to_numpy(phi)}
+    wavelengths = _wavelengths(cfg)
+    det_out = {md: {"detphi": {}} for md in rfcw}
+    phi_out = {md: {"phi": {}} for md in rfcw}
+    for wv in wavelengths:
+        for md in rfcw:
+            det, phi, _, _, info = forward_device(cfg, mode=md, wv=wv, **kwargs)
+            det_out[md]["detphi"][wv] = det.cpu().numpy()
+            phi_out[md]["phi"][wv] = engine.host_pool.to_numpy(phi)
+    # the reference's nesting: modes, then wavelengths, each level dropped when single
+    if len(wavelengths) == 1:
+        for md in rfcw:
+            det_out[md]["detphi"] = det_out[md]["detphi"][wavelengths[0]]
+            phi_out[md]["phi"] = phi_out[md]["phi"][wavelengths[0]]
     if len(rfcw) == 1:
         return det_out[rfcw[0]]["detphi"], phi_out[rfcw[0]]["phi"]
     return det_out, phi_out
@@ -65,12 +74,11 @@ def femlhs(cfg, deldotdel_mat=None, wavelength="", mode=1):
 
     Assembled on the GPU from ``deldotdel_mat`` (as the reference does;
     None = the mesh's own, computed on the GPU) and ``cfg['evol']``."""
-    _check_single_wavelength(cfg)
     mesh = engine.mesh_of(cfg)
     ddd = None
     if deldotdel_mat is not None and deldotdel_mat is not cfg.get("deldotdel"):
         ddd = torch.as_tensor(np.ascontiguousarray(deldotdel_mat, dtype=np.float64), device=mesh.device)
-    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode), ddd=ddd)
+    mat = engine.assemble(mesh, engine.Optics.from_cfg(mesh, cfg, mode, wavelength), ddd=ddd)
     A = mesh.csr_host(mat.val64)
     A.has_sorted_indices = True
     return A
@@ -80,9 +88,8 @@ def femrhs(cfg, sd=None, wv="", md=1):
     """Point-optode RHS ``(rhs, loc, bary, optode)`` (redbirdpy/forward.py:259-362):
     rhs is Nn x (Nsrc+Ndet) CSR with 4 barycentric weights per column, loc
     1-based (NaN outside the mesh)."""
-    _check_single_wavelength(cfg)
     mesh = engine.mesh_of(cfg)
-    opt = engine.locate_optodes(mesh, cfg)
+    opt = engine.locate_optodes(mesh, cfg, wv)
     nn = mesh.nn
     if opt.npts == 0:
         return sparse.csr_matrix((nn, 0)), np.array([]), np.array([]).reshape(0, 4), np.array([])

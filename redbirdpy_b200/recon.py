@@ -167,7 +167,7 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     warm_start = kwargs.get("warm_start", True)
     if kwargs.get("prior") or "lmat" in kwargs or "ltl" in kwargs:
         raise NotImplementedError("structural priors are outside this engine's scope")
-    if "param" in recon or isinstance(recon.get("prop"), dict):
+    if "param" in recon or isinstance(recon.get("prop"), dict) or isinstance(cfg.get("prop"), dict):
         raise NotImplementedError("multi-spectral reconstruction is outside this engine's scope")
     if "node" in recon and "elem" in recon and "mapid" in recon:
         raise NotImplementedError("dual-mesh reconstruction is outside this engine's scope")

@@ -122,9 +122,13 @@ def getbulk(cfg):
     prop = cfg.get("prop")
     if prop is None:
         return default
-    if isinstance(prop, dict):
-        raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
-    prop = np.atleast_2d(prop)
+    if isinstance(prop, dict):  # one bulk per wavelength (property.py:267-271)
+        return {wv: _bulk_from_prop(np.atleast_2d(p), cfg, default) for wv, p in prop.items()}
+    return _bulk_from_prop(np.atleast_2d(prop), cfg, default)
+
+
+def _bulk_from_prop(prop, cfg, default):
+    """The bulk row of one property table (property.py:275-332)."""
     nn = cfg["node"].shape[0]
     ne = cfg["elem"].shape[0]
     face = cfg.get("face")
@@ -156,8 +160,11 @@ def getbulk(cfg):
 
 
 def getltr(cfg, wv=""):
-    """Transport mean free path 1/(mua + musp) of the bulk (utility.py:862-876)."""
+    """Transport mean free path 1/(mua + musp) of the bulk (utility.py:862-876);
+    with per-wavelength properties, of wavelength ``wv`` (default: the first)."""
     bk = getbulk(cfg)
+    if isinstance(bk, dict):
+        bk = bk[wv if wv else next(iter(bk))]
     return 1.0 / (bk[0] + bk[1] * (1 - bk[2]))
 
 
@@ -210,8 +217,14 @@ def sdmap(cfg, maxdist=np.inf, **kwargs):
     if maxdist < np.inf:
         dist = getdistance(cfg["srcpos"], cfg["detpos"], badsrc, baddet)
         active = np.array([1.0 if dist[int(d) - ns, int(s)] < maxdist else 0.0 for s, d in sd])
-        return np.column_stack([sd, active])
-    return np.column_stack([sd, np.ones(len(sd))])
+        out = np.column_stack([sd, active])
+    else:
+        out = np.column_stack([sd, np.ones(len(sd))])
+    if isinstance(cfg.get("prop"), dict):
+        # one table per wavelength, with a fourth column of ones (utility.py:733-768)
+        out = np.column_stack([out, np.ones(len(out))])
+        return {wv: out.copy() for wv in cfg["prop"]}
+    return out
 
 
 def elem2node(elem, elemval, nodelen=None):
@@ -270,12 +283,16 @@ def meshprep(cfg):
         raise ValueError("cfg.srcpos is required")
     if "srcdir" not in cfg:
         raise ValueError("cfg.srcdir is required")
-    if isinstance(cfg.get("prop"), dict):
-        raise NotImplementedError("multi-wavelength prop dicts are outside this engine's scope")
+    if isinstance(cfg.get("prop"), dict) and "param" in cfg:
+        raise NotImplementedError("chromophore (multi-spectral 'param') properties are outside this engine's scope")
     if cfg.get("reff") is None:
         bk = getbulk(cfg)
-        cfg["reff"] = getreff(bk[3], 1.0)
-        cfg["musp0"] = bk[1] * (1 - bk[2])
+        if isinstance(bk, dict):  # per wavelength (utility.py:198-205)
+            cfg["reff"] = {wv: getreff(b[3], 1.0) for wv, b in bk.items()}
+            cfg["musp0"] = {wv: b[1] * (1 - b[2]) for wv, b in bk.items()}
+        else:
+            cfg["reff"] = getreff(bk[3], 1.0)
+            cfg["musp0"] = bk[1] * (1 - bk[2])
     srctype = cfg.get("srctype", "pencil")
     dettype = cfg.get("dettype", "pencil")
     if srctype not in ("pencil", "isotropic") or dettype not in ("pencil", "isotropic") \

@@ -90,9 +90,38 @@ def run_case(rb, cfg, with_jac=True):
     return out
 
 
+def multi_wavelength(rb):
+    """Per-wavelength properties (cfg['prop'] keyed by wavelength): meshprep's
+    reff per wavelength, runforward's detval / phi per wavelength."""
+    cfg = nodal_cfg()
+    p1 = cfg["prop"]
+    p2 = p1.copy()
+    p2[:, 0] *= 1.5
+    p2[:, 1] *= 0.8
+    p2[:, 3] = 1.40
+    cfg["prop"] = {"690": p1, "830": p2}
+    cfg, sd = rb.meshprep(cfg)
+    det, phi = rb.run(cfg)
+    out = dict(node=cfg["node"], elem=cfg["elem"], face=cfg["face"], area=cfg["area"], evol=cfg["evol"],
+               deldotdel=cfg["deldotdel"], srcpos=cfg["srcpos"], detpos=cfg["detpos"], omega=cfg["omega"])
+    for wv in ("690", "830"):
+        out["prop_" + wv] = cfg["prop"][wv]
+        out["reff_" + wv] = cfg["reff"][wv]
+        out["detval_" + wv] = det[wv]
+        out["phi_" + wv] = phi[wv]
+        out["sd_" + wv] = sd[wv]
+    np.savez_compressed(os.path.join(HERE, "nodal_multiwl.npz"), **out)
+
+
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference"
     rb = load_reference(ref)
+    if "--only-multiwl" in sys.argv:
+        multi_wavelength(rb)
+        print("golden fixture written to", HERE)
+        return
+    multi_wavelength(rb)
     np.savez_compressed(os.path.join(HERE, "c1_cw.npz"), **run_case(rb, c1_cfg()))
     np.savez_compressed(os.path.join(HERE, "c1_fd.npz"),
                         **run_case(rb, c1_cfg(2 * np.pi * 1e8), with_jac=False))

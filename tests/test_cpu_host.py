@@ -93,3 +93,21 @@ def test_batch_boxes_workload():
         assert np.all((c["prop"][:, 0] >= 0.005) & (c["prop"][:, 0] <= 0.03))
         assert np.all((c["prop"][:, 1] >= 0.5) & (c["prop"][:, 1] <= 2.0))
         assert np.all(c["srcpos"][:, 2] == 0) and np.all(c["srcpos"][:, :2] >= h)
+
+
+def test_multi_wavelength_host_pieces(golden):
+    """Per-wavelength bulk, reff and sd tables (property.py:267-271,
+    utility.py:198-205, 733-760) against the reference's meshprep output."""
+    from redbirdpy_b200 import utility as u
+
+    g = golden("nodal_multiwl")
+    cfg = dict(node=g["node"], elem=g["elem"], face=g["face"], srcpos=g["srcpos"], detpos=g["detpos"],
+               prop={"690": g["prop_690"], "830": g["prop_830"]})
+    bk = u.getbulk(cfg)
+    assert set(bk) == {"690", "830"}
+    for wv in ("690", "830"):
+        assert u.getreff(bk[wv][3], 1.0) == pytest.approx(float(g["reff_" + wv]), rel=1e-14)
+        assert u.getltr(cfg, wv) == pytest.approx(1.0 / (bk[wv][0] + bk[wv][1] * (1 - bk[wv][2])))
+    sd = u.sdmap(cfg)
+    for wv in ("690", "830"):
+        assert np.array_equal(sd[wv], g["sd_" + wv])

@@ -321,3 +321,25 @@ def test_femsolve_warm_start(golden):
     assert (torch.abs(x_warm - x_cold).max() / torch.abs(x_cold).max()).item() < 1e-12
     with pytest.raises(ValueError):
         eng.solve(mat, B, x0=x_cold[:, :3])
+
+
+def test_multi_wavelength_forward_matches_reference(golden):
+    """cfg['prop'] keyed by wavelength: meshprep's per-wavelength reff and
+    runforward's per-wavelength detval / phi, as the reference returns them."""
+    g = golden("nodal_multiwl")
+    cfg = dict(node=g["node"].copy(), elem=g["elem"].copy(), srcpos=g["srcpos"], srcdir=np.array([[0, 0, 1.0]]),
+               detpos=g["detpos"], detdir=np.array([[0, 0, 1.0]]), omega=float(g["omega"]),
+               prop={"690": g["prop_690"].copy(), "830": g["prop_830"].copy()})
+    cfg, sd = rbb.meshprep(cfg)
+    assert isinstance(cfg["reff"], dict) and isinstance(sd, dict)
+    det, phi = rbb.run(cfg)
+    assert set(det) == {"690", "830"} and set(phi) == {"690", "830"}
+    for wv in ("690", "830"):
+        assert cfg["reff"][wv] == pytest.approx(float(g["reff_" + wv]), rel=1e-14)
+        ref = g["detval_" + wv]
+        assert det[wv].shape == ref.shape
+        assert np.max(np.abs(det[wv] - ref) / np.abs(ref)) <= 1e-6
+        assert np.abs(phi[wv] - g["phi_" + wv]).max() / np.abs(g["phi_" + wv]).max() <= 1e-9
+    # one wavelength's matrix through femlhs(cfg, ddd, wavelength)
+    A = rbb.femlhs(cfg, cfg["deldotdel"], "830")
+    assert A.shape == (cfg["node"].shape[0],) * 2
