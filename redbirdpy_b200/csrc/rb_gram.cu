@@ -137,7 +137,11 @@ __device__ __host__ __forceinline__ int64_t gram_col_tiles(int64_t bj, int64_t n
 template <bool BF16>
 __global__ void __launch_bounds__(kGThreads, 1)
 gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_lo, int segs,
-                 int64_t M, int64_t K, double* __restrict__ H, int64_t ldh, double alpha, int* __restrict__ err) {
+                 int64_t M, int64_t kbeg, int64_t kend, int accumulate, double* __restrict__ H, int64_t ldh,
+                 double alpha, int* __restrict__ err) {
+  // K range [kbeg, kend) of this launch; accumulate: add to H instead of
+  // writing its first partial sums
+  const int64_t K = kend - kbeg;
   extern __shared__ __align__(1024) unsigned char gsm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kGStages * kGStageBytes);
@@ -187,7 +191,7 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         const uint32_t a = smem_u32(sm + s * kGStageBytes);
         const uint32_t b = a + kGABytes;
         const uint32_t bar = smem_u32(&full[s]);
-        const int seg = kb / nk1, kx = (kb - seg * nk1) * kE;
+        const int seg = kb / nk1, kx = (int)kbeg + (kb - seg * nk1) * kE;
         const CUtensorMap* ma = (seg == 2) ? &tmap_lo : &tmap;
         const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
         mbar_expect_tx(bar, kGStageBytes);
@@ -261,7 +265,7 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
             for (int u = 0; u < 32; ++u)
               if ((int64_t)j0 + c0 + u < M) {
                 const double x = alpha * (double)__uint_as_float(v[u]);
-                dst[u] = (c == 0) ? x : dst[u] + x;
+                dst[u] = (c == 0 && !accumulate) ? x : dst[u] + x;
               }
           }
         }
@@ -348,14 +352,22 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
   const int64_t nbi = ceil_div(M, kGM), nbj = ceil_div(M, kGN);
   int64_t tiles = 0;
   for (int64_t bj = 0; bj < nbj; ++bj) tiles += gram_col_tiles(bj, nbi);
-  if (bf16) {
-    RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-    gram_tf32_kernel<true><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, K, H, ldh, alpha, err);
-  } else {
-    RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-    gram_tf32_kernel<false><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, K, H, ldh, alpha, err);
+  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  // K in ranges of 65536 per launch (a multiple of every stage row): a
+  // launch's CTAs stay close to each other in K, so more of the slab of J they
+  // share is still in L2 (measured 5-6% faster than one launch at K = 10^6)
+  const int64_t kspan = 65536;
+  for (int64_t kb = 0; kb < K; kb += kspan) {
+    const int64_t ke = std::min<int64_t>(K, kb + kspan);
+    if (bf16)
+      gram_tf32_kernel<true><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, kb, ke, kb > 0, H, ldh,
+                                                                          alpha, err);
+    else
+      gram_tf32_kernel<false><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, kb, ke, kb > 0, H,
+                                                                           ldh, alpha, err);
+    RB_LAUNCH_CHECK();
   }
-  RB_LAUNCH_CHECK();
   dim3 mg((unsigned)ceil_div(M, 32), (unsigned)ceil_div(M, 32));
   mirror_upper_kernel<<<mg, dim3(32, 8), 0, st>>>(H, M, ldh);
   RB_LAUNCH_CHECK();
