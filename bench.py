@@ -174,24 +174,24 @@ def run_b200(args):
     optics = engine.Optics.from_cfg(mesh, cfg)
     nrhs = cfg["srcpos"].shape[0] + cfg["detpos"].shape[0]
 
-    def step(precision, profile=False):
+    def step(precision, profile=False, coarse="auto"):
         opt = engine.locate_optodes(mesh, cfg)
         B = opt.rhs(mesh)
         mat = engine.assemble(mesh, optics)
-        X, info = engine.solve(mat, B, precision=precision, profile=profile)
+        X, info = engine.solve(mat, B, precision=precision, profile=profile, coarse=coarse)
         det = engine.getdet(mesh, opt, X)
         return det, X, info
 
-    def timed(precision, k, w, profile=False):
+    def timed(precision, k, w, profile=False, coarse="auto"):
         for _ in range(w):
-            step(precision)
+            step(precision, coarse=coarse)
         torch.cuda.synchronize()
         barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         infos = []
         for _ in range(k):
-            det, X, info = step(precision, profile)
+            det, X, info = step(precision, profile, coarse)
             infos.append(info)
         e1.record()
         torch.cuda.synchronize()
@@ -209,6 +209,8 @@ def run_b200(args):
     _, _, pinfos = timed("mixed", 2, 0, profile=True)
     # plain FP64 form, same GPU, same accuracy target
     ms_fp64, det_fp64, infos64 = timed("fp64", max(1, min(args.steps, 3)), 1)
+    # the same solve with the Jacobi preconditioner alone (no coarse space)
+    ms_jac, _, infos_jac = timed("mixed", max(1, min(args.steps, 3)), 1, coarse=False)
     d64 = det_fp64.cpu().numpy()
     dmx = det_mixed.cpu().numpy()
     rel_err = float(np.max(np.abs(dmx - d64) / np.abs(d64)))
@@ -269,13 +271,17 @@ def run_b200(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
         "config": {"workload": "box 100x100x50 mm, 1 mm Kuhn (520251 nodes, 3000000 tets), 64 src + 64 det, CW",
-                   "nnz": nnz, "nrhs": nrhs, "precision": "mixed (FP32 Jacobi-PCG in FP64 refinement)",
+                   "nnz": nnz, "nrhs": nrhs,
+                   "precision": "mixed (FP32 PCG in FP64 refinement; Jacobi + aggregation coarse space)",
                    "l2": "working set > L2 (5 x 266 MB vectors), no flush", "parallelism": f"replicas x{world}"},
         "fp64_value": round(world * nrhs / (ms_fp64 * 1e-3), 3), "fp64_ms_per_step": round(ms_fp64, 3),
         "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
         "det_max_rel_err_vs_fp64": rel_err,
         "krylov": {"iters": it["iters"], "sweeps": it["outer"], "relres": it["relres"], "flag": it["flag"],
-                   "fp64_iters": infos64[-1]["iters"]},
+                   "fp64_iters": infos64[-1]["iters"], "coarse_aggregates": it["coarse_nc"],
+                   "coarse_ms_per_iter": round(sum(i["coarse_ms"] for i in pinfos)
+                                               / max(1, sum(i["coarse_launches"] for i in pinfos)), 4),
+                   "jacobi_only_ms_per_step": round(ms_jac, 3), "jacobi_only_iters": infos_jac[-1]["iters"]},
         "gpu_launches": int(sum(i["launches"] for i in infos) / len(infos)) + 6,
         "roofline": {"bound": "hbm", "kernel": "spmm_kernel<float> (CSR SpMM, 128 RHS, fused p.Ap)",
                      "achieved": round(sp_gbs, 1) if sp_gbs else None, "peak": peak, "unit": "GB/s",

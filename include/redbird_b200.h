@@ -174,6 +174,36 @@ typedef struct rb_csr {
   int32_t is_complex;
 } rb_csr;
 
+/* Coarse space of the two-level preconditioner: the rows are grouped into nc
+ * aggregates (e.g. the mesh nodes binned by position).  With P the n x nc 0/1
+ * matrix of the grouping, the Krylov preconditioner becomes
+ *   z = D^-1 r + P (P^T A P)^-1 P^T r
+ * (Jacobi plus an exact solve of the aggregated operator, which removes the
+ * smooth error components Jacobi-CG converges on slowly).  P^T A P is built
+ * and inverted on the device once per rb_femsolve call.  Device arrays. */
+typedef struct rb_coarse {
+  int64_t nc;              /* aggregates, 1..4096; every aggregate nonempty */
+  const int32_t* agg;      /* n: aggregate of each row (0-based) */
+  const int32_t* agg_ptr;  /* nc + 1: offsets into agg_rows */
+  const int32_t* agg_rows; /* n: the rows of each aggregate, ascending */
+} rb_coarse;
+
+/* Workspace that a coarse space adds to rb_femsolve_work_bytes(). */
+size_t rb_coarse_work_bytes(int64_t nc, int64_t nrhs, int32_t is_complex, int32_t precision);
+
+/* Aggregates from node positions (node: nn x 3 FP64, device): node i falls
+ * in the cube (bx, by, bz) = floor((p - (x0, y0, z0)) / h), clamped to the
+ * nbx x nby x nbz grid; the nonempty cubes, numbered in cube order
+ * (x fastest), are the aggregates.  Writes agg (nn), agg_ptr (nc + 1; room
+ * for 4097) and agg_rows (nn, each aggregate's rows ascending), and *nc
+ * (host).  Deterministic.  RB_ESIZE when more than 4096 cubes are nonempty
+ * (*nc holds the count: take a larger h). */
+size_t rb_coarse_aggregate_work_bytes(int64_t nn, int64_t nbins);
+int rb_coarse_aggregate(const double* node, int64_t nn, double x0, double y0, double z0, double h,
+                        int32_t nbx, int32_t nby, int32_t nbz, int32_t* agg, int32_t* agg_ptr,
+                        int32_t* agg_rows, int64_t* nc /* host */, void* work, size_t work_bytes,
+                        void* stream);
+
 typedef struct rb_solve_opts {
   int32_t precision;   /* RB_MIXED: FP32 Krylov + FP64 refinement; RB_FP64 */
   int32_t max_outer;   /* refinement sweeps (mixed) */
@@ -184,6 +214,7 @@ typedef struct rb_solve_opts {
   int32_t profile;     /* nonzero: time the Krylov kernels with CUDA events */
   int32_t use_x0;      /* nonzero: X holds an initial guess (e.g. the previous
                           Gauss-Newton iterate's fields); zero: start from 0 */
+  const rb_coarse* coarse; /* host pointer; NULL: Jacobi preconditioner only */
 } rb_solve_opts;
 
 typedef struct rb_solve_info {
@@ -196,6 +227,8 @@ typedef struct rb_solve_info {
   double update_ms;    /* profile only: total time of the vector-update launches */
   int32_t spmm_launches;
   int32_t update_launches;
+  double coarse_ms;    /* profile only: total time of the coarse corrections */
+  int32_t coarse_launches; /* profile only: coarse corrections timed */
 } rb_solve_info;
 
 /* femsolve (redbirdpy/solver.py:385-948) for all columns at once: Jacobi-

@@ -42,14 +42,20 @@ class RbCsr(ctypes.Structure):
                 ("val32", _vp), ("dinv64", _vp), ("dinv32", _vp), ("is_complex", _i32)]
 
 
+class RbCoarse(ctypes.Structure):
+    _fields_ = [("nc", _i64), ("agg", _vp), ("agg_ptr", _vp), ("agg_rows", _vp)]
+
+
 class RbSolveOpts(ctypes.Structure):
     _fields_ = [("precision", _i32), ("max_outer", _i32), ("maxiter", _i32), ("check_every", _i32),
-                ("tol", _dbl), ("inner_tol", _dbl), ("profile", _i32), ("use_x0", _i32)]
+                ("tol", _dbl), ("inner_tol", _dbl), ("profile", _i32), ("use_x0", _i32),
+                ("coarse", ctypes.POINTER(RbCoarse))]
 
 
 class RbSolveInfo(ctypes.Structure):
     _fields_ = [("iters", _i32), ("outer", _i32), ("flag", _i32), ("launches", _i32), ("relres", _dbl),
-                ("spmm_ms", _dbl), ("update_ms", _dbl), ("spmm_launches", _i32), ("update_launches", _i32)]
+                ("spmm_ms", _dbl), ("update_ms", _dbl), ("spmm_launches", _i32), ("update_launches", _i32),
+                ("coarse_ms", _dbl), ("coarse_launches", _i32)]
 
 
 _SIGS = {
@@ -72,6 +78,10 @@ _SIGS = {
     "rb_adjoint_fields": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _vp, _vp]),
     "rb_femgetdet": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i64, _i64, _i32, _vp, _vp]),
     "rb_femsolve_work_bytes": (_sz, [_i64, _i64, _i64, _i32, _i32]),
+    "rb_coarse_work_bytes": (_sz, [_i64, _i64, _i32, _i32]),
+    "rb_coarse_aggregate_work_bytes": (_sz, [_i64, _i64]),
+    "rb_coarse_aggregate": (ctypes.c_int, [_vp, _i64, _dbl, _dbl, _dbl, _dbl, _i32, _i32, _i32, _vp, _vp, _vp,
+                                           ctypes.POINTER(_i64), _vp, _sz, _vp]),
     "rb_femsolve": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _vp, _i64, ctypes.POINTER(RbSolveOpts),
                                    ctypes.POINTER(RbSolveInfo), _vp, _sz, _vp]),
     "rb_csr_prepare": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _vp, _vp, _vp]),

@@ -554,11 +554,19 @@ template <> __device__ __forceinline__ cdouble from_c<cdouble>(cdouble v) { retu
 __device__ __forceinline__ cdouble to_c(double v) { return make_double2(v, 0.0); }
 __device__ __forceinline__ cdouble to_c(cdouble v) { return v; }
 
-// init: p = Dinv r; acc0 += r.p (unconj), acc1 += |r|^2; x = 0
+}  // namespace rb
+
+#include "rb_coarse.cuh"
+
+namespace rb {
+
+// init: p = z = Dinv r (+ ec[agg[row]], the coarse correction, when agg is
+// given); acc0 += r.p (unconj), acc1 += |r|^2; x = 0
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __restrict__ R, T* __restrict__ P,
-               T* __restrict__ Xs, typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
+               T* __restrict__ Xs, typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr,
+               const int32_t* __restrict__ agg, const T* __restrict__ ec) {
   typedef typename Scalar<T>::acc A;
   __shared__ A sm[kBlk * V];
   __shared__ double smr[kBlk * V];
@@ -573,11 +581,17 @@ cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __rest
   for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     if (!on) continue;
     const T d = dinv[row];
-    alignas(16) T r[V], p[V], z[V];
+    alignas(16) T r[V], p[V], z[V], e[V];
     ldv<T, V>(R + row * k + c0, r);
+    if (agg) {
+      ldv<T, V>(ec + (int64_t)agg[row] * k + c0, e);
+    } else {
+#pragma unroll
+      for (int j = 0; j < V; ++j) e[j] = s_zero(T());
+    }
 #pragma unroll
     for (int j = 0; j < V; ++j) {
-      p[j] = s_mul(d, r[j]);
+      p[j] = s_fma(d, r[j], e[j]);
       z[j] = s_zero(T());
       arz[j] = acc_fma(r[j], p[j], arz[j]);
       arr[j] += s_abs2(r[j]);
@@ -638,11 +652,12 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
   block_colreduce<double, L, V>(arr, part_rr, k, smr);
 }
 
-// p = Dinv r + beta p  (active columns only)
+// p = z + beta p, z = Dinv r (+ ec[agg[row]] with a coarse space)  (active columns only)
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
-                  const T* __restrict__ R, T* __restrict__ P) {
+                  const T* __restrict__ R, T* __restrict__ P, const int32_t* __restrict__ agg,
+                  const T* __restrict__ ec) {
   const int lane = threadIdx.x % L;
   const int64_t c0 = (int64_t)lane * V;
   if (c0 >= k) return;
@@ -658,12 +673,18 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
   if (!any) return;
   for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     const T d = dinv[row];
-    alignas(16) T r[V], p[V];
+    alignas(16) T r[V], p[V], e[V];
     ldv<T, V>(R + row * k + c0, r);
     ldv<T, V>(P + row * k + c0, p);
+    if (agg) {
+      ldv<T, V>(ec + (int64_t)agg[row] * k + c0, e);
+    } else {
+#pragma unroll
+      for (int j = 0; j < V; ++j) e[j] = s_zero(T());
+    }
 #pragma unroll
     for (int j = 0; j < V; ++j)
-      if (act[j]) p[j] = s_fma(be[j], p[j], s_mul(d, r[j]));
+      if (act[j]) p[j] = s_fma(be[j], p[j], s_fma(d, r[j], e[j]));
     stv<T, V>(P + row * k + c0, p);
   }
 }
@@ -738,13 +759,19 @@ __global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* 
   cs[c] = s;
 }
 
-// beta = rz_new / rz; convergence ||r|| <= tol ||r0||; counts active columns
+// beta = rz_new / rz; convergence ||r|| <= tol ||r0||; counts active columns.
+// With a coarse space rz_new adds the coarse part (P^T r).(X P^T r), whose
+// per-block partials are part_c (nbc blocks).
 template <typename A>
 __global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
-                                double tol2, int32_t* nactive) {
+                                double tol2, int32_t* nactive, const A* part_c, int nbc) {
   RB_FIN_WARP();
   if (!cs[c].active) return;
-  const cdouble rzn = sum_part<A>(part_rz, nb, k, c, lane);
+  cdouble rzn = sum_part<A>(part_rz, nb, k, c, lane);
+  if (part_c) {
+    const cdouble rc = sum_part<A>(part_c, nbc, k, c, lane);
+    rzn = make_double2(rzn.x + rc.x, rzn.y + rc.y);
+  }
   const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
   if (lane) return;
   ColState s = cs[c];
@@ -1073,8 +1100,9 @@ struct KernelTimer {
   bool on = false;
   std::vector<cudaEvent_t> ev;
   int used = 0;
-  double spmm_ms = 0, upd_ms = 0;
-  int spmm_n = 0, upd_n = 0;
+  double spmm_ms = 0, upd_ms = 0, coarse_ms = 0;
+  int spmm_n = 0, upd_n = 0, coarse_n = 0;
+  bool with_coarse = false;
   int ensure(int n) {
     while ((int)ev.size() < n) {
       cudaEvent_t e;
@@ -1089,17 +1117,23 @@ struct KernelTimer {
     RB_CUDA_TRY(cudaEventRecord(ev[used++], st));
     return RB_OK;
   }
-  // events come in triples: before spmm, after spmm, after update
+  // events come in fours: before spmm, after spmm, after update, after the
+  // coarse correction (restriction, coarse product, dot)
   int harvest() {
     if (!on) return RB_OK;
-    for (int i = 0; i + 2 < used; i += 3) {
-      float a = 0, b = 0;
+    for (int i = 0; i + 3 < used; i += 4) {
+      float a = 0, b = 0, c = 0;
       RB_CUDA_TRY(cudaEventElapsedTime(&a, ev[i], ev[i + 1]));
       RB_CUDA_TRY(cudaEventElapsedTime(&b, ev[i + 1], ev[i + 2]));
+      RB_CUDA_TRY(cudaEventElapsedTime(&c, ev[i + 2], ev[i + 3]));
       spmm_ms += a;
       upd_ms += b;
       spmm_n++;
       upd_n++;
+      if (with_coarse) {
+        coarse_ms += c;
+        coarse_n++;
+      }
     }
     used = 0;
     return RB_OK;
@@ -1115,12 +1149,20 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
                        double* part_b, T* Xs, T* R, T* P, T* Q, ColState* cs, const int32_t* enable,
                        const OuterState* os, int32_t* counter, double tol, int maxiter, int check_every,
                        int* iters_out,
-                       int* launches, KernelTimer& tm, const GroupPlan* gp, cudaStream_t st) {
+                       int* launches, KernelTimer& tm, const GroupPlan* gp, const CoarseOp<T>* co,
+                       cudaStream_t st) {
   typedef typename Scalar<T>::acc Acc;
   const int64_t n = A.n;
   const unsigned fg = (unsigned)ceil_div(k, 8);
+  const int32_t* agg = co ? co->agg : nullptr;
+  const T* ec = co ? co->ec : nullptr;
+  const Acc* part_c = co ? (const Acc*)co->part : nullptr;
+  if (co) {
+    RB_TRY(coarse_apply<T>(*co, R, k, st));
+    *launches += 3;
+  }
 #define RB_INIT(L_, V_) \
-  cg_init_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, dinv, R, P, Xs, (Acc*)part_a, part_b)
+  cg_init_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, dinv, R, P, Xs, (Acc*)part_a, part_b, agg, ec)
   RB_DISPATCH_LV(sh, RB_INIT);
 #undef RB_INIT
   RB_LAUNCH_CHECK();
@@ -1147,9 +1189,15 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       RB_TRY(tm.record(st));
+      if (co) {
+        RB_TRY(coarse_apply<T>(*co, R, k, st));
+        *launches += 3;
+      }
+      RB_TRY(tm.record(st));
       if (b == burst - 1) RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter);
-#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P)
+      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter, part_c,
+                                               kCdotGrid);
+#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P, agg, ec)
       RB_DISPATCH_LV(sh, RB_PUP);
 #undef RB_PUP
       RB_LAUNCH_CHECK();
@@ -1169,7 +1217,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
 template <typename T64, typename T>
 static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, int64_t k, const rb_solve_opts& o,
                        rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv,
-                       const GroupPlan* gp, cudaStream_t st) {
+                       const GroupPlan* gp, const CoarseOp<T>* co, cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
   const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
@@ -1189,6 +1237,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   const double stall = 0.25;
   KernelTimer tm;
   tm.on = o.profile != 0;
+  tm.with_coarse = o.coarse != nullptr;
   int total_iters = 0, outer = 0;
   int sweep_flag = 0;
   for (outer = 0; outer <= o.max_outer; ++outer) {
@@ -1209,7 +1258,8 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     launches += 1;
     int it = 0;
     RB_TRY(inner_solve<T>(A, val, dinv, k, sh, shs, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
-                          b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, st));
+                          b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, co,
+                          st));
     total_iters += it;
     if (it >= o.maxiter) sweep_flag = 1;
     correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, b.os, X);
@@ -1242,6 +1292,8 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   info.spmm_launches += tm.spmm_n;
   info.update_ms += tm.upd_ms;
   info.update_launches += tm.upd_n;
+  info.coarse_ms += tm.coarse_ms;
+  info.coarse_launches += tm.coarse_n;
   return RB_OK;
 }
 
@@ -1255,7 +1307,20 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
   SolveBufs<T64, T> b;
   carve(cv, b, n, A.nnz, kb);
   if (!b.scan_work) return fail(RB_EARG, "rb_femsolve: workspace too small");
+  CoarseBufs<T64, T> cb;
+  if (o.coarse) {
+    cb.op.agg = o.coarse->agg;
+    cb.op.agg_ptr = o.coarse->agg_ptr;
+    cb.op.agg_rows = o.coarse->agg_rows;
+    coarse_carve(cv, cb, o.coarse->nc, kb);
+    if (!cb.A64 || !cb.Rb || !cb.Cb || !cb.Dinv || !cb.op.X || !cb.op.rc || !cb.op.ec || !cb.op.part || !cb.err)
+      return fail(RB_EARG, "rb_femsolve: workspace too small for the coarse space");
+  }
   RB_CUDA_TRY(cudaMemsetAsync(b.counter, 0, 4 * sizeof(int32_t), st));
+  if (o.coarse) {
+    RB_TRY((coarse_setup<T64, T>(A, cb, st)));
+    info.launches += 3 + 5 * (int)ceil_div(cb.op.nc, kGjB);
+  }
   GroupPlan gp{nullptr, nullptr, nullptr, 0};
   if (GrpCfg<T>::enabled && grp_cols_ok(kb) && n > 0) RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask,
                                                                       b.scan_work, b.scan_bytes, &gp, st));
@@ -1263,7 +1328,8 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
   for (int64_t c0 = 0; c0 < nrhs; c0 += kMaxCols) {
     const int64_t k = std::min<int64_t>(kMaxCols, nrhs - c0);
     if (!split) {
-      RB_TRY((solve_block<T64, T>(A, B, X, k, k, o, info, b, val, dinv, gp.ng ? &gp : nullptr, st)));
+      RB_TRY((solve_block<T64, T>(A, B, X, k, k, o, info, b, val, dinv, gp.ng ? &gp : nullptr,
+                                  o.coarse ? &cb.op : nullptr, st)));
     } else {
       return fail(RB_ESIZE, "rb_femsolve: more than %lld right-hand sides per call", (long long)kMaxCols);
     }
@@ -1320,6 +1386,20 @@ size_t rb_femsolve_work_bytes(int64_t n, int64_t nnz, int64_t nrhs, int32_t is_c
   return carve(cv, b, n, nnz, k) + 4096;
 }
 
+size_t rb_coarse_work_bytes(int64_t nc, int64_t nrhs, int32_t is_complex, int32_t precision) {
+  const int64_t k = std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols);
+  Carver cv{nullptr, 0};
+  if (nc < 1) return 0;
+  if (is_complex) {
+    if (precision == RB_FP64) { CoarseBufs<cdouble, cdouble> c; return coarse_carve(cv, c, nc, k); }
+    CoarseBufs<cdouble, cfloat> c;
+    return coarse_carve(cv, c, nc, k);
+  }
+  if (precision == RB_FP64) { CoarseBufs<double, double> c; return coarse_carve(cv, c, nc, k); }
+  CoarseBufs<double, float> c;
+  return coarse_carve(cv, c, nc, k);
+}
+
 int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs, const rb_solve_opts* opts,
                 rb_solve_info* info, void* work, size_t work_bytes, void* stream) {
   if (!A || !B || !X || !opts || !info || !work) return fail(RB_EARG, "rb_femsolve: null argument");
@@ -1331,8 +1411,14 @@ int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs, const r
   if (o.precision == RB_MIXED && (!A->val32 || !A->dinv32)) return fail(RB_EARG, "rb_femsolve: mixed precision needs val32/dinv32");
   if (o.maxiter < 1 || o.check_every < 1 || o.max_outer < 1 || !(o.tol > 0) || !(o.inner_tol > 0))
     return fail(RB_EARG, "rb_femsolve: bad options");
-  if (work_bytes < rb_femsolve_work_bytes(A->n, A->nnz, nrhs, A->is_complex, o.precision))
-    return fail(RB_EARG, "rb_femsolve: workspace too small");
+  size_t need = rb_femsolve_work_bytes(A->n, A->nnz, nrhs, A->is_complex, o.precision);
+  if (o.coarse) {
+    const rb_coarse& c = *o.coarse;
+    if (c.nc < 1 || c.nc > kCoarseMax || c.nc > A->n || !c.agg || !c.agg_ptr || !c.agg_rows)
+      return fail(RB_EARG, "rb_femsolve: coarse space needs 1 <= nc <= min(n, %d) and its three arrays", kCoarseMax);
+    need += rb_coarse_work_bytes(c.nc, nrhs, A->is_complex, o.precision);
+  }
+  if (work_bytes < need) return fail(RB_EARG, "rb_femsolve: workspace too small");
   *info = rb_solve_info{};
   cudaStream_t st = as_stream(stream);
   if (A->is_complex) {

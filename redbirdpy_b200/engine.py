@@ -44,6 +44,9 @@ class DeviceMesh:
         self.nn = int(node.shape[0])
         self.ne = int(elem.shape[0])
         self.node = _f64(node[:, :3], dev)
+        with np.errstate(invalid="ignore"):
+            self.bbox = (np.nanmin(node[:, :3], axis=0), np.nanmax(node[:, :3], axis=0)) if self.nn else None
+        self._coarse = {}
         self.elem = _i32(np.asarray(elem)[:, :4].astype(np.int64) - 1, dev)
         face = np.zeros((0, 3), np.int64) if face is None else np.asarray(face)
         self.nf = int(face.shape[0])
@@ -115,6 +118,13 @@ class DeviceMesh:
         if self._labels[0] != key:
             self._labels = (key, _i32(np.asarray(seg).ravel(), self.device))
         return self._labels[1]
+
+    def coarse_space(self, target):
+        """The CoarseSpace of about ``target`` aggregates (cached per target)."""
+        target = int(target)
+        if target not in self._coarse:
+            self._coarse[target] = CoarseSpace(self, target)
+        return self._coarse[target]
 
     def deldotdel_host(self):
         return self.ddd.cpu().numpy()
@@ -390,17 +400,91 @@ def getdet(mesh, opt, phi):
 
 # -------------------------------------------------------------------- solve
 DEFAULT_TOL = 1e-15
+COARSE_MAX = 4096      # aggregates the library's coarse solver takes at most
+COARSE_MIN_NODES = 20000  # smaller systems converge fast enough on Jacobi alone
+
+
+def coarse_target(nn):
+    """Default aggregate count of the two-level preconditioner for nn nodes."""
+    return int(min(2048, max(256, nn // 200)))
+
+
+class CoarseSpace:
+    """Aggregates of the two-level preconditioner (``rb_coarse``): the mesh
+    nodes binned into cubes of edge h chosen for about ``target`` cubes over
+    the bounding box (fewer are nonempty on a mesh that does not fill its
+    box).  Built on the device by rb_coarse_aggregate."""
+
+    def __init__(self, mesh, target):
+        dev = mesh.device
+        nn = mesh.nn
+        lo, hi = mesh.bbox
+        if not (np.all(np.isfinite(lo)) and np.all(np.isfinite(hi))):
+            raise ValueError("coarse space: node coordinates are not finite")
+        ext = np.maximum(hi - lo, 0.0)
+        span = max(float(ext.max()), 1e-300)
+        ext = np.maximum(ext, span * 1e-6)
+        h = float(np.cbrt(np.prod(ext) / max(1, min(int(target), COARSE_MAX))))
+        self.agg = torch.empty(nn, dtype=torch.int32, device=dev)
+        self.agg_ptr = torch.empty(COARSE_MAX + 1, dtype=torch.int32, device=dev)
+        self.agg_rows = torch.empty(nn, dtype=torch.int32, device=dev)
+        nc = ctypes.c_int64(0)
+        for _ in range(64):
+            nb = np.maximum(np.ceil(ext / h).astype(np.int64), 1)
+            if int(np.prod(nb)) > (1 << 24):
+                h *= 1.25
+                continue
+            wb = _lib.lib().rb_coarse_aggregate_work_bytes(nn, int(np.prod(nb)))
+            work = torch.empty(wb, dtype=torch.uint8, device=dev)
+            code = _lib.lib().rb_coarse_aggregate(
+                ptr(mesh.node), nn, float(lo[0]), float(lo[1]), float(lo[2]), h, int(nb[0]), int(nb[1]), int(nb[2]),
+                ptr(self.agg), ptr(self.agg_ptr), ptr(self.agg_rows), ctypes.byref(nc), ptr(work), wb, stream())
+            if code == _lib.RB_OK:
+                break
+            if code != _lib.RB_ESIZE:
+                raise _lib.RedbirdError("rb_coarse_aggregate", code, _lib.lib().rb_last_error().decode())
+            h *= 1.15
+        else:
+            raise RuntimeError("coarse space: no bin size found")
+        self.nc = int(nc.value)
+        self.h = h
+        self.nb = tuple(int(v) for v in nb)
+        self.struct = _lib.RbCoarse(self.nc, self.agg.data_ptr(), self.agg_ptr.data_ptr(), self.agg_rows.data_ptr())
+
+
+def _resolve_coarse(mat, coarse):
+    """CoarseSpace for solve(coarse=...): 'auto' (meshes of at least
+    COARSE_MIN_NODES nodes), True, an aggregate count, a CoarseSpace, or
+    None/False for Jacobi only."""
+    if coarse is None or coarse is False:
+        return None
+    if isinstance(coarse, CoarseSpace):
+        return coarse
+    mesh = getattr(mat, "mesh", None)
+    if not hasattr(mesh, "coarse_space"):
+        if coarse == "auto":
+            return None
+        raise ValueError("a coarse space needs a matrix assembled on a DeviceMesh")
+    if coarse == "auto":
+        return mesh.coarse_space(coarse_target(mat.n)) if mat.n >= COARSE_MIN_NODES else None
+    if coarse is True:
+        return mesh.coarse_space(coarse_target(mat.n))
+    if isinstance(coarse, (int, np.integer)) and not isinstance(coarse, bool):
+        return mesh.coarse_space(int(coarse))
+    raise ValueError(f"coarse: unsupported value {coarse!r}")
 
 
 def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=2000, max_outer=10,
-          check_every=10, profile=False, x0=None):
+          check_every=10, profile=False, x0=None, coarse="auto"):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
     Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
     corrections inside FP64 iterative refinement; ``'fp64'``: the same loop
     entirely in FP64.  Up to 128 columns per library call; wider B is solved
     in column blocks.  ``x0`` (nn x k, the solution's dtype) is an initial
-    guess: the refinement starts from its FP64 residual instead of from zero."""
+    guess: the refinement starts from its FP64 residual instead of from zero.
+    ``coarse`` adds the aggregation coarse space to the Jacobi preconditioner
+    (see _resolve_coarse; 'auto' uses it on meshes of 20000 nodes or more)."""
     prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
     n, k = B.shape
     xdt = torch.complex128 if mat.is_complex else torch.float64
@@ -411,11 +495,13 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
     else:
         X = torch.empty((n, k), dtype=xdt, device=B.device)
     info = {"iters": 0, "outer": 0, "flag": 0, "launches": 0, "relres": 0.0, "spmm_ms": 0.0, "update_ms": 0.0,
-            "spmm_launches": 0, "update_launches": 0}
+            "spmm_launches": 0, "update_launches": 0, "coarse_ms": 0.0, "coarse_launches": 0}
     if prec == _lib.RB_FP64 and inner_tol > 1e-6:
         inner_tol = max(tol, 1e-15)
+    cs = _resolve_coarse(mat, coarse)
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
-                            int(bool(profile)), int(x0 is not None))
+                            int(bool(profile)), int(x0 is not None),
+                            ctypes.pointer(cs.struct) if cs is not None else None)
     for c0 in range(0, k, 128):
         kb = min(128, k - c0)
         Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
@@ -424,6 +510,8 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
         else:
             Xb = X
         wb = _lib.lib().rb_femsolve_work_bytes(n, mat.struct.nnz, kb, int(mat.is_complex), prec)
+        if cs is not None:
+            wb += _lib.lib().rb_coarse_work_bytes(cs.nc, kb, int(mat.is_complex), prec)
         work = torch.empty(wb, dtype=torch.uint8, device=B.device)
         inf = _lib.RbSolveInfo()
         call("rb_femsolve", ctypes.byref(mat.struct), ptr(Bb), ptr(Xb), kb, ctypes.byref(opts), ctypes.byref(inf),
@@ -435,8 +523,9 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
         info["flag"] = max(info["flag"], inf.flag)
         info["launches"] += inf.launches
         info["relres"] = max(info["relres"], inf.relres)
-        for key in ("spmm_ms", "update_ms", "spmm_launches", "update_launches"):
+        for key in ("spmm_ms", "update_ms", "spmm_launches", "update_launches", "coarse_ms", "coarse_launches"):
             info[key] += getattr(inf, key)
+    info["coarse_nc"] = cs.nc if cs is not None else 0
     return X, info
 
 
