@@ -15,6 +15,8 @@
 //     r.z = sum_i r_i d_i r_i + sum_I (P^T r)_I (X P^T r)_I .
 #pragma once
 
+#include <type_traits>
+
 namespace rb {
 
 constexpr int kCoarseMax = 4096;  // largest aggregate count (one row of P^T A P in shared memory)
@@ -88,6 +90,82 @@ static int gemm(int64_t m, int64_t n, int64_t kk, T alpha, const T* A, int64_t l
                                     cstride);
   RB_LAUNCH_CHECK();
   return RB_OK;
+}
+
+// E_z = X[:, kz] RC[kz, :] for the coarse product, X symmetric (the
+// inverse of the symmetric aggregated operator): the A-operand tile element
+// (i, q) = X[q][i] is read along X's rows, so both operand tiles load
+// coalesced and land in shared memory untransposed.  64 x BN tiles, 16-deep
+// k steps, 256 threads with 4 x TN outputs each (a 4-vector of the X tile
+// and TN-vector of the RC tile per k step); the next k step's tiles are
+// fetched into registers while the current one is used.  Split K over
+// blockIdx.z as gemm_kernel.
+template <typename T, int BN>
+__global__ void __launch_bounds__(256) coarse_gemm_kernel(int64_t m, int64_t n, const T* __restrict__ X, int64_t ldx,
+                                                          const T* __restrict__ B, int64_t ldb, T* __restrict__ C,
+                                                          int64_t ldc, int64_t kchunk, int64_t cstride) {
+  constexpr int BM = 64, BK = 16, TM = 4, TN = BN / 16;
+  constexpr int LA = BM * BK / 256, LB = BN * BK / 256;  // tile elements each thread loads
+  __shared__ __align__(16) T As[BK][BM];
+  __shared__ __align__(16) T Bs[BK][BN];
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;  // output columns tx*TN.., rows ty*TM..
+  const int64_t r0 = (int64_t)blockIdx.y * BM, c0 = (int64_t)blockIdx.x * BN;
+  const int64_t kb = (int64_t)blockIdx.z * kchunk, ke = std::min<int64_t>(m, kb + kchunk);  // X is m x m
+  C += (int64_t)blockIdx.z * cstride;
+  T acc[TM][TN];
+#pragma unroll
+  for (int u = 0; u < TM; ++u)
+#pragma unroll
+    for (int v = 0; v < TN; ++v) acc[u][v] = s_zero(T());
+  T ra[LA], rb[LB];
+  auto fetch = [&](int64_t k0) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + 256 * l, q = e / BM, i = e % BM;
+      ra[l] = (k0 + q < ke && r0 + i < m) ? X[(k0 + q) * ldx + r0 + i] : s_zero(T());
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + 256 * l, q = e / BN, j = e % BN;
+      rb[l] = (k0 + q < ke && c0 + j < n) ? B[(k0 + q) * ldb + c0 + j] : s_zero(T());
+    }
+  };
+  if (kb < ke) fetch(kb);
+  for (int64_t k0 = kb; k0 < ke; k0 += BK) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + 256 * l;
+      As[e / BM][e % BM] = ra[l];
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + 256 * l;
+      Bs[e / BN][e % BN] = rb[l];
+    }
+    __syncthreads();
+    if (k0 + BK < ke) fetch(k0 + BK);
+#pragma unroll
+    for (int q = 0; q < BK; ++q) {
+      T a[TM], b[TN];
+#pragma unroll
+      for (int u = 0; u < TM; ++u) a[u] = As[q][ty * TM + u];
+#pragma unroll
+      for (int v = 0; v < TN; ++v) b[v] = Bs[q][tx * TN + v];
+#pragma unroll
+      for (int u = 0; u < TM; ++u)
+#pragma unroll
+        for (int v = 0; v < TN; ++v) acc[u][v] = s_fma(a[u], b[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < TM; ++u)
+#pragma unroll
+    for (int v = 0; v < TN; ++v) {
+      const int64_t i = r0 + ty * TM + u, j = c0 + tx * TN + v;
+      if (i < m && j < n) C[i * ldc + j] = acc[u][v];
+    }
 }
 
 __device__ __forceinline__ double s_inv(double a) { return 1.0 / a; }
@@ -406,21 +484,44 @@ static int coarse_setup(const rb_csr& A, CoarseBufs<T64, T>& c, cudaStream_t st)
   return RB_OK;
 }
 
-// rc = P^T r, ec = X rc, part = column sums of rc * ec
+// rc = P^T r (unless R is NULL: rc already holds it), ec = X rc,
+// part = column sums of rc * ec
 template <typename T>
 static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_t st) {
   const int64_t nc = c.nc;
-  restrict_kernel<T><<<(unsigned)std::min<int64_t>(nc, 148 * 16), 256, 0, st>>>(nc, k, R, c.agg_ptr, c.agg_rows,
-                                                                                c.rc);
-  RB_LAUNCH_CHECK();
-  const T one = h_real<T>(1.0), zero = h_real<T>(0.0);
+  if (R) {
+    restrict_kernel<T><<<(unsigned)std::min<int64_t>(nc, 148 * 16), 256, 0, st>>>(nc, k, R, c.agg_ptr, c.agg_rows,
+                                                                                  c.rc);
+    RB_LAUNCH_CHECK();
+  }
   // enough blocks for two per SM: split the nc-long sums (fixed order, no atomics)
-  const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, 64);
-  const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
-                                                                   ceil_div(nc, 256)}));
-  RB_TRY(gemm<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k));
-  coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec, (typename Scalar<T>::acc*)c.part);
-  RB_LAUNCH_CHECK();
+  if constexpr (std::is_same<T, cdouble>::value) {
+    const T one = h_real<T>(1.0), zero = h_real<T>(0.0);
+    const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, 64);
+    const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
+                                                                     ceil_div(nc, 256)}));
+    RB_TRY(gemm<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k));
+    coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec,
+                                                    (typename Scalar<T>::acc*)c.part);
+    RB_LAUNCH_CHECK();
+  } else {
+    // 64 x 128 tiles for FP32 (127 registers); 64 x 64 for 8-byte scalars,
+    // whose 64 x 128 tile needs ~180 registers (one block per SM)
+    const int bn = (k > 64 && sizeof(T) == 4) ? 128 : 64;
+    const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, bn);
+    const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
+                                                                     ceil_div(nc, 256)}));
+    const int64_t kchunk = ceil_div(ceil_div(nc, splits), 16) * 16;
+    dim3 g((unsigned)ceil_div(k, bn), (unsigned)ceil_div(nc, 64), (unsigned)splits);
+    if (bn == 128)
+      coarse_gemm_kernel<T, 128><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
+    else
+      coarse_gemm_kernel<T, 64><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
+    RB_LAUNCH_CHECK();
+    coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec,
+                                                    (typename Scalar<T>::acc*)c.part);
+    RB_LAUNCH_CHECK();
+  }
   return RB_OK;
 }
 

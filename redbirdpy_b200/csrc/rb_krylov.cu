@@ -689,6 +689,139 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
   }
 }
 
+// Aggregate-ordered forms of the two kernels above, used with a coarse
+// space on real systems: block b takes aggregates b, b + grid, ...; the
+// block's lane groups take the aggregate's rows (agg_rows) in turn.  The
+// vector updates are row-local, so the order changes no value; what it buys
+// is the coarse restriction rc[I] = sum of the aggregate's new r rows, summed
+// in registers and then over the groups in fixed order (no extra pass over
+// r), and one read of ec[I] per aggregate in the p-update.  Measured on the
+// 520k-node box at 128 columns: FP32 update 0.265 ms either order and 0.12 ms
+// less per iteration in all; complex64 update 0.83 ms against 0.54 ms in row
+// order (scattered 1 KB rows), so complex systems keep the row order and a
+// separate restriction kernel.
+template <typename T> struct AggOrder { static constexpr bool value = !Scalar<T>::is_complex; };
+template <typename A, int L, int V, typename T>
+__device__ __forceinline__ void block_colsum_row(const A (&acc)[V], T* __restrict__ out, int64_t k, A* sm) {
+  const int lane = threadIdx.x % L, grp = threadIdx.x / L;
+  constexpr int G = kBlk / L;
+#pragma unroll
+  for (int j = 0; j < V; ++j) sm[(grp * L + lane) * V + j] = acc[j];
+  __syncthreads();
+  for (int c = threadIdx.x; c < L * V && c < k; c += kBlk) {
+    const int l = c / V, j = c % V;
+    A s = acc_zero<A>();
+    for (int g = 0; g < G; ++g) s = acc_add(s, sm[(g * L + l) * V + j]);
+    if constexpr (Scalar<T>::is_complex) {
+      out[c] = T{(typename Scalar<T>::real)s.x, (typename Scalar<T>::real)s.y};
+    } else {
+      out[c] = (T)s;
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T, int L, int V>
+__global__ void __launch_bounds__(kBlk, Bps<T>::value)
+cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
+                     T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
+                     const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
+                     T* __restrict__ rc, typename Scalar<T>::acc* __restrict__ part_rz,
+                     double* __restrict__ part_rr) {
+  typedef typename Scalar<T>::acc A;
+  __shared__ A sm[kBlk * V];
+  __shared__ double smr[kBlk * V];
+  constexpr int G = kBlk / L;
+  const int lane = threadIdx.x % L, grp = threadIdx.x / L;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  alignas(16) T al[V];
+  bool act[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    act[j] = on && cs[c0 + j].active;
+    al[j] = act[j] ? from_c<T>(cs[c0 + j].alpha) : s_zero(T());
+  }
+  alignas(16) A arz[V];
+  alignas(16) double arr[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
+  for (int64_t I = blockIdx.x; I < nc; I += gridDim.x) {
+    alignas(16) A rs[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) rs[j] = acc_zero<A>();
+    const int32_t q1 = agg_ptr[I + 1];
+    int32_t q = agg_ptr[I] + grp;
+    int32_t nrow = q < q1 ? agg_rows[q] : 0;
+    for (; q < q1; q += G) {
+      const int64_t row = nrow;
+      if (q + G < q1) nrow = agg_rows[q + G];  // next row's index in flight
+      if (!on) continue;
+      const T d = dinv[row];
+      alignas(16) T x[V], r[V], p[V], qv[V];
+      ldv<T, V>(Xs + row * k + c0, x);
+      ldv<T, V>(R + row * k + c0, r);
+      ldv<T, V>(P + row * k + c0, p);
+      ldv<T, V>(Q + row * k + c0, qv);
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        if (act[j]) {
+          x[j] = s_fma(al[j], p[j], x[j]);
+          r[j] = s_sub(r[j], s_mul(al[j], qv[j]));
+        }
+        const T z = s_mul(d, r[j]);
+        arz[j] = acc_fma(r[j], z, arz[j]);
+        arr[j] += s_abs2(r[j]);
+        rs[j] = acc_add(rs[j], to_acc(r[j]));
+      }
+      stv<T, V>(Xs + row * k + c0, x);
+      stv<T, V>(R + row * k + c0, r);
+    }
+    block_colsum_row<A, L, V, T>(rs, rc + I * k, k, sm);
+  }
+  block_colreduce<A, L, V>(arz, part_rz, k, sm);
+  block_colreduce<double, L, V>(arr, part_rr, k, smr);
+}
+
+template <typename T, int L, int V>
+__global__ void __launch_bounds__(kBlk, Bps<T>::value)
+cg_pupdate_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
+                      const T* __restrict__ R, T* __restrict__ P, const int32_t* __restrict__ agg_ptr,
+                      const int32_t* __restrict__ agg_rows, const T* __restrict__ ec) {
+  constexpr int G = kBlk / L;
+  const int lane = threadIdx.x % L, grp = threadIdx.x / L;
+  const int64_t c0 = (int64_t)lane * V;
+  if (c0 >= k) return;
+  alignas(16) T be[V];
+  bool act[V], any = false;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    act[j] = cs[c0 + j].active;
+    be[j] = from_c<T>(cs[c0 + j].beta);
+    any |= act[j];
+  }
+  if (!any) return;
+  for (int64_t I = blockIdx.x; I < nc; I += gridDim.x) {
+    alignas(16) T e[V];
+    ldv<T, V>(ec + I * k + c0, e);
+    const int32_t q1 = agg_ptr[I + 1];
+    int32_t q = agg_ptr[I] + grp;
+    int32_t nrow = q < q1 ? agg_rows[q] : 0;
+    for (; q < q1; q += G) {
+      const int64_t row = nrow;
+      if (q + G < q1) nrow = agg_rows[q + G];
+      const T d = dinv[row];
+      alignas(16) T r[V], p[V];
+      ldv<T, V>(R + row * k + c0, r);
+      ldv<T, V>(P + row * k + c0, p);
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if (act[j]) p[j] = s_fma(be[j], p[j], s_fma(d, r[j], e[j]));
+      stv<T, V>(P + row * k + c0, p);
+    }
+  }
+}
+
 // ----------------------------------------------------------- finalizers
 __device__ __forceinline__ cdouble cdiv(cdouble a, cdouble b) {
   const double d = b.x * b.x + b.y * b.y;
@@ -1157,6 +1290,12 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
   const int32_t* agg = co ? co->agg : nullptr;
   const T* ec = co ? co->ec : nullptr;
   const Acc* part_c = co ? (const Acc*)co->part : nullptr;
+  // blocks of the aggregate-ordered kernels: two waves of resident blocks
+  // (the second evens out aggregates of unequal size), within the partials
+  const unsigned agrid = co ? (unsigned)std::max<int64_t>(1, std::min<int64_t>(co->nc, std::min<int64_t>(
+                                                                   2 * (int64_t)sh.grid, kGridMax)))
+                            : 0u;
+  const unsigned ugrid = (co && AggOrder<T>::value) ? agrid : sh.grid;  // blocks of the update kernel (partials)
   if (co) {
     RB_TRY(coarse_apply<T>(*co, R, k, st));
     *launches += 3;
@@ -1184,22 +1323,39 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       }
       RB_TRY(tm.record(st));
       fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)nb, (const Acc*)part_a, cs);
+      if (co && AggOrder<T>::value) {
+        // aggregate order: the update also restricts the new r to rc
+#define RB_UPD(L_, V_)                                                                                           \
+  cg_update_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, Xs, R, P, Q, co->agg_ptr,      \
+                                                         co->agg_rows, co->rc, (Acc*)part_a, part_b)
+        RB_DISPATCH_LV(sh, RB_UPD);
+#undef RB_UPD
+      } else {
 #define RB_UPD(L_, V_) \
   cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b)
-      RB_DISPATCH_LV(sh, RB_UPD);
+        RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
+      }
       RB_TRY(tm.record(st));
       if (co) {
-        RB_TRY(coarse_apply<T>(*co, R, k, st));
-        *launches += 3;
+        RB_TRY(coarse_apply<T>(*co, AggOrder<T>::value ? nullptr : R, k, st));
+        *launches += AggOrder<T>::value ? 2 : 3;
       }
       RB_TRY(tm.record(st));
       if (b == burst - 1) RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, tol2, counter, part_c,
+      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2, counter, part_c,
                                                kCdotGrid);
-#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P, agg, ec)
-      RB_DISPATCH_LV(sh, RB_PUP);
+      if (co && AggOrder<T>::value) {
+#define RB_PUP(L_, V_)                                                                                   \
+  cg_pupdate_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, P, co->agg_ptr,   \
+                                                          co->agg_rows, ec)
+        RB_DISPATCH_LV(sh, RB_PUP);
 #undef RB_PUP
+      } else {
+#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P, agg, ec)
+        RB_DISPATCH_LV(sh, RB_PUP);
+#undef RB_PUP
+      }
       RB_LAUNCH_CHECK();
       *launches += 5;
     }
