@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256) restrict_kernel(int64_t nc, int64_t k, co
 
 // ec[I][c] = sum over the splits s (in order) of es[s][I][c];
 // part[block][c] = sum over this block's aggregates of rc[I][c] ec[I][c] (unconjugated)
-constexpr int kCdotGrid = 64;
+constexpr int kCdotGrid = 256;  // one aggregate per warp at nc = 2048
 template <typename T>
 __global__ void __launch_bounds__(256) coarse_dot_kernel(int64_t nc, int64_t k, const T* __restrict__ rc,
                                                          const T* __restrict__ es, int splits,
@@ -505,9 +505,11 @@ static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_
                                                     (typename Scalar<T>::acc*)c.part);
     RB_LAUNCH_CHECK();
   } else {
-    // 64 x 128 tiles for FP32 (127 registers); 64 x 64 for 8-byte scalars,
-    // whose 64 x 128 tile needs ~180 registers (one block per SM)
-    const int bn = (k > 64 && sizeof(T) == 4) ? 128 : 64;
+    // 64 x 64 tiles (79 registers for FP32, three blocks per SM): 54 us per
+    // product at nc = 2048, k = 128 against 67 us for 64 x 128 tiles (127
+    // registers, two blocks per SM); 8-byte scalars would need ~180 registers
+    // for 64 x 128
+    const int bn = 64;
     const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, bn);
     const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
                                                                      ceil_div(nc, 256)}));
