@@ -505,20 +505,17 @@ static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_
                                                     (typename Scalar<T>::acc*)c.part);
     RB_LAUNCH_CHECK();
   } else {
-    // 64 x 64 tiles (79 registers for FP32, three blocks per SM): 54 us per
-    // product at nc = 2048, k = 128 against 67 us for 64 x 128 tiles (127
-    // registers, two blocks per SM); 8-byte scalars would need ~180 registers
-    // for 64 x 128
+    // 64 x 64 tiles (79 registers for FP32, three blocks per SM): product and
+    // dot 54 us per iteration at nc = 2048, k = 128 against 67 us with 64 x 128
+    // tiles (127 registers, two blocks per SM); 8-byte scalars would need ~180
+    // registers for 64 x 128
     const int bn = 64;
     const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, bn);
     const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
                                                                      ceil_div(nc, 256)}));
     const int64_t kchunk = ceil_div(ceil_div(nc, splits), 16) * 16;
     dim3 g((unsigned)ceil_div(k, bn), (unsigned)ceil_div(nc, 64), (unsigned)splits);
-    if (bn == 128)
-      coarse_gemm_kernel<T, 128><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
-    else
-      coarse_gemm_kernel<T, 64><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
+    coarse_gemm_kernel<T, 64><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
     RB_LAUNCH_CHECK();
     coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec,
                                                     (typename Scalar<T>::acc*)c.part);
