@@ -481,7 +481,7 @@ def _resolve_coarse(mat, coarse):
     raise ValueError(f"coarse: unsupported value {coarse!r}")
 
 
-def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=2000, max_outer=10,
+def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=2000, max_outer=10,
           check_every=10, profile=False, x0=None, coarse="auto"):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
@@ -491,7 +491,12 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
     in column blocks.  ``x0`` (nn x k, the solution's dtype) is an initial
     guess: the refinement starts from its FP64 residual instead of from zero.
     ``coarse`` adds the aggregation coarse space to the Jacobi preconditioner
-    (see _resolve_coarse; 'auto' uses it on meshes of 20000 nodes or more)."""
+    (see _resolve_coarse; 'auto' uses it on meshes of 20000 nodes or more).
+    ``inner_tol`` (relative residual of each FP32 correction sweep) defaults to
+    1e-5 with a coarse space and 1e-4 without: on the 520k-node box at 128
+    columns, 1e-5 took 3 sweeps / 130 iterations / 113.5 ms against 4 / 150 /
+    129.3 ms at 1e-4 and 3 / 150 / 128.6 ms at 1e-6, while Jacobi alone is
+    fastest at 1e-4."""
     prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
     n, k = B.shape
     xdt = torch.complex128 if mat.is_complex else torch.float64
@@ -503,9 +508,11 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=1e-4, maxiter=20
         X = torch.empty((n, k), dtype=xdt, device=B.device)
     info = {"iters": 0, "outer": 0, "flag": 0, "launches": 0, "relres": 0.0, "spmm_ms": 0.0, "update_ms": 0.0,
             "spmm_launches": 0, "update_launches": 0, "coarse_ms": 0.0, "coarse_launches": 0}
+    cs = _resolve_coarse(mat, coarse)
+    if inner_tol is None:
+        inner_tol = 1e-5 if cs is not None else 1e-4
     if prec == _lib.RB_FP64 and inner_tol > 1e-6:
         inner_tol = max(tol, 1e-15)
-    cs = _resolve_coarse(mat, coarse)
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
                             int(bool(profile)), int(x0 is not None),
                             ctypes.pointer(cs.struct) if cs is not None else None)

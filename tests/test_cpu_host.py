@@ -111,3 +111,48 @@ def test_multi_wavelength_host_pieces(golden):
     sd = u.sdmap(cfg)
     for wv in ("690", "830"):
         assert np.array_equal(sd[wv], g["sd_" + wv])
+
+
+def test_coarse_space_host_rules():
+    """Aggregate counts and the coarse option's resolution (no GPU needed)."""
+    from redbirdpy_b200 import engine
+
+    assert engine.coarse_target(520251) == 2048 and engine.coarse_target(520251, True) == 1024
+    assert engine.coarse_target(67626) == 1056 and engine.coarse_target(67626, True) == 528
+    assert engine.coarse_target(20000) == 312
+    assert engine.coarse_target(1000) == 62  # never above nn / 16
+    assert all(1 <= engine.coarse_target(n, c) <= engine.COARSE_MAX for n in (1, 17, 10 ** 7) for c in (0, 1))
+
+    class Mat:  # a matrix without a DeviceMesh (e.g. uploaded from scipy)
+        n, is_complex, mesh = 10 ** 6, False, None
+
+    assert engine._resolve_coarse(Mat(), None) is None
+    assert engine._resolve_coarse(Mat(), False) is None
+    assert engine._resolve_coarse(Mat(), "auto") is None
+    with pytest.raises(ValueError):
+        engine._resolve_coarse(Mat(), True)
+
+    class Mesh:
+        def coarse_space(self, target):
+            return ("space", target)
+
+    class MeshMat(Mat):
+        mesh = Mesh()
+
+    m = MeshMat()
+    assert engine._resolve_coarse(m, "auto") == ("space", 2048)
+    assert engine._resolve_coarse(m, 300) == ("space", 300)
+    m.n = 1000
+    assert engine._resolve_coarse(m, "auto") is None  # below COARSE_MIN_NODES
+    assert engine._resolve_coarse(m, True) == ("space", 62)
+    with pytest.raises(ValueError):
+        engine._resolve_coarse(m, "sometimes")
+    # the C ABI sizes: nothing without aggregates, growing with nc and columns
+    from redbirdpy_b200 import _lib
+
+    wb = _lib.lib().rb_coarse_work_bytes
+    assert wb(0, 128, 0, 0) == 0
+    assert 0 < wb(256, 128, 0, 0) < wb(2048, 128, 0, 0) < wb(2048, 128, 1, 0)
+    assert wb(2048, 32, 0, 0) < wb(2048, 128, 0, 0)
+    ab = _lib.lib().rb_coarse_aggregate_work_bytes
+    assert ab(0, 10) == 0 and ab(1000, 512) > 0
