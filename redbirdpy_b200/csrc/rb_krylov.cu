@@ -24,8 +24,13 @@ constexpr int kBlk = 256;
 // register budget (__launch_bounds__) and the single-wave grid size
 template <typename T> struct Bps { static constexpr int value = 4; };
 template <> struct Bps<cdouble> { static constexpr int value = 3; };
-// SpMM: same budget (8 gathers in flight need the registers; measured best)
+// complex64 vector kernels: 3 blocks (85 registers); at 4 the CG update
+// spilled (88 B in row order, 272 B in aggregate order)
+template <> struct Bps<cfloat> { static constexpr int value = 3; };
+// SpMM: 4 blocks per SM for the FP32 types (8 gathers in flight need the
+// registers; measured best), 3 for complex128
 template <typename T> struct BpsSpmm { static constexpr int value = Bps<T>::value; };
+template <> struct BpsSpmm<cfloat> { static constexpr int value = 4; };
 constexpr int kGridMax = 148 * 8;       // upper bound of any grid (partials arrays)
 
 // ----------------------------------------------------------- vector access
@@ -696,11 +701,13 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
 // is the coarse restriction rc[I] = sum of the aggregate's new r rows, summed
 // in registers and then over the groups in fixed order (no extra pass over
 // r), and one read of ec[I] per aggregate in the p-update.  Measured on the
-// 520k-node box at 128 columns: FP32 update 0.265 ms either order and 0.12 ms
-// less per iteration in all; complex64 update 0.83 ms against 0.54 ms in row
-// order (scattered 1 KB rows), so complex systems keep the row order and a
-// separate restriction kernel.
-template <typename T> struct AggOrder { static constexpr bool value = !Scalar<T>::is_complex; };
+// 520k-node box at 128 columns: FP32 update 0.265 ms in either order, 0.12 ms
+// less per iteration in all; complex64 update 0.577 ms against 0.525 ms in
+// row order, but the coarse step 0.070 ms against 0.285 ms with a separate
+// restriction kernel (FD forward 276 ms against 299 ms).  Each lane group
+// sums its rows of the aggregate in the vector type (about 30 rows), the
+// groups are added in FP64 and the result rounded to the vector type.
+template <typename T> struct AggOrder { static constexpr bool value = true; };
 template <typename A, int L, int V, typename T>
 __device__ __forceinline__ void block_colsum_row(const A (&acc)[V], T* __restrict__ out, int64_t k, A* sm) {
   const int lane = threadIdx.x % L, grp = threadIdx.x / L;
@@ -747,9 +754,9 @@ cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, con
 #pragma unroll
   for (int j = 0; j < V; ++j) { arz[j] = acc_zero<A>(); arr[j] = 0.0; }
   for (int64_t I = blockIdx.x; I < nc; I += gridDim.x) {
-    alignas(16) A rs[V];
+    alignas(16) T rs[V];
 #pragma unroll
-    for (int j = 0; j < V; ++j) rs[j] = acc_zero<A>();
+    for (int j = 0; j < V; ++j) rs[j] = s_zero(T());
     const int32_t q1 = agg_ptr[I + 1];
     int32_t q = agg_ptr[I] + grp;
     int32_t nrow = q < q1 ? agg_rows[q] : 0;
@@ -772,12 +779,17 @@ cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, con
         const T z = s_mul(d, r[j]);
         arz[j] = acc_fma(r[j], z, arz[j]);
         arr[j] += s_abs2(r[j]);
-        rs[j] = acc_add(rs[j], to_acc(r[j]));
+        rs[j] = s_add(rs[j], r[j]);
       }
       stv<T, V>(Xs + row * k + c0, x);
       stv<T, V>(R + row * k + c0, r);
     }
-    block_colsum_row<A, L, V, T>(rs, rc + I * k, k, sm);
+    {
+      alignas(16) A rsa[V];
+#pragma unroll
+      for (int j = 0; j < V; ++j) rsa[j] = to_acc(rs[j]);
+      block_colsum_row<A, L, V, T>(rsa, rc + I * k, k, sm);
+    }
   }
   block_colreduce<A, L, V>(arz, part_rz, k, sm);
   block_colreduce<double, L, V>(arr, part_rr, k, smr);

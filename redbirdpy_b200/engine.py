@@ -409,9 +409,9 @@ def coarse_target(nn, is_complex=False):
     nn / 64 within [256, 2048] for real systems, nn / 128 within [256, 1024]
     for complex ones (their coarse product costs four times as much), never
     above nn / 16.  Measured on the 100 x 100 x 50 mm box at 128 columns
-    (forward solve, ms; Jacobi alone in brackets): 520k nodes CW 2048
-    aggregates 134, 1183 142 (262); frequency domain 1183 327, 2048 333 (572);
-    68k nodes CW 1183 20.1, 2048 26.7 (24.0)."""
+    (forward solve with 1e-4 sweeps, ms; Jacobi alone in brackets): 520k
+    nodes CW 2048 aggregates 134, 1183 142 (262); frequency domain 1183 327,
+    2048 333 (572); 68k nodes CW 1183 20.1, 2048 26.7 (24.0)."""
     lo, hi, per = (256, 1024, 128) if is_complex else (256, 2048, 64)
     return int(max(1, min(max(lo, min(hi, nn // per)), nn // 16)))
 
