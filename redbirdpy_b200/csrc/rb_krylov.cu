@@ -23,14 +23,17 @@ constexpr int kBlk = 256;
 // resident blocks per SM of the row kernels, by scalar type: sets both the
 // register budget (__launch_bounds__) and the single-wave grid size
 template <typename T> struct Bps { static constexpr int value = 4; };
-template <> struct Bps<cdouble> { static constexpr int value = 3; };
+// complex128 vector kernels: 2 blocks (128 registers); at 3 the CG update
+// spilled 300 B (row order) and 476 B (aggregate order)
+template <> struct Bps<cdouble> { static constexpr int value = 2; };
 // complex64 vector kernels: 3 blocks (85 registers); at 4 the CG update
 // spilled (88 B in row order, 272 B in aggregate order)
 template <> struct Bps<cfloat> { static constexpr int value = 3; };
 // SpMM: 4 blocks per SM for the FP32 types (8 gathers in flight need the
-// registers; measured best), 3 for complex128
+// registers; measured best), 3 for complex128 (no spills in the residual form)
 template <typename T> struct BpsSpmm { static constexpr int value = Bps<T>::value; };
 template <> struct BpsSpmm<cfloat> { static constexpr int value = 4; };
+template <> struct BpsSpmm<cdouble> { static constexpr int value = 3; };
 constexpr int kGridMax = 148 * 8;       // upper bound of any grid (partials arrays)
 
 // ----------------------------------------------------------- vector access
@@ -1389,7 +1392,7 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
   const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
-  const Shape sh64 = pick_shape(n, k, Bps<T64>::value);  // FP64 residual kernels
+  const Shape sh64 = pick_shape(n, k, BpsSpmm<T64>::value);  // FP64 residual kernels
   const unsigned fg = (unsigned)ceil_div(k, 8);
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
   int launches = 0;
