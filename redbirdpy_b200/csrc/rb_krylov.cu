@@ -1080,6 +1080,44 @@ static Shape pick_shape(int64_t n, int64_t k, int bps) {
   return s;
 }
 
+// Column counts the lane layout of pick_shape covers (L V >= k): up to 32
+// columns of any count, even counts up to 64, multiples of 4 up to 128.  A
+// solve of another count runs on a copy padded with zero columns to the next
+// multiple of 4 (zero right-hand sides stay inactive and exactly zero).
+static int64_t solve_cols(int64_t k) {
+  if (k <= 32 || k % 4 == 0 || (k % 2 == 0 && k <= 64)) return k;
+  return ceil_div(k, 4) * 4;
+}
+static bool shape_covers(const Shape& s, int64_t k) { return (int64_t)s.S * s.L * s.V >= k; }
+
+// D[i][c] = S[i][c] for c < ks, 0 beyond (row-major, ld ks and kd)
+template <typename T>
+__global__ void copy_cols_kernel(int64_t n, int64_t ks, int64_t kd, const T* __restrict__ S, T* __restrict__ D) {
+  const int64_t total = n * kd;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / kd, c = i % kd;
+    D[i] = c < ks ? S[r * ks + c] : s_zero(T());
+  }
+}
+
+// Y = A X for any column count: a warp per row, lanes over columns (plain
+// loads; rb_spmm's path for counts the vectorised layout does not cover)
+template <typename T>
+__global__ void spmm_any_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr,
+                                const int32_t* __restrict__ indices, const T* __restrict__ val,
+                                const T* __restrict__ X, T* __restrict__ Y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < n; row += warps) {
+    const int32_t b = indptr[row], e = indptr[row + 1];
+    for (int64_t c = lane; c < k; c += 32) {
+      T y = s_zero(T());
+      for (int32_t p = b; p < e; ++p) y = s_fma(val[p], X[(int64_t)indices[p] * k + c], y);
+      Y[row * k + c] = y;
+    }
+  }
+}
+
 // SpMM shape: complex64 at 128 columns takes two 64-column slices (2 values
 // of 8 bytes per lane, 8 gathers in flight), measured 23% faster per launch
 // than one slice of 4 values with 4 gathers in flight
@@ -1397,6 +1435,8 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);
   int launches = 0;
   if (ldx != k) return fail(RB_EARG, "solve_block: internal ldx");
+  if (!shape_covers(sh, k) || !shape_covers(shs, k) || !shape_covers(sh64, k))
+    return fail(RB_EARG, "solve_block: %lld columns not covered by the lane layout", (long long)k);
   // ||b|| per column
 #define RB_CN(L_, V_) colnorm_kernel<L_, V_><<<sh64.grid, kBlk, 0, st>>>(n, k, B, b.part_b)
   RB_DISPATCH_LV(sh64, RB_CN);
@@ -1473,11 +1513,19 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
                       rb_solve_info& info, void* work, size_t work_bytes, const T* val, const T* dinv,
                       cudaStream_t st) {
   const int64_t n = A.n;
-  const int64_t kb = std::min<int64_t>(nrhs, kMaxCols);
+  if (nrhs > kMaxCols) return fail(RB_ESIZE, "rb_femsolve: more than %lld right-hand sides per call", (long long)kMaxCols);
+  const int64_t kb = solve_cols(nrhs);  // columns of the solve (padded when the layout needs it)
   Carver cv{reinterpret_cast<char*>(work), work_bytes};
   SolveBufs<T64, T> b;
   carve(cv, b, n, A.nnz, kb);
   if (!b.scan_work) return fail(RB_EARG, "rb_femsolve: workspace too small");
+  double* Bp = nullptr;
+  T64* Xp = nullptr;
+  if (kb != nrhs) {
+    Bp = cv.take<double>(n * kb);
+    Xp = cv.take<T64>(n * kb);
+    if (!Bp || !Xp) return fail(RB_EARG, "rb_femsolve: workspace too small");
+  }
   CoarseBufs<T64, T> cb;
   if (o.coarse) {
     cb.op.agg = o.coarse->agg;
@@ -1495,15 +1543,21 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
   GroupPlan gp{nullptr, nullptr, nullptr, 0};
   if (GrpCfg<T>::enabled && grp_cols_ok(kb) && n > 0) RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask,
                                                                       b.scan_work, b.scan_bytes, &gp, st));
-  const bool split = nrhs > kMaxCols;
-  for (int64_t c0 = 0; c0 < nrhs; c0 += kMaxCols) {
-    const int64_t k = std::min<int64_t>(kMaxCols, nrhs - c0);
-    if (!split) {
-      RB_TRY((solve_block<T64, T>(A, B, X, k, k, o, info, b, val, dinv, gp.ng ? &gp : nullptr,
-                                  o.coarse ? &cb.op : nullptr, st)));
-    } else {
-      return fail(RB_ESIZE, "rb_femsolve: more than %lld right-hand sides per call", (long long)kMaxCols);
+  const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * kb, 256), 148 * 16);
+  if (Bp) {
+    copy_cols_kernel<double><<<eg, 256, 0, st>>>(n, nrhs, kb, B, Bp);
+    RB_LAUNCH_CHECK();
+    if (o.use_x0) {
+      copy_cols_kernel<T64><<<eg, 256, 0, st>>>(n, nrhs, kb, X, Xp);
+      RB_LAUNCH_CHECK();
     }
+  }
+  RB_TRY((solve_block<T64, T>(A, Bp ? Bp : B, Xp ? Xp : X, kb, kb, o, info, b, val, dinv, gp.ng ? &gp : nullptr,
+                              o.coarse ? &cb.op : nullptr, st)));
+  if (Xp) {
+    copy_cols_kernel<T64><<<eg, 256, 0, st>>>(n, kb, nrhs, Xp, X);
+    RB_LAUNCH_CHECK();
+    info.launches += o.use_x0 ? 3 : 2;
   }
   return RB_OK;
 }
@@ -1545,20 +1599,27 @@ using namespace rb;
 extern "C" {
 
 size_t rb_femsolve_work_bytes(int64_t n, int64_t nnz, int64_t nrhs, int32_t is_complex, int32_t precision) {
-  const int64_t k = std::min<int64_t>(nrhs, kMaxCols);
+  const int64_t k0 = std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols), k = solve_cols(k0);
   Carver cv{nullptr, 0};
+  size_t bytes;
   if (is_complex) {
-    if (precision == RB_FP64) { SolveBufs<cdouble, cdouble> b; return carve(cv, b, n, nnz, k) + 4096; }
-    SolveBufs<cdouble, cfloat> b;
-    return carve(cv, b, n, nnz, k) + 4096;
+    if (precision == RB_FP64) { SolveBufs<cdouble, cdouble> b; bytes = carve(cv, b, n, nnz, k); }
+    else { SolveBufs<cdouble, cfloat> b; bytes = carve(cv, b, n, nnz, k); }
+  } else {
+    if (precision == RB_FP64) { SolveBufs<double, double> b; bytes = carve(cv, b, n, nnz, k); }
+    else { SolveBufs<double, float> b; bytes = carve(cv, b, n, nnz, k); }
   }
-  if (precision == RB_FP64) { SolveBufs<double, double> b; return carve(cv, b, n, nnz, k) + 4096; }
-  SolveBufs<double, float> b;
-  return carve(cv, b, n, nnz, k) + 4096;
+  if (k != k0) {  // the padded copies of B and X
+    cv.take<double>(n * k);
+    if (is_complex) cv.take<cdouble>(n * k);
+    else cv.take<double>(n * k);
+    bytes = cv.used;
+  }
+  return bytes + 4096;
 }
 
 size_t rb_coarse_work_bytes(int64_t nc, int64_t nrhs, int32_t is_complex, int32_t precision) {
-  const int64_t k = std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols);
+  const int64_t k = solve_cols(std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols));
   Carver cv{nullptr, 0};
   if (nc < 1) return 0;
   if (is_complex) {
@@ -1611,6 +1672,18 @@ int rb_spmm(const rb_csr* A, int32_t kind, const void* X, void* Y, int64_t nrhs,
   if (nrhs > kMaxCols) return fail(RB_ESIZE, "rb_spmm: at most %lld columns", (long long)kMaxCols);
   const Shape sh = pick_shape(A->n, nrhs, 3);
   cudaStream_t st = as_stream(stream);
+  if (!shape_covers(sh, nrhs)) {
+    const unsigned g = (unsigned)std::min<int64_t>(ceil_div(A->n, 8), 148 * 16);
+    switch (kind) {
+      case RB_F64: spmm_any_kernel<double><<<g, 256, 0, st>>>(A->n, nrhs, A->indptr, A->indices, (const double*)A->val64, (const double*)X, (double*)Y); break;
+      case RB_C128: spmm_any_kernel<cdouble><<<g, 256, 0, st>>>(A->n, nrhs, A->indptr, A->indices, (const cdouble*)A->val64, (const cdouble*)X, (cdouble*)Y); break;
+      case RB_F32: spmm_any_kernel<float><<<g, 256, 0, st>>>(A->n, nrhs, A->indptr, A->indices, (const float*)A->val32, (const float*)X, (float*)Y); break;
+      case RB_C64: spmm_any_kernel<cfloat><<<g, 256, 0, st>>>(A->n, nrhs, A->indptr, A->indices, (const cfloat*)A->val32, (const cfloat*)X, (cfloat*)Y); break;
+      default: return fail(RB_EARG, "rb_spmm: bad kind");
+    }
+    RB_LAUNCH_CHECK();
+    return RB_OK;
+  }
   switch (kind) {
     case RB_F64: return spmm_t<double, EPI_STORE>(*A, (const double*)A->val64, (const double*)X, (double*)Y, nullptr, nullptr, nrhs, sh, st);
     case RB_C128: return spmm_t<cdouble, EPI_STORE>(*A, (const cdouble*)A->val64, (const cdouble*)X, (cdouble*)Y, nullptr, nullptr, nrhs, sh, st);

@@ -109,3 +109,47 @@ def test_coarse_auto_threshold():
     assert info["coarse_nc"] == 0  # below the node count where 'auto' turns it on
     _, _, _, _, info = forward_device(cfg, coarse=64)
     assert 0 < info["coarse_nc"] <= 64 * 2
+
+
+def ellipsoid_cfg(omega, nsrc, ndet):
+    """A 60 x 60 x 39 mm ellipsoid carved from a 1.5 mm Kuhn box (about 24k
+    nodes: many cubes of the coarse grid are partly or wholly empty), with a
+    high-contrast spherical inclusion (label 2: mua 0.08, mus 5) and optodes
+    on inner planes near the top and bottom."""
+    node, elem = kuhn_box([60, 60, 39], 1.5)
+    c = node[elem - 1].mean(axis=1)
+    keep = ((c[:, 0] - 30) / 30) ** 2 + ((c[:, 1] - 30) / 30) ** 2 + ((c[:, 2] - 19.5) / 19.5) ** 2 <= 1.0
+    elem = elem[keep]
+    used = np.unique(elem)
+    remap = np.zeros(node.shape[0] + 1, dtype=np.int64)
+    remap[used] = np.arange(1, used.size + 1)
+    node, elem = node[used - 1], remap[elem]
+    cc = node[elem - 1].mean(axis=1)
+    seg = np.where(np.sum((cc - [30, 30, 12]) ** 2, axis=1) <= 36.0, 2, 1).astype(np.int32)
+    rng = np.random.default_rng(7)
+    src = np.column_stack([rng.uniform(25, 35, nsrc), rng.uniform(25, 35, nsrc), np.full(nsrc, 36.0)])
+    det = np.column_stack([rng.uniform(25, 35, ndet), rng.uniform(25, 35, ndet), np.full(ndet, 3.0)])
+    cfg = dict(node=node, elem=elem, seg=seg, prop=np.array([[0, 0, 1, 1], [0.01, 1.0, 0, 1.37], [0.08, 5.0, 0, 1.37]]),
+               srcpos=src, srcdir=np.array([[0, 0, -1.0]]), detpos=det, detdir=np.array([[0, 0, 1.0]]), omega=omega)
+    cfg, _ = rbb.meshprep(cfg)
+    return cfg
+
+
+@pytest.mark.parametrize("omega", [0.0, 2 * np.pi * 1e8])
+@pytest.mark.parametrize("cols", [(3, 2), (20, 17)])
+def test_coarse_irregular_mesh_odd_columns(omega, cols):
+    """Partly empty aggregates, a 8x mua / 5x mus inclusion, 5 and 37 columns
+    (the narrow lane-group shapes of the aggregate-ordered kernels): the
+    solution matches the Jacobi-only and the plain FP64 solves."""
+    cfg = ellipsoid_cfg(omega, *cols)
+    d0, p0, _, _, i0 = forward_device(cfg, coarse=False)
+    d1, p1, _, _, i1 = forward_device(cfg, coarse=True)
+    d2, p2, _, _, i2 = forward_device(cfg, coarse=True, precision="fp64")
+    assert i0["flag"] == 0 and i1["flag"] == 0 and i2["flag"] == 0
+    assert 0 < i1["coarse_nc"] and i2["coarse_nc"] == i1["coarse_nc"]
+    assert i1["iters"] < i0["iters"], (i1["iters"], i0["iters"])
+    for p, d in ((p1, d1), (p2, d2)):
+        err = (torch.abs(p - p0).max() / torch.abs(p0).max()).item()
+        assert err <= 1e-9, err
+        derr = (torch.abs(d - d0) / torch.abs(d0)).max().item()
+        assert derr <= 1e-6, derr

@@ -266,6 +266,44 @@ def test_femsolve_row_group_spmm(golden, k, precision):
         assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-11
 
 
+@pytest.mark.parametrize("k", [33, 37, 66, 70, 127])
+def test_femsolve_column_counts_outside_the_lane_layout(golden, k):
+    """Odd counts above 32 and counts 2 mod 4 above 64 (the vector kernels'
+    lane layout covers 32 / 64 / 128 of those): the solve runs on a copy
+    padded with zero columns.  Against SuperLU, mixed and FP64, cold and warm;
+    rb_spmm at the same counts against scipy."""
+    import ctypes
+
+    from scipy import sparse
+    from scipy.sparse.linalg import splu
+
+    g = golden("nodal_fd")
+    A = sparse.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"]))
+    rng = np.random.default_rng(k)
+    b = rng.standard_normal((A.shape[0], k))
+    b[:, k - 1] = 0.0
+    ref = splu(A.tocsc()).solve(b.astype(complex))
+    for precision in ("mixed", "fp64"):
+        x, flag = rbb.femsolve(A, b, precision=precision)
+        assert flag == 0
+        assert np.all(x[:, k - 1] == 0)
+        assert np.abs(x - ref).max() / np.abs(ref).max() < 1e-11, precision
+    mat = engine.DeviceMatrix.from_scipy(A)
+    B = torch.as_tensor(b, device="cuda")
+    x_cold, i_cold = engine.solve(mat, B)
+    x_warm, i_warm = engine.solve(mat, B, x0=x_cold)
+    assert i_warm["iters"] == 0 and torch.equal(x_warm, x_cold)
+    # rb_spmm (FP64 complex values) at the same column count
+    X = torch.as_tensor(rng.standard_normal((A.shape[0], k)) + 1j * rng.standard_normal((A.shape[0], k)),
+                        device="cuda")
+    Y = torch.empty_like(X)
+    from redbirdpy_b200 import _lib
+
+    _lib.call("rb_spmm", ctypes.byref(mat.struct), _lib.RB_C128, _lib.ptr(X), _lib.ptr(Y), k, _lib.stream())
+    yref = A @ X.cpu().numpy()
+    assert np.abs(Y.cpu().numpy() - yref).max() / np.abs(yref).max() < 1e-13
+
+
 def test_pinned_result_pool_never_overwrites_live_arrays():
     """runforward copies phi into reused page-locked buffers: a buffer comes
     back only after the array from it, and every view of it, is gone."""
