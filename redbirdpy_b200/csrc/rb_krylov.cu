@@ -153,6 +153,8 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   typedef std::conditional_t<EPI == EPI_RESID, double, typename Scalar<T>::acc> A;
   A* part = reinterpret_cast<A*>(part_);
   __shared__ A sm[(EPI == EPI_STORE) ? 1 : kBlk * V];
+  __shared__ __align__(16) int32_t s_idx[L == 32 ? kBlk : 1];  // per-warp (index, value) chunks
+  __shared__ __align__(16) T s_val[L == 32 ? kBlk : 1];
   const int lane = threadIdx.x % L;
   const int64_t task0 = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L;
   const int64_t c0 = (task0 % S) * (int64_t)(L * V) + (int64_t)lane * V;
@@ -168,31 +170,30 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
 #pragma unroll
     for (int j = 0; j < V; ++j) y[j] = s_zero(T());
     if constexpr (L == 32) {
-      // whole warp on one row: lanes fetch the row's indices/values once and
-      // broadcast them by shuffle
+      // whole warp on one row: lanes fetch a chunk of the row's indices and
+      // values once (coalesced) into the warp's shared-memory slot, and every
+      // lane then reads U of them at a time with 16-byte broadcast loads.
+      // (Broadcasting by shuffle cost two L1 data-pipe wavefronts per nonzero,
+      // ~30% of that pipe, the SpMM's binding unit; this costs about 0.5.)
+      // The chunk is padded to a multiple of U with copies of its last index
+      // at coefficient 0 (same NaN behaviour as the exact product) rather
+      // than falling back to one dependent load at a time.
+      constexpr int U = (V * sizeof(T) <= 16) ? 8 : 4;
+      int32_t* const wi = s_idx + (threadIdx.x & ~31);
+      T* const wv = s_val + (threadIdx.x & ~31);
       for (int32_t p0 = b; p0 < e; p0 += 32) {
         const int cnt = min(32, e - p0);
-        int32_t my_i = 0;
-        T my_v = s_zero(T());
-        if (lane < cnt) {
-          my_i = indices[p0 + lane];
-          my_v = val[p0 + lane];
+        const int cntp = (cnt + U - 1) / U * U;
+        if (lane < cntp) {
+          wi[lane] = indices[p0 + min(lane, cnt - 1)];
+          wv[lane] = (lane < cnt) ? val[p0 + lane] : s_zero(T());
         }
-        // batches of U gathers in flight.  The last batch of a row is padded
-        // with copies of the row's last entry taken with coefficient 0 (same
-        // NaN behaviour as the exact product) rather than falling back to
-        // one dependent load at a time.
-        constexpr int U = (V * sizeof(T) <= 16) ? 8 : 4;
-        for (int j = 0; j < cnt; j += U) {
-          int32_t ii[U];
-          T aa[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int src = min(j + u, cnt - 1);
-            ii[u] = __shfl_sync(0xffffffffu, my_i, src);
-            const T a = shfl_s(my_v, src);
-            aa[u] = (j + u < cnt) ? a : s_zero(T());
-          }
+        __syncwarp();
+        for (int j = 0; j < cntp; j += U) {
+          alignas(16) int32_t ii[U];
+          alignas(16) T aa[U];
+          ldv_s<int32_t, U>(wi + j, ii);
+          ldv_s<T, U>(wv + j, aa);
           if (on) {
             alignas(16) T xv[U][V];
 #pragma unroll
@@ -203,6 +204,7 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
               for (int q = 0; q < V; ++q) y[q] = s_fma(aa[u], xv[u][q], y[q]);
           }
         }
+        __syncwarp();  // the slot is rewritten by the next chunk
       }
     } else if (on) {
 #pragma unroll 4
