@@ -24,86 +24,21 @@ constexpr int kGjB = 64;          // Gauss-Jordan block
 constexpr int kCoarseSplits = 8;  // most K splits of the X rc product
 
 // ------------------------------------------------------------------ GEMM
-// C = alpha A B + beta C (row-major; beta == 0 does not read C), 64 x 64
-// tiles, 16-deep k steps, 4 x 4 outputs per thread.  Split K: block z takes
-// the k range [z kchunk, (z + 1) kchunk) and writes C + z cstride.
-template <typename T>
-__global__ void __launch_bounds__(256) gemm_kernel(int64_t m, int64_t n, int64_t kk, T alpha, const T* __restrict__ A,
-                                                   int64_t lda, const T* __restrict__ B, int64_t ldb, T beta,
-                                                   T* __restrict__ C, int64_t ldc, int beta_zero, int64_t kchunk,
-                                                   int64_t cstride) {
-  __shared__ T As[16][64 + 1];
-  __shared__ T Bs[16][64 + 1];
-  const int tid = threadIdx.x;
-  const int tr = (tid >> 4) * 4, tc = (tid & 15) * 4;
-  const int64_t r0 = (int64_t)blockIdx.y * 64, c0 = (int64_t)blockIdx.x * 64;
-  const int64_t kb = (int64_t)blockIdx.z * kchunk, ke = std::min<int64_t>(kk, kb + kchunk);
-  C += (int64_t)blockIdx.z * cstride;
-  T acc[4][4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] = s_zero(T());
-  for (int64_t k0 = kb; k0 < ke; k0 += 16) {
-    for (int e = tid; e < 64 * 16; e += 256) {
-      const int i = e >> 4, q = e & 15;
-      As[q][i] = (r0 + i < m && k0 + q < ke) ? A[(r0 + i) * lda + k0 + q] : s_zero(T());
-      const int qb = e >> 6, j = e & 63;
-      Bs[qb][j] = (k0 + qb < ke && c0 + j < n) ? B[(k0 + qb) * ldb + c0 + j] : s_zero(T());
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      T a[4], b[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        a[u] = As[q][tr + u];
-        b[u] = Bs[q][tc + u];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = s_fma(a[u], b[v], acc[u][v]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int64_t i = r0 + tr + u, j = c0 + tc + v;
-      if (i < m && j < n) {
-        T x = s_mul(alpha, acc[u][v]);
-        if (!beta_zero) x = s_fma(beta, C[i * ldc + j], x);
-        C[i * ldc + j] = x;
-      }
-    }
-}
-
-template <typename T>
-static int gemm(int64_t m, int64_t n, int64_t kk, T alpha, const T* A, int64_t lda, const T* B, int64_t ldb, T beta,
-                bool beta_zero, T* C, int64_t ldc, cudaStream_t st, int splits = 1, int64_t cstride = 0) {
-  if (m <= 0 || n <= 0) return RB_OK;
-  const int64_t kchunk = ceil_div(ceil_div(kk, splits), 16) * 16;
-  dim3 g((unsigned)ceil_div(n, 64), (unsigned)ceil_div(m, 64), (unsigned)splits);
-  gemm_kernel<T><<<g, 256, 0, st>>>(m, n, kk, alpha, A, lda, B, ldb, beta, C, ldc, beta_zero ? 1 : 0, kchunk,
-                                    cstride);
-  RB_LAUNCH_CHECK();
-  return RB_OK;
-}
-
-// E_z = X[:, kz] RC[kz, :] for the coarse product, X symmetric (the
-// inverse of the symmetric aggregated operator): the A-operand tile element
-// (i, q) = X[q][i] is read along X's rows, so both operand tiles load
-// coalesced and land in shared memory untransposed.  64 x BN tiles, 16-deep
-// k steps, 256 threads with 4 x TN outputs each (a 4-vector of the X tile
-// and TN-vector of the RC tile per k step); the next k step's tiles are
-// fetched into registers while the current one is used.  Split K over
-// blockIdx.z as gemm_kernel.
-template <typename T, int BN>
-__global__ void __launch_bounds__(256) coarse_gemm_kernel(int64_t m, int64_t n, const T* __restrict__ X, int64_t ldx,
-                                                          const T* __restrict__ B, int64_t ldb, T* __restrict__ C,
-                                                          int64_t ldc, int64_t kchunk, int64_t cstride) {
+// C_z = alpha AT^T B + beta C (row-major; AT is kk x m, B is kk x n, so both
+// operand tiles load along rows and land in shared memory untransposed; beta
+// == 0 does not read C).  The coarse product passes X itself as AT (X is
+// symmetric: the inverse of the symmetric aggregated operator); Gauss-Jordan
+// passes the block column transposed.  64 x BN tiles, 16-deep k steps, 256
+// threads with 4 x BN/16 outputs each; the next k step's tiles are fetched
+// into registers while the current one is used.  Split K: block z takes the
+// k range [z kchunk, (z + 1) kchunk) and writes C + z cstride.  SCALE false:
+// C = AT^T B with a plain store (the coarse product; measured 0.054 against
+// 0.0625 ms per iteration with the scaled epilogue).
+template <typename T, int BN, bool SCALE>
+__global__ void __launch_bounds__(256) gemm_tn_kernel(int64_t m, int64_t n, int64_t kk, T alpha,
+                                                      const T* __restrict__ AT, int64_t lda, const T* __restrict__ B,
+                                                      int64_t ldb, T beta, int beta_zero, T* __restrict__ C,
+                                                      int64_t ldc, int64_t kchunk, int64_t cstride) {
   constexpr int BM = 64, BK = 16, TM = 4, TN = BN / 16;
   constexpr int LA = BM * BK / 256, LB = BN * BK / 256;  // tile elements each thread loads
   __shared__ __align__(16) T As[BK][BM];
@@ -111,7 +46,7 @@ __global__ void __launch_bounds__(256) coarse_gemm_kernel(int64_t m, int64_t n, 
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;  // output columns tx*TN.., rows ty*TM..
   const int64_t r0 = (int64_t)blockIdx.y * BM, c0 = (int64_t)blockIdx.x * BN;
-  const int64_t kb = (int64_t)blockIdx.z * kchunk, ke = std::min<int64_t>(m, kb + kchunk);  // X is m x m
+  const int64_t kb = (int64_t)blockIdx.z * kchunk, ke = std::min<int64_t>(kk, kb + kchunk);
   C += (int64_t)blockIdx.z * cstride;
   T acc[TM][TN];
 #pragma unroll
@@ -123,7 +58,7 @@ __global__ void __launch_bounds__(256) coarse_gemm_kernel(int64_t m, int64_t n, 
 #pragma unroll
     for (int l = 0; l < LA; ++l) {
       const int e = tid + 256 * l, q = e / BM, i = e % BM;
-      ra[l] = (k0 + q < ke && r0 + i < m) ? X[(k0 + q) * ldx + r0 + i] : s_zero(T());
+      ra[l] = (k0 + q < ke && r0 + i < m) ? AT[(k0 + q) * lda + r0 + i] : s_zero(T());
     }
 #pragma unroll
     for (int l = 0; l < LB; ++l) {
@@ -164,8 +99,45 @@ __global__ void __launch_bounds__(256) coarse_gemm_kernel(int64_t m, int64_t n, 
 #pragma unroll
     for (int v = 0; v < TN; ++v) {
       const int64_t i = r0 + ty * TM + u, j = c0 + tx * TN + v;
-      if (i < m && j < n) C[i * ldc + j] = acc[u][v];
+      if (i < m && j < n) {
+        if constexpr (SCALE) {
+          T x = s_mul(alpha, acc[u][v]);
+          if (!beta_zero) x = s_fma(beta, C[i * ldc + j], x);
+          C[i * ldc + j] = x;
+        } else {
+          C[i * ldc + j] = acc[u][v];
+        }
+      }
     }
+}
+
+// 64 x 64 tiles (79 registers for FP32, three blocks per SM): coarse product
+// and dot 54 us per iteration at nc = 2048, k = 128 against 67 us with 64 x 128
+// tiles (127 registers, two blocks per SM); complex128 takes 64 x 32 tiles
+template <typename T> constexpr int gemm_bn() { return sizeof(T) >= 16 ? 32 : 64; }
+
+template <typename T> static T h_real(double v);
+static bool h_is_one(float a) { return a == 1.0f; }
+static bool h_is_one(double a) { return a == 1.0; }
+static bool h_is_one(cfloat a) { return a.x == 1.0f && a.y == 0.0f; }
+static bool h_is_one(cdouble a) { return a.x == 1.0 && a.y == 0.0; }
+
+template <typename T>
+static int gemm_tn(int64_t m, int64_t n, int64_t kk, T alpha, const T* AT, int64_t lda, const T* B, int64_t ldb,
+                   T beta, bool beta_zero, T* C, int64_t ldc, cudaStream_t st, int splits = 1, int64_t cstride = 0) {
+  if (m <= 0 || n <= 0) return RB_OK;
+  constexpr int BN = gemm_bn<T>();
+  const int64_t kchunk = ceil_div(ceil_div(kk, splits), 16) * 16;
+  dim3 g((unsigned)ceil_div(n, BN), (unsigned)ceil_div(m, 64), (unsigned)splits);
+  const bool plain = beta_zero && h_is_one(alpha);
+  if (plain)
+    gemm_tn_kernel<T, BN, false><<<g, 256, 0, st>>>(m, n, kk, alpha, AT, lda, B, ldb, beta, 1, C, ldc, kchunk,
+                                                   cstride);
+  else
+    gemm_tn_kernel<T, BN, true><<<g, 256, 0, st>>>(m, n, kk, alpha, AT, lda, B, ldb, beta, beta_zero ? 1 : 0, C, ldc,
+                                                  kchunk, cstride);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
 }
 
 __device__ __forceinline__ double s_inv(double a) { return 1.0 / a; }
@@ -231,14 +203,15 @@ __global__ void __launch_bounds__(256) gj_diag_kernel(const T* __restrict__ A, i
   }
 }
 
-// Cb[i][j] = A[i][b0 + j] (rows of the block itself zero); nc x nb, ld kGjB
+// CbT[j][i] = A[i][b0 + j], the block column transposed (rows of the block
+// itself zero); kGjB x nc, ld nc
 template <typename T>
-__global__ void gj_cols_kernel(const T* __restrict__ A, int64_t nc, int64_t b0, int nb, T* __restrict__ Cb) {
+__global__ void gj_cols_kernel(const T* __restrict__ A, int64_t nc, int64_t b0, int nb, T* __restrict__ CbT) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nc * kGjB;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e / kGjB;
-    const int j = (int)(e % kGjB);
-    Cb[e] = (j < nb && (i < b0 || i >= b0 + nb)) ? A[i * nc + b0 + j] : s_zero(T());
+    const int j = (int)(e / nc);
+    const int64_t i = e % nc;
+    CbT[e] = (j < nb && (i < b0 || i >= b0 + nb)) ? A[i * nc + b0 + j] : s_zero(T());
   }
 }
 
@@ -424,7 +397,7 @@ struct CoarseOp {
 template <typename T64, typename T>
 struct CoarseBufs {
   CoarseOp<T> op;
-  T64 *A64 = nullptr, *Rb = nullptr, *Cb = nullptr, *Dinv = nullptr;
+  T64 *A64 = nullptr, *Rb = nullptr, *Cb = nullptr, *Dinv = nullptr;  // Cb: the block column, transposed
   int* err = nullptr;
 };
 
@@ -462,15 +435,16 @@ static int coarse_setup(const rb_csr& A, CoarseBufs<T64, T>& c, cudaStream_t st)
     const int nb = (int)std::min<int64_t>(kGjB, nc - b0);
     gj_diag_kernel<T64><<<1, 256, gj_smem, st>>>(c.A64, nc, b0, nb, c.Dinv, c.err);
     RB_LAUNCH_CHECK();
-    // R = Dinv A[b, :]
-    RB_TRY(gemm<T64>(nb, nc, nb, one, c.Dinv, kGjB, c.A64 + b0 * nc, nc, zero, true, c.Rb, nc, st));
-    // Cb = A[:, b] with the block's own rows zeroed
+    // R = Dinv A[b, :]  (Dinv is symmetric: the inverse of a diagonal block
+    // of the symmetric Schur complement, so it serves as its own transpose)
+    RB_TRY(gemm_tn<T64>(nb, nc, nb, one, c.Dinv, kGjB, c.A64 + b0 * nc, nc, zero, true, c.Rb, nc, st));
+    // CbT = (A[:, b])^T with the block's own rows zeroed
     gj_cols_kernel<T64><<<eg, 256, 0, st>>>(c.A64, nc, b0, nb, c.Cb);
     RB_LAUNCH_CHECK();
     // A -= Cb R (rank-nb update of every row outside the block)
-    RB_TRY(gemm<T64>(nc, nc, nb, mone, c.Cb, kGjB, c.Rb, nc, one, false, c.A64, nc, st));
+    RB_TRY(gemm_tn<T64>(nc, nc, nb, mone, c.Cb, nc, c.Rb, nc, one, false, c.A64, nc, st));
     // A[:, b] = -Cb Dinv outside the block; A[b, :] = R; A[b, b] = Dinv
-    RB_TRY(gemm<T64>(nc, nb, nb, mone, c.Cb, kGjB, c.Dinv, kGjB, zero, true, c.A64 + b0, nc, st));
+    RB_TRY(gemm_tn<T64>(nc, nb, nb, mone, c.Cb, nc, c.Dinv, kGjB, zero, true, c.A64 + b0, nc, st));
     gj_rows_kernel<T64><<<eg, 256, 0, st>>>(c.A64, nc, b0, nb, c.Rb, c.Dinv);
     RB_LAUNCH_CHECK();
   }
@@ -495,32 +469,13 @@ static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_
     RB_LAUNCH_CHECK();
   }
   // enough blocks for two per SM: split the nc-long sums (fixed order, no atomics)
-  if constexpr (std::is_same<T, cdouble>::value) {
-    const T one = h_real<T>(1.0), zero = h_real<T>(0.0);
-    const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, 64);
-    const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
-                                                                     ceil_div(nc, 256)}));
-    RB_TRY(gemm<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k));
-    coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec,
-                                                    (typename Scalar<T>::acc*)c.part);
-    RB_LAUNCH_CHECK();
-  } else {
-    // 64 x 64 tiles (79 registers for FP32, three blocks per SM): product and
-    // dot 54 us per iteration at nc = 2048, k = 128 against 67 us with 64 x 128
-    // tiles (127 registers, two blocks per SM); 8-byte scalars would need ~180
-    // registers for 64 x 128
-    const int bn = 64;
-    const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, bn);
-    const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
-                                                                     ceil_div(nc, 256)}));
-    const int64_t kchunk = ceil_div(ceil_div(nc, splits), 16) * 16;
-    dim3 g((unsigned)ceil_div(k, bn), (unsigned)ceil_div(nc, 64), (unsigned)splits);
-    coarse_gemm_kernel<T, 64><<<g, 256, 0, st>>>(nc, k, c.X, nc, c.rc, k, c.es, k, kchunk, nc * k);
-    RB_LAUNCH_CHECK();
-    coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec,
-                                                    (typename Scalar<T>::acc*)c.part);
-    RB_LAUNCH_CHECK();
-  }
+  const T one = h_real<T>(1.0), zero = h_real<T>(0.0);
+  const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, gemm_bn<T>());
+  const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
+                                                                   ceil_div(nc, 256)}));
+  RB_TRY(gemm_tn<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k));
+  coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec, (typename Scalar<T>::acc*)c.part);
+  RB_LAUNCH_CHECK();
   return RB_OK;
 }
 
