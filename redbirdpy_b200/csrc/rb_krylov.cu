@@ -144,7 +144,9 @@ enum { EPI_STORE = 0, EPI_PQDOT = 1, EPI_RESID = 2 };
 // takes (row, slice) tasks, slice = task % S, so that a lane keeps 16 bytes
 // per gathered row and 8 gathers in flight; the group count is a multiple of
 // S, so a group always sees the same slice (and its column sums stay put).
-template <typename T, int L, int V, int EPI, int S = 1>
+// O32: n k < 2^31, so that the staged x row offsets (index k, in elements)
+// fit an int32 and a gather address is one wide multiply-add
+template <typename T, int L, int V, int EPI, int S = 1, bool O32 = true>
 __global__ void __launch_bounds__(kBlk, BpsSpmm<T>::value)
 spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
             const T* __restrict__ val, const T* __restrict__ X, T* __restrict__ Y,
@@ -153,8 +155,10 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   typedef std::conditional_t<EPI == EPI_RESID, double, typename Scalar<T>::acc> A;
   A* part = reinterpret_cast<A*>(part_);
   __shared__ A sm[(EPI == EPI_STORE) ? 1 : kBlk * V];
-  __shared__ __align__(16) int32_t s_idx[L == 32 ? kBlk : 1];  // per-warp (index, value) chunks
+  __shared__ __align__(16) int32_t s_off[L == 32 ? kBlk : 1];  // per-warp (x row offset or index, value) chunks
   __shared__ __align__(16) T s_val[L == 32 ? kBlk : 1];
+  // what a chunk entry holds: the x row offset index * k (O32), else the index
+  auto staged = [&](int32_t idx) -> int32_t { return O32 ? idx * (int32_t)k : idx; };
   const int lane = threadIdx.x % L;
   const int64_t task0 = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L;
   const int64_t c0 = (task0 % S) * (int64_t)(L * V) + (int64_t)lane * V;
@@ -172,13 +176,13 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
   constexpr bool PIPE = (L == 32) && std::is_same<T, float>::value;
   constexpr int U = (V * sizeof(T) <= 16) ? 8 : 4;
   const int64_t ntask = n * S;
-  auto chunk0 = [&](int32_t bb, int32_t ee, int32_t& ii, T& vv) {
+  auto chunk0 = [&](int32_t bb, int32_t ee, int32_t& oo, T& vv) {
     const int c = min(32, ee - bb);
     const int cp = (c + U - 1) / U * U;
-    ii = 0;
+    oo = 0;
     vv = s_zero(T());
     if (lane < cp) {
-      ii = indices[bb + min(lane, c - 1)];
+      oo = staged(indices[bb + min(lane, c - 1)]);
       if (lane < c) vv = val[bb + lane];
     }
   };
@@ -210,15 +214,19 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
     for (int j = 0; j < V; ++j) y[j] = s_zero(T());
     if constexpr (L == 32) {
       // whole warp on one row: lanes fetch a chunk of the row's indices and
-      // values once (coalesced) into the warp's shared-memory slot, and every
-      // lane then reads U of them at a time with 16-byte broadcast loads.
-      // (Broadcasting by shuffle cost two L1 data-pipe wavefronts per nonzero,
-      // ~30% of that pipe, the SpMM's binding unit; this costs about 0.5.)
-      // The chunk is padded to a multiple of U with copies of its last index
-      // at coefficient 0 (same NaN behaviour as the exact product) rather
-      // than falling back to one dependent load at a time.
-      int32_t* const wi = s_idx + (threadIdx.x & ~31);
+      // values once (coalesced) into the warp's shared-memory slot, the index
+      // already turned into the element offset of its x row, and every lane
+      // then reads U of them at a time with 16-byte broadcast loads and
+      // gathers from its own base pointer with one wide multiply-add.  (Broadcasting by
+      // shuffle cost two L1 data-pipe wavefronts per nonzero, ~30% of that
+      // pipe, the SpMM's binding unit; the index arithmetic per gather was
+      // most of the issued instructions.)  The chunk is padded to a multiple
+      // of U with copies of its last index at coefficient 0 (same NaN
+      // behaviour as the exact product) rather than falling back to one
+      // dependent load at a time.
+      int32_t* const wo = s_off + (threadIdx.x & ~31);
       T* const wv = s_val + (threadIdx.x & ~31);
+      const T* const xl = X + c0;  // this lane's columns of x row 0
       int32_t pb2 = 0, pe2 = 0, ni = 0;
       T nv = s_zero(T());
       if constexpr (PIPE) {
@@ -234,23 +242,26 @@ spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int3
         const int cntp = (cnt + U - 1) / U * U;
         if (PIPE && p0 == b) {
           if (lane < cntp) {
-            wi[lane] = ci;
+            wo[lane] = ci;
             wv[lane] = cv;
           }
         } else if (lane < cntp) {
-          wi[lane] = indices[p0 + min(lane, cnt - 1)];
+          wo[lane] = staged(indices[p0 + min(lane, cnt - 1)]);
           wv[lane] = (lane < cnt) ? val[p0 + lane] : s_zero(T());
         }
         __syncwarp();
         for (int j = 0; j < cntp; j += U) {
-          alignas(16) int32_t ii[U];
+          alignas(16) int32_t oo[U];
           alignas(16) T aa[U];
-          ldv_s<int32_t, U>(wi + j, ii);
+          ldv_s<int32_t, U>(wo + j, oo);
           ldv_s<T, U>(wv + j, aa);
           if (on) {
             alignas(16) T xv[U][V];
 #pragma unroll
-            for (int u = 0; u < U; ++u) ldv<T, V>(X + (int64_t)ii[u] * k + c0, xv[u]);
+            for (int u = 0; u < U; ++u) {
+              const T* src = O32 ? xl + (uint32_t)oo[u] : xl + (int64_t)oo[u] * k;
+              ldv<T, V>(src, xv[u]);
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -1218,9 +1229,21 @@ static Shape pick_spmm_shape(int64_t n, int64_t k) {
 template <typename T, int EPI>
 int spmm_t(const rb_csr& A, const T* val, const T* X, T* Y, const double* B, void* part, int64_t k,
            const Shape& sh, cudaStream_t st) {
+  const bool o32 = (uint64_t)A.n * (uint64_t)k < (1ull << 31);
   if (sh.S == 2) {
     if (sh.L != 32 || sh.V != 2 || k != 128) return fail(RB_EARG, "bad sliced SpMM shape");
-    spmm_kernel<T, 32, 2, EPI, 2><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+    if (o32)
+      spmm_kernel<T, 32, 2, EPI, 2, true><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+    else
+      spmm_kernel<T, 32, 2, EPI, 2, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+    RB_LAUNCH_CHECK();
+    return RB_OK;
+  }
+  if (sh.L == 32 && !o32) {  // offsets beyond int32: the 64-bit index arithmetic
+#define RB_SPMM(L_, V_) \
+  spmm_kernel<T, L_, V_, EPI, 1, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part)
+    RB_DISPATCH_LV(sh, RB_SPMM);
+#undef RB_SPMM
     RB_LAUNCH_CHECK();
     return RB_OK;
   }
