@@ -341,10 +341,13 @@ template <typename T> struct GrpCfg {
   static constexpr int C = 4096 / (32 * 4 * (int)sizeof(T)) > 0 ? 4096 / (32 * 4 * (int)sizeof(T)) : 1;
 };
 template <> struct GrpCfg<float> {
-  static constexpr bool enabled = false;
-  static constexpr int G = 8;
-  static constexpr int C = 8;  // union entries per chunk (2 chunks in flight)
+  static constexpr bool enabled = false;  // FP32 takes the row-pair SpMM below
+  static constexpr int G = 2;             // rows per group of its union plan
+  static constexpr int C = 8;
 };
+// FP32 row-pair SpMM: used at 65..128 columns (multiples of 4: L = 32, V = 4)
+template <typename T> struct PairCfg { static constexpr bool enabled = std::is_same<T, float>::value; };
+static bool pair_cols_ok(int64_t k) { return k > 64 && k <= 128 && k % 4 == 0; }
 constexpr int kGrpWarps = 4;     // warps per block
 constexpr int kGrpVals = 256;    // staged matrix values per group (else read from global)
 constexpr int kWaitSpins = 1 << 22;
@@ -599,6 +602,107 @@ template <typename T>
 constexpr size_t grp_smem_bytes() {
   return (size_t)kGrpWarps *
          ((size_t)2 * GrpCfg<T>::C * 32 * 4 * sizeof(T) + (size_t)kGrpVals * sizeof(T) + 16);
+}
+
+// ----------------------------------------------------- row-pair SpMM (FP32)
+// A warp takes rows 2t and 2t+1 together and walks the union of their
+// column lists (the group plan with G = 2: ascending columns, each with a
+// 2-bit mask of the rows holding it), gathering each x row once and applying
+// it to both rows (coefficient 0 where a row lacks the column).  On the
+// tetrahedral box the union holds 73% of the two rows' nonzeros, so 27% fewer
+// 512-byte gathers go through L1, the per-row kernel's binding unit, for
+// twice the FMAs per gather.  A row's coefficients come straight from its
+// CSR values: the position of a union entry within row r is the count of
+// earlier entries with bit r set (warp ballot + popc, carried across chunks).
+// Chunks of 32 union entries are staged in shared memory as (x row offset,
+// coefficient of row 0, coefficient of row 1), padded to a multiple of U with
+// the last offset at coefficient 0.  EPI as spmm_kernel (PQDOT only here).
+template <int EPI>
+__global__ void __launch_bounds__(kBlk, BpsSpmm<float>::value)
+spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const float* __restrict__ val, GroupPlan gp,
+                 const float* __restrict__ X, float* __restrict__ Y, void* __restrict__ part_) {
+  constexpr int V = 4, U = 8;
+  typedef double A;
+  static_assert(EPI == EPI_PQDOT, "row-pair SpMM: p.Ap epilogue only");
+  __shared__ A sm[kBlk * V];
+  __shared__ __align__(16) int32_t s_off[kBlk];
+  __shared__ __align__(16) float s_va[kBlk];
+  __shared__ __align__(16) float s_vb[kBlk];
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t c0 = (int64_t)lane * V;
+  const bool on = c0 < k;
+  const int64_t groups = (int64_t)gridDim.x * (kBlk / 32);
+  int32_t* const wo = s_off + (threadIdx.x & ~31);
+  float* const wa = s_va + (threadIdx.x & ~31);
+  float* const wb = s_vb + (threadIdx.x & ~31);
+  const float* const xl = X + c0;
+  alignas(16) A acc[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) acc[j] = 0.0;
+  for (int64_t t = blockIdx.x * (int64_t)(kBlk / 32) + (threadIdx.x >> 5); t < gp.ng; t += groups) {
+    const int64_t r0 = 2 * t;
+    const bool has1 = r0 + 1 < n;
+    const int32_t ub = gp.gptr[t], ue = gp.gptr[t + 1];
+    const int32_t ba = indptr[r0], bb = indptr[r0 + 1];  // value ranges of rows r0 and r0 + 1
+    int32_t ca = 0, cb = 0;                              // entries of each row consumed so far
+    alignas(16) float ya[V], yb[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) ya[j] = yb[j] = 0.f;
+    for (int32_t u0 = ub; u0 < ue; u0 += 32) {
+      const int cnt = min(32, ue - u0);
+      const int cntp = (cnt + U - 1) / U * U;
+      const bool in = lane < cnt;
+      const int32_t col = in ? gp.ucol[u0 + lane] : 0;
+      const uint32_t m = in ? gp.umask[u0 + lane] : 0u;
+      const unsigned bma = __ballot_sync(0xffffffffu, m & 1u), bmb = __ballot_sync(0xffffffffu, m & 2u);
+      const float va = (m & 1u) ? val[ba + ca + __popc(bma & lt)] : 0.f;
+      const float vb = (m & 2u) ? val[bb + cb + __popc(bmb & lt)] : 0.f;
+      ca += __popc(bma);
+      cb += __popc(bmb);
+      const int32_t last = __shfl_sync(0xffffffffu, col, cnt - 1);
+      if (lane < cntp) {
+        wo[lane] = (in ? col : last) * (int32_t)k;
+        wa[lane] = va;
+        wb[lane] = vb;
+      }
+      __syncwarp();
+      for (int j = 0; j < cntp; j += U) {
+        alignas(16) int32_t oo[U];
+        ldv_s<int32_t, U>(wo + j, oo);
+        if (on) {
+          alignas(16) float xv[U][V];
+#pragma unroll
+          for (int u = 0; u < U; ++u) ldv<float, V>(xl + (uint32_t)oo[u], xv[u]);
+          alignas(16) float aa[U], bbv[U];
+          ldv_s<float, U>(wa + j, aa);
+          ldv_s<float, U>(wb + j, bbv);
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+              ya[q] = fmaf(aa[u], xv[u][q], ya[q]);
+              yb[q] = fmaf(bbv[u], xv[u][q], yb[q]);
+            }
+        }
+      }
+      __syncwarp();  // the slot is rewritten by the next chunk
+    }
+    if (on) {
+      alignas(16) float pv[V];
+      ldv<float, V>(X + r0 * k + c0, pv);
+#pragma unroll
+      for (int j = 0; j < V; ++j) acc[j] = acc_fma(pv[j], ya[j], acc[j]);
+      stv<float, V>(Y + r0 * k + c0, ya);
+      if (has1) {
+        ldv<float, V>(X + (r0 + 1) * k + c0, pv);
+#pragma unroll
+        for (int j = 0; j < V; ++j) acc[j] = acc_fma(pv[j], yb[j], acc[j]);
+        stv<float, V>(Y + (r0 + 1) * k + c0, yb);
+      }
+    }
+  }
+  block_colreduce<A, 32, V>(acc, reinterpret_cast<A*>(part_), k, sm);
 }
 
 // ------------------------------------------------------- CG vector kernels
@@ -1291,6 +1395,18 @@ static int spmm_grp(const rb_csr& A, const T* val, const GroupPlan& gp, const T*
   }
 }
 
+template <int EPI>
+static int spmm_pair(const rb_csr& A, const float* val, const GroupPlan& gp, const float* X, float* Y, void* part,
+                     int64_t k, unsigned* grid_out, cudaStream_t st) {
+  if (!pair_cols_ok(k) || A.n * k >= (int64_t(1) << 31)) return fail(RB_EARG, "row-pair SpMM: %lld columns", (long long)k);
+  const unsigned grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(num_sms() * BpsSpmm<float>::value, ceil_div(gp.ng, kBlk / 32)));
+  spmm_pair_kernel<EPI><<<grid, kBlk, 0, st>>>(A.n, k, A.indptr, val, gp, X, Y, part);
+  RB_LAUNCH_CHECK();
+  *grid_out = grid;
+  return RB_OK;
+}
+
 // union lists of the row groups: count, scan, fill
 template <int G>
 static int build_group_plan(const rb_csr& A, int32_t* gcnt, int32_t* gptr, int32_t* ucol, uint8_t* umask,
@@ -1456,7 +1572,11 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       RB_TRY(tm.record(st));
       unsigned nb = shs.grid;
       if (gp) {
-        RB_TRY((spmm_grp<T, EPI_PQDOT>(A, val, *gp, P, Q, nullptr, part_a, k, counter + 2, &nb, st)));
+        if constexpr (PairCfg<T>::enabled) {
+          RB_TRY((spmm_pair<EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st)));
+        } else {
+          RB_TRY((spmm_grp<T, EPI_PQDOT>(A, val, *gp, P, Q, nullptr, part_a, k, counter + 2, &nb, st)));
+        }
       } else {
         RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, shs, st)));
       }
@@ -1627,8 +1747,10 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     info.launches += 3 + 5 * (int)ceil_div(cb.op.nc, kGjB);
   }
   GroupPlan gp{nullptr, nullptr, nullptr, 0};
-  if (GrpCfg<T>::enabled && grp_cols_ok(kb) && n > 0) RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask,
-                                                                      b.scan_work, b.scan_bytes, &gp, st));
+  const bool plan = (GrpCfg<T>::enabled && grp_cols_ok(kb)) ||
+                    (PairCfg<T>::enabled && pair_cols_ok(kb) && n * kb < (int64_t(1) << 31));
+  if (plan && n > 0)
+    RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask, b.scan_work, b.scan_bytes, &gp, st));
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * kb, 256), 148 * 16);
   if (Bp) {
     copy_cols_kernel<double><<<eg, 256, 0, st>>>(n, nrhs, kb, B, Bp);
