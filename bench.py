@@ -217,6 +217,8 @@ def run_b200(args):
 
     # roofline of the SpMM kernel (dominant bytes per Krylov iteration)
     n, nnz, k = mesh.nn, mesh.nnz, nrhs
+    # the product's own bytes: the CSR matrix (FP32 values, int32 indices) and
+    # x and y once each, whatever plan the kernel walks
     spmm_bytes = nnz * (4 + 4) + 4 * (n + 1) + 2 * k * n * 4
     # x, r, p, q read + x, r written (FP32), dinv and the aggregate row list
     # read, the restricted residual (nc x k) written
@@ -285,11 +287,11 @@ def run_b200(args):
                                                / max(1, sum(i["coarse_launches"] for i in pinfos)), 4),
                    "jacobi_only_ms_per_step": round(ms_jac, 3), "jacobi_only_iters": infos_jac[-1]["iters"]},
         "gpu_launches": int(sum(i["launches"] for i in infos) / len(infos)) + 6,
-        "roofline": {"bound": "hbm", "kernel": "spmm_kernel<float> (CSR SpMM, 128 RHS, fused p.Ap)",
+        "roofline": {"bound": "hbm", "kernel": "spmm_pair_kernel (FP32 CSR SpMM, two rows per warp over their column union, 128 RHS, fused p.Ap)",
                      "achieved": round(sp_gbs, 1) if sp_gbs else None, "peak": peak, "unit": "GB/s",
                      "frac": round(sp_gbs / peak, 4) if sp_gbs else None, "peak_source": peak_kind,
                      "algorithmic_bytes": spmm_bytes, "launch_ms": round(sp_ms, 4),
-                     "traffic": traffic.get("spmm_kernel<float,32,4,EPI_PQDOT>"),
+                     "traffic": traffic.get("spmm_pair_kernel<EPI_PQDOT>"),
                      "traffic_source": "ncu capture, profiles/forward_3Mtet_128rhs_launches_and_kernels.md"},
         "roofline_update": {"kernel": "cg_update_agg_kernel<float> (x, r update + r.z, r.r, coarse restriction)",
                             "achieved": round(up_gbs, 1) if up_gbs else None,
