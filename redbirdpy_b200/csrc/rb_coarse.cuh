@@ -38,7 +38,9 @@ template <typename T, int BN, bool SCALE>
 __global__ void __launch_bounds__(256) gemm_tn_kernel(int64_t m, int64_t n, int64_t kk, T alpha,
                                                       const T* __restrict__ AT, int64_t lda, const T* __restrict__ B,
                                                       int64_t ldb, T beta, int beta_zero, T* __restrict__ C,
-                                                      int64_t ldc, int64_t kchunk, int64_t cstride) {
+                                                      int64_t ldc, int64_t kchunk, int64_t cstride,
+                                                      const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // inside the Krylov loop: every column converged
   constexpr int BM = 64, BK = 16, TM = 4, TN = BN / 16;
   constexpr int LA = BM * BK / 256, LB = BN * BK / 256;  // tile elements each thread loads
   __shared__ __align__(16) T As[BK][BM];
@@ -124,7 +126,8 @@ static bool h_is_one(cdouble a) { return a.x == 1.0 && a.y == 0.0; }
 
 template <typename T>
 static int gemm_tn(int64_t m, int64_t n, int64_t kk, T alpha, const T* AT, int64_t lda, const T* B, int64_t ldb,
-                   T beta, bool beta_zero, T* C, int64_t ldc, cudaStream_t st, int splits = 1, int64_t cstride = 0) {
+                   T beta, bool beta_zero, T* C, int64_t ldc, cudaStream_t st, int splits = 1, int64_t cstride = 0,
+                   const int32_t* live = nullptr) {
   if (m <= 0 || n <= 0) return RB_OK;
   constexpr int BN = gemm_bn<T>();
   const int64_t kchunk = ceil_div(ceil_div(kk, splits), 16) * 16;
@@ -132,10 +135,10 @@ static int gemm_tn(int64_t m, int64_t n, int64_t kk, T alpha, const T* AT, int64
   const bool plain = beta_zero && h_is_one(alpha);
   if (plain)
     gemm_tn_kernel<T, BN, false><<<g, 256, 0, st>>>(m, n, kk, alpha, AT, lda, B, ldb, beta, 1, C, ldc, kchunk,
-                                                   cstride);
+                                                   cstride, live);
   else
     gemm_tn_kernel<T, BN, true><<<g, 256, 0, st>>>(m, n, kk, alpha, AT, lda, B, ldb, beta, beta_zero ? 1 : 0, C, ldc,
-                                                  kchunk, cstride);
+                                                  kchunk, cstride, live);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }
@@ -294,7 +297,9 @@ __global__ void cast_kernel(int64_t count, const T64* __restrict__ a, T* __restr
 template <typename T>
 __global__ void __launch_bounds__(256) restrict_kernel(int64_t nc, int64_t k, const T* __restrict__ R,
                                                        const int32_t* __restrict__ agg_ptr,
-                                                       const int32_t* __restrict__ agg_rows, T* __restrict__ rc) {
+                                                       const int32_t* __restrict__ agg_rows, T* __restrict__ rc,
+                                                       const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // inside the Krylov loop: every column converged
   typedef typename Scalar<T>::acc A;
   __shared__ A red[8][128];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -347,7 +352,9 @@ template <typename T>
 __global__ void __launch_bounds__(256) coarse_dot_kernel(int64_t nc, int64_t k, const T* __restrict__ rc,
                                                          const T* __restrict__ es, int splits,
                                                          T* __restrict__ ec,
-                                                         typename Scalar<T>::acc* __restrict__ part) {
+                                                         typename Scalar<T>::acc* __restrict__ part,
+                                                         const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // inside the Krylov loop: every column converged
   typedef typename Scalar<T>::acc A;
   __shared__ A red[8][128];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -459,13 +466,14 @@ static int coarse_setup(const rb_csr& A, CoarseBufs<T64, T>& c, cudaStream_t st)
 }
 
 // rc = P^T r (unless R is NULL: rc already holds it), ec = X rc,
-// part = column sums of rc * ec
+// part = column sums of rc * ec; live as the Krylov loop's kernels
 template <typename T>
-static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_t st) {
+static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_t st,
+                        const int32_t* live = nullptr) {
   const int64_t nc = c.nc;
   if (R) {
     restrict_kernel<T><<<(unsigned)std::min<int64_t>(nc, 148 * 16), 256, 0, st>>>(nc, k, R, c.agg_ptr, c.agg_rows,
-                                                                                  c.rc);
+                                                                                  c.rc, live);
     RB_LAUNCH_CHECK();
   }
   // enough blocks for two per SM: split the nc-long sums (fixed order, no atomics)
@@ -473,8 +481,9 @@ static int coarse_apply(const CoarseOp<T>& c, const T* R, int64_t k, cudaStream_
   const int64_t tiles = ceil_div(nc, 64) * ceil_div(k, gemm_bn<T>());
   const int splits = (int)std::max<int64_t>(1, std::min<int64_t>({kCoarseSplits, ceil_div(2 * 148, tiles),
                                                                    ceil_div(nc, 256)}));
-  RB_TRY(gemm_tn<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k));
-  coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec, (typename Scalar<T>::acc*)c.part);
+  RB_TRY(gemm_tn<T>(nc, k, nc, one, c.X, nc, c.rc, k, zero, true, c.es, k, st, splits, nc * k, live));
+  coarse_dot_kernel<T><<<kCdotGrid, 256, 0, st>>>(nc, k, c.rc, c.es, splits, c.ec, (typename Scalar<T>::acc*)c.part,
+                                                  live);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }

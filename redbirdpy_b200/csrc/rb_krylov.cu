@@ -150,7 +150,8 @@ template <typename T, int L, int V, int EPI, int S = 1, bool O32 = true>
 __global__ void __launch_bounds__(kBlk, BpsSpmm<T>::value)
 spmm_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
             const T* __restrict__ val, const T* __restrict__ X, T* __restrict__ Y,
-            const double* __restrict__ B, void* __restrict__ part_) {
+            const double* __restrict__ B, void* __restrict__ part_, const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // every column converged: a no-op iteration
   // residual norms accumulate |r|^2 in double; dot products in the acc type
   typedef std::conditional_t<EPI == EPI_RESID, double, typename Scalar<T>::acc> A;
   A* part = reinterpret_cast<A*>(part_);
@@ -462,7 +463,8 @@ template <typename T, int V, int EPI>
 __global__ void __launch_bounds__(kGrpWarps * 32)
 spmm_grp_kernel(int64_t n, const int32_t* __restrict__ indptr, const T* __restrict__ val, GroupPlan gp,
                 const T* __restrict__ X, T* __restrict__ Y, const double* __restrict__ B, void* __restrict__ part_,
-                int32_t* __restrict__ err) {
+                int32_t* __restrict__ err, const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // every column converged: a no-op iteration
   constexpr int G = GrpCfg<T>::G, C = GrpCfg<T>::C;
   constexpr int64_t k = 32 * V;
   constexpr uint32_t rowbytes = (uint32_t)(k * sizeof(T));
@@ -620,7 +622,9 @@ constexpr size_t grp_smem_bytes() {
 template <int EPI>
 __global__ void __launch_bounds__(kBlk, BpsSpmm<float>::value)
 spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const float* __restrict__ val, GroupPlan gp,
-                 const float* __restrict__ X, float* __restrict__ Y, void* __restrict__ part_) {
+                 const float* __restrict__ X, float* __restrict__ Y, void* __restrict__ part_,
+                 const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // every column converged: a no-op iteration
   constexpr int V = 4, U = 8;
   typedef double A;
   static_assert(EPI == EPI_PQDOT, "row-pair SpMM: p.Ap epilogue only");
@@ -794,7 +798,9 @@ template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
                  T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
-                 typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr) {
+                 typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr,
+                 const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // every column converged: a no-op iteration
   typedef typename Scalar<T>::acc A;
   __shared__ A sm[kBlk * V];
   __shared__ double smr[kBlk * V];
@@ -915,7 +921,8 @@ cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, con
                      T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
                      const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
                      T* __restrict__ rc, typename Scalar<T>::acc* __restrict__ part_rz,
-                     double* __restrict__ part_rr) {
+                     double* __restrict__ part_rr, const int32_t* __restrict__ live) {
+  if (live && *live == 0) return;  // every column converged: a no-op iteration
   typedef typename Scalar<T>::acc A;
   __shared__ A sm[kBlk * V];
   __shared__ double smr[kBlk * V];
@@ -1049,7 +1056,8 @@ __device__ __forceinline__ cdouble sum_part(const A* __restrict__ part, int nb, 
 // after init: rz, rr0; a column is active iff its rhs is nonzero and enabled
 template <typename A>
 __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
-                                const int32_t* __restrict__ enable, const OuterState* __restrict__ os) {
+                                const int32_t* __restrict__ enable, const OuterState* __restrict__ os,
+                                int32_t* __restrict__ live) {
   RB_FIN_WARP();
   const cdouble rz = sum_part<A>(part_rz, nb, k, c, lane);
   const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
@@ -1065,10 +1073,14 @@ __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const doubl
   s.alpha = make_double2(0, 0);
   s.beta = make_double2(0, 0);
   cs[c] = s;
+  if (s.active) atomicAdd(live, 1);
 }
 
+// also clears the live-column slot that this iteration's fin_beta counts
+// into (its previous readers, the kernels of the iteration before, are done)
 template <typename A>
-__global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs) {
+__global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs, int32_t* __restrict__ clear) {
+  if (clear && blockIdx.x == 0 && threadIdx.x == 0) *clear = 0;
   RB_FIN_WARP();
   if (!cs[c].active) return;
   const cdouble pq = sum_part<A>(part_pq, nb, k, c, lane);
@@ -1330,29 +1342,31 @@ static Shape pick_spmm_shape(int64_t n, int64_t k) {
     default: return fail(RB_EARG, "bad shape");      \
   }
 
+// live: the live-column count the iteration kernels read (NULL outside the
+// Krylov loop)
 template <typename T, int EPI>
 int spmm_t(const rb_csr& A, const T* val, const T* X, T* Y, const double* B, void* part, int64_t k,
-           const Shape& sh, cudaStream_t st) {
+           const Shape& sh, cudaStream_t st, const int32_t* live = nullptr) {
   const bool o32 = (uint64_t)A.n * (uint64_t)k < (1ull << 31);
   if (sh.S == 2) {
     if (sh.L != 32 || sh.V != 2 || k != 128) return fail(RB_EARG, "bad sliced SpMM shape");
     if (o32)
-      spmm_kernel<T, 32, 2, EPI, 2, true><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+      spmm_kernel<T, 32, 2, EPI, 2, true><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part, live);
     else
-      spmm_kernel<T, 32, 2, EPI, 2, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part);
+      spmm_kernel<T, 32, 2, EPI, 2, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part, live);
     RB_LAUNCH_CHECK();
     return RB_OK;
   }
   if (sh.L == 32 && !o32) {  // offsets beyond int32: the 64-bit index arithmetic
 #define RB_SPMM(L_, V_) \
-  spmm_kernel<T, L_, V_, EPI, 1, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part)
+  spmm_kernel<T, L_, V_, EPI, 1, false><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part, live)
     RB_DISPATCH_LV(sh, RB_SPMM);
 #undef RB_SPMM
     RB_LAUNCH_CHECK();
     return RB_OK;
   }
 #define RB_SPMM(L_, V_) \
-  spmm_kernel<T, L_, V_, EPI><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part)
+  spmm_kernel<T, L_, V_, EPI><<<sh.grid, kBlk, 0, st>>>(A.n, k, A.indptr, A.indices, val, X, Y, B, part, live)
   RB_DISPATCH_LV(sh, RB_SPMM);
 #undef RB_SPMM
   RB_LAUNCH_CHECK();
@@ -1364,7 +1378,7 @@ static bool grp_cols_ok(int64_t k) { return k == 32 || k == 64 || k == 128; }
 
 template <typename T, int V, int EPI>
 static int spmm_grp_v(const rb_csr& A, const T* val, const GroupPlan& gp, const T* X, T* Y, const double* B,
-                      void* part, int32_t* err, unsigned* grid_out, cudaStream_t st) {
+                      void* part, int32_t* err, unsigned* grid_out, cudaStream_t st, const int32_t* live) {
   static int bps = 0;  // resident blocks per SM of this instantiation
   constexpr size_t smem = grp_smem_bytes<T>();
   if (!bps) {
@@ -1378,7 +1392,7 @@ static int spmm_grp_v(const rb_csr& A, const T* val, const GroupPlan& gp, const 
   const int64_t grid = std::max<int64_t>(
       1, std::min<int64_t>(std::min<int64_t>(num_sms() * bps, ceil_div(gp.ng, kGrpWarps)), kGridMax));
   spmm_grp_kernel<T, V, EPI><<<(unsigned)grid, kGrpWarps * 32, smem, st>>>(A.n, A.indptr, val, gp, X, Y, B, part,
-                                                                            err);
+                                                                            err, live);
   RB_LAUNCH_CHECK();
   *grid_out = (unsigned)grid;
   return RB_OK;
@@ -1386,22 +1400,23 @@ static int spmm_grp_v(const rb_csr& A, const T* val, const GroupPlan& gp, const 
 
 template <typename T, int EPI>
 static int spmm_grp(const rb_csr& A, const T* val, const GroupPlan& gp, const T* X, T* Y, const double* B,
-                    void* part, int64_t k, int32_t* err, unsigned* grid_out, cudaStream_t st) {
+                    void* part, int64_t k, int32_t* err, unsigned* grid_out, cudaStream_t st,
+                    const int32_t* live) {
   switch (k) {
-    case 32: return spmm_grp_v<T, 1, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st);
-    case 64: return spmm_grp_v<T, 2, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st);
-    case 128: return spmm_grp_v<T, 4, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st);
+    case 32: return spmm_grp_v<T, 1, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st, live);
+    case 64: return spmm_grp_v<T, 2, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st, live);
+    case 128: return spmm_grp_v<T, 4, EPI>(A, val, gp, X, Y, B, part, err, grid_out, st, live);
     default: return fail(RB_EARG, "row-group SpMM: %lld columns", (long long)k);
   }
 }
 
 template <int EPI>
 static int spmm_pair(const rb_csr& A, const float* val, const GroupPlan& gp, const float* X, float* Y, void* part,
-                     int64_t k, unsigned* grid_out, cudaStream_t st) {
+                     int64_t k, unsigned* grid_out, cudaStream_t st, const int32_t* live) {
   if (!pair_cols_ok(k) || A.n * k >= (int64_t(1) << 31)) return fail(RB_EARG, "row-pair SpMM: %lld columns", (long long)k);
   const unsigned grid = (unsigned)std::max<int64_t>(
       1, std::min<int64_t>(num_sms() * BpsSpmm<float>::value, ceil_div(gp.ng, kBlk / 32)));
-  spmm_pair_kernel<EPI><<<grid, kBlk, 0, st>>>(A.n, k, A.indptr, val, gp, X, Y, part);
+  spmm_pair_kernel<EPI><<<grid, kBlk, 0, st>>>(A.n, k, A.indptr, val, gp, X, Y, part, live);
   RB_LAUNCH_CHECK();
   *grid_out = grid;
   return RB_OK;
@@ -1449,7 +1464,8 @@ struct SolveBufs {
   ColState* cs;
   OuterState* os;
   int32_t* enable;
-  int32_t* counter;  // [0] active inner columns, [1] active outer columns, [2] SpMM wait timeout
+  int32_t* counter;  // [1] active outer columns, [2] SpMM wait timeout, [4..5] live inner columns
+                     // (two slots, alternating per iteration), [6..7] their values at burst ends
   // row-group plan of the SpMM (k = 32, 64 or 128 columns)
   int32_t *gcnt, *gptr, *ucol;
   uint8_t* umask;
@@ -1469,7 +1485,7 @@ static size_t carve(Carver& cv, SolveBufs<T64, T>& b, int64_t n, int64_t nnz, in
   b.cs = cv.take<ColState>(k);
   b.os = cv.take<OuterState>(k);
   b.enable = cv.take<int32_t>(k);
-  b.counter = cv.take<int32_t>(4);
+  b.counter = cv.take<int32_t>(8);
   const int64_t ng = ceil_div(n, GrpCfg<T>::G);
   b.gcnt = cv.take<int32_t>(ng + 1);
   b.gptr = cv.take<int32_t>(ng + 1);
@@ -1531,6 +1547,40 @@ struct KernelTimer {
   }
 };
 
+// Host side of the burst pipeline: one event per snapshot slot and a side
+// stream (per device, created once) on which the 4-byte snapshot is read
+// back, so that the read waits for its own burst only, not for the burst
+// queued behind it on the solve's stream.
+static cudaStream_t side_stream() {
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+  return streams[dev];
+}
+
+struct BurstSync {
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaStream_t side = nullptr;
+  int init() {
+    side = side_stream();
+    if (!side) return fail(RB_ECUDA, "rb_femsolve: no side stream");
+    for (auto& e : ev) RB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return RB_OK;
+  }
+  // the live count at the end of the burst recorded in slot s
+  int read(int s, const int32_t* snap, int32_t* v) {
+    RB_CUDA_TRY(cudaEventSynchronize(ev[s]));
+    RB_CUDA_TRY(cudaMemcpyAsync(v, snap + s, sizeof(int32_t), cudaMemcpyDeviceToHost, side));
+    RB_CUDA_TRY(cudaStreamSynchronize(side));
+    return RB_OK;
+  }
+  ~BurstSync() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
 template <typename T>
 static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, const Shape& sh, const Shape& shs,
                        void* part_a,
@@ -1555,54 +1605,59 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
     RB_TRY(coarse_apply<T>(*co, R, k, st));
     *launches += 3;
   }
+  // live-column count: iteration i's kernels read slot rd and return at once
+  // when it is 0; its fin_beta counts the columns still active into the
+  // other slot (cleared by its fin_alpha), which the next iteration reads
+  int32_t* slot[2] = {counter + 4, counter + 5};
+  int32_t* snap = counter + 6;
+  int rd = 1;
+  RB_CUDA_TRY(cudaMemsetAsync(slot[rd], 0, sizeof(int32_t), st));
 #define RB_INIT(L_, V_) \
   cg_init_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, dinv, R, P, Xs, (Acc*)part_a, part_b, agg, ec)
   RB_DISPATCH_LV(sh, RB_INIT);
 #undef RB_INIT
   RB_LAUNCH_CHECK();
-  fin_init_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable, os);
+  fin_init_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)sh.grid, (const Acc*)part_a, part_b, cs, enable, os, slot[rd]);
   RB_LAUNCH_CHECK();
   *launches += 2;
-  int it = 0;
   const double tol2 = tol * tol;
-  while (it < maxiter) {
-    const int burst = std::min(check_every, maxiter - it);
-    RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+  auto enqueue_burst = [&](int burst) -> int {
     for (int b = 0; b < burst; ++b) {
+      const int32_t* live = slot[rd];
+      int32_t* next = slot[rd ^ 1];
       RB_TRY(tm.record(st));
       unsigned nb = shs.grid;
       if (gp) {
         if constexpr (PairCfg<T>::enabled) {
-          RB_TRY((spmm_pair<EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st)));
+          RB_TRY((spmm_pair<EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st, live)));
         } else {
-          RB_TRY((spmm_grp<T, EPI_PQDOT>(A, val, *gp, P, Q, nullptr, part_a, k, counter + 2, &nb, st)));
+          RB_TRY((spmm_grp<T, EPI_PQDOT>(A, val, *gp, P, Q, nullptr, part_a, k, counter + 2, &nb, st, live)));
         }
       } else {
-        RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, shs, st)));
+        RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, shs, st, live)));
       }
       RB_TRY(tm.record(st));
-      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)nb, (const Acc*)part_a, cs);
+      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)nb, (const Acc*)part_a, cs, next);
       if (co && AggOrder<T>::value) {
         // aggregate order: the update also restricts the new r to rc
 #define RB_UPD(L_, V_)                                                                                           \
   cg_update_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, Xs, R, P, Q, co->agg_ptr,      \
-                                                         co->agg_rows, co->rc, (Acc*)part_a, part_b)
+                                                         co->agg_rows, co->rc, (Acc*)part_a, part_b, live)
         RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       } else {
-#define RB_UPD(L_, V_) \
-  cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b)
+#define RB_UPD(L_, V_)                                                                                           \
+  cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b, live)
         RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       }
       RB_TRY(tm.record(st));
       if (co) {
-        RB_TRY(coarse_apply<T>(*co, AggOrder<T>::value ? nullptr : R, k, st));
+        RB_TRY(coarse_apply<T>(*co, AggOrder<T>::value ? nullptr : R, k, st, live));
         *launches += AggOrder<T>::value ? 2 : 3;
       }
       RB_TRY(tm.record(st));
-      if (b == burst - 1) RB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2, counter, part_c,
+      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2, next, part_c,
                                                kCdotGrid);
       if (co && AggOrder<T>::value) {
 #define RB_PUP(L_, V_)                                                                                   \
@@ -1617,14 +1672,51 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       }
       RB_LAUNCH_CHECK();
       *launches += 5;
+      rd ^= 1;
     }
+    return RB_OK;
+  };
+  // Bursts of check_every iterations; the host reads a burst's live count
+  // (copied to a snapshot slot at its end) only after it has queued the next
+  // burst, so the GPU always has one burst of work queued while the host
+  // waits: a host thread that is late by less than a burst's duration costs
+  // no GPU time.  The burst queued after the converged one runs as no-ops.
+  // With per-kernel timing on, bursts are read one at a time (the timer's
+  // events are harvested at each read).
+  BurstSync bs;
+  RB_TRY(bs.init());
+  int it = 0, pend = -1, pend_it = 0, next_snap = 0;
+  bool converged = false;
+  while (it < maxiter) {
+    const int burst = std::min(check_every, maxiter - it);
+    RB_TRY(enqueue_burst(burst));
     it += burst;
-    int32_t nact = 0;
-    RB_CUDA_TRY(cudaMemcpyAsync(&nact, counter, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    RB_CUDA_TRY(cudaStreamSynchronize(st));
-    RB_TRY(tm.harvest());
-    if (nact == 0) break;
+    RB_CUDA_TRY(cudaMemcpyAsync(snap + next_snap, slot[rd], sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    RB_CUDA_TRY(cudaEventRecord(bs.ev[next_snap], st));
+    if (tm.on) {
+      int32_t v = 0;
+      RB_TRY(bs.read(next_snap, snap, &v));
+      RB_TRY(tm.harvest());
+      if (v == 0) {
+        converged = true;
+        break;
+      }
+      continue;
+    }
+    if (pend >= 0) {
+      int32_t v = 0;
+      RB_TRY(bs.read(pend, snap, &v));
+      if (v == 0) {
+        converged = true;
+        it = pend_it;
+        break;
+      }
+    }
+    pend = next_snap;
+    pend_it = it;
+    next_snap ^= 1;
   }
+  (void)converged;
   *iters_out = it;
   return RB_OK;
 }
@@ -1741,7 +1833,7 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     if (!cb.A64 || !cb.Rb || !cb.Cb || !cb.Dinv || !cb.op.X || !cb.op.rc || !cb.op.ec || !cb.op.part || !cb.err)
       return fail(RB_EARG, "rb_femsolve: workspace too small for the coarse space");
   }
-  RB_CUDA_TRY(cudaMemsetAsync(b.counter, 0, 4 * sizeof(int32_t), st));
+  RB_CUDA_TRY(cudaMemsetAsync(b.counter, 0, 8 * sizeof(int32_t), st));
   if (o.coarse) {
     RB_TRY((coarse_setup<T64, T>(A, cb, st)));
     info.launches += 3 + 5 * (int)ceil_div(cb.op.nc, kGjB);
