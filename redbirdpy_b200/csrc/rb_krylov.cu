@@ -1076,15 +1076,42 @@ __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const doubl
   if (s.active) atomicAdd(live, 1);
 }
 
+// The per-iteration finalizers take one block of kFinThreads per column: each
+// thread sums the partials b = tid, tid + kFinThreads, ... (two accumulators),
+// then warps and the block's warps are added in fixed order (deterministic),
+// 8 times shorter load chains than one warp per column (the update kernel
+// leaves 1184 partials per column).  The sum is valid in thread 0.
+constexpr int kFinThreads = 256;
+template <typename A>
+__device__ __forceinline__ cdouble block_sum_part(const A* __restrict__ part, int nb, int64_t k, int64_t c) {
+  __shared__ cdouble red[kFinThreads / 32];
+  A s0 = acc_zero<A>(), s1 = acc_zero<A>();
+  int b = threadIdx.x;
+  for (; b + kFinThreads < nb; b += 2 * kFinThreads) {
+    s0 = acc_add(s0, part[(int64_t)b * k + c]);
+    s1 = acc_add(s1, part[(int64_t)(b + kFinThreads) * k + c]);
+  }
+  for (; b < nb; b += kFinThreads) s0 = acc_add(s0, part[(int64_t)b * k + c]);
+  const cdouble w = to_c(wsum(acc_add(s0, s1)));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = w;
+  __syncthreads();
+  cdouble t = make_double2(0.0, 0.0);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < kFinThreads / 32; ++q) t = make_double2(t.x + red[q].x, t.y + red[q].y);
+  __syncthreads();  // red is reused by the next sum
+  return t;
+}
+
 // also clears the live-column slot that this iteration's fin_beta counts
 // into (its previous readers, the kernels of the iteration before, are done)
 template <typename A>
-__global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs, int32_t* __restrict__ clear) {
+__global__ void __launch_bounds__(kFinThreads) fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* cs,
+                                                               int32_t* __restrict__ clear) {
   if (clear && blockIdx.x == 0 && threadIdx.x == 0) *clear = 0;
-  RB_FIN_WARP();
-  if (!cs[c].active) return;
-  const cdouble pq = sum_part<A>(part_pq, nb, k, c, lane);
-  if (lane) return;
+  const int64_t c = blockIdx.x;
+  if (c >= k || !cs[c].active) return;  // uniform over the block
+  const cdouble pq = block_sum_part<A>(part_pq, nb, k, c);
+  if (threadIdx.x) return;
   ColState s = cs[c];
   s.pq = pq;
   if (!finite_c(s.pq) || (s.pq.x == 0.0 && s.pq.y == 0.0)) {
@@ -1101,17 +1128,18 @@ __global__ void fin_alpha_kernel(int64_t k, int nb, const A* part_pq, ColState* 
 // With a coarse space rz_new adds the coarse part (P^T r).(X P^T r), whose
 // per-block partials are part_c (nbc blocks).
 template <typename A>
-__global__ void fin_beta_kernel(int64_t k, int nb, const A* part_rz, const double* part_rr, ColState* cs,
-                                double tol2, int32_t* nactive, const A* part_c, int nbc) {
-  RB_FIN_WARP();
-  if (!cs[c].active) return;
-  cdouble rzn = sum_part<A>(part_rz, nb, k, c, lane);
+__global__ void __launch_bounds__(kFinThreads) fin_beta_kernel(int64_t k, int nb, const A* part_rz,
+                                                              const double* part_rr, ColState* cs, double tol2,
+                                                              int32_t* nactive, const A* part_c, int nbc) {
+  const int64_t c = blockIdx.x;
+  if (c >= k || !cs[c].active) return;  // uniform over the block
+  cdouble rzn = block_sum_part<A>(part_rz, nb, k, c);
   if (part_c) {
-    const cdouble rc = sum_part<A>(part_c, nbc, k, c, lane);
+    const cdouble rc = block_sum_part<A>(part_c, nbc, k, c);
     rzn = make_double2(rzn.x + rc.x, rzn.y + rc.y);
   }
-  const double rr = sum_part<double>(part_rr, nb, k, c, lane).x;
-  if (lane) return;
+  const double rr = block_sum_part<double>(part_rr, nb, k, c).x;
+  if (threadIdx.x) return;
   ColState s = cs[c];
   s.iters += 1;
   s.rr = rr;
@@ -1637,7 +1665,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
         RB_TRY((spmm_t<T, EPI_PQDOT>(A, val, P, Q, nullptr, part_a, k, shs, st, live)));
       }
       RB_TRY(tm.record(st));
-      fin_alpha_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)nb, (const Acc*)part_a, cs, next);
+      fin_alpha_kernel<Acc><<<(unsigned)k, kFinThreads, 0, st>>>(k, (int)nb, (const Acc*)part_a, cs, next);
       if (co && AggOrder<T>::value) {
         // aggregate order: the update also restricts the new r to rc
 #define RB_UPD(L_, V_)                                                                                           \
@@ -1657,8 +1685,8 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
         *launches += AggOrder<T>::value ? 2 : 3;
       }
       RB_TRY(tm.record(st));
-      fin_beta_kernel<Acc><<<fg, 256, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2, next, part_c,
-                                               kCdotGrid);
+      fin_beta_kernel<Acc><<<(unsigned)k, kFinThreads, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2,
+                                                               next, part_c, kCdotGrid);
       if (co && AggOrder<T>::value) {
 #define RB_PUP(L_, V_)                                                                                   \
   cg_pupdate_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, P, co->agg_ptr,   \
