@@ -346,9 +346,22 @@ template <> struct GrpCfg<float> {
   static constexpr int G = 2;             // rows per group of its union plan
   static constexpr int C = 8;
 };
-// FP32 row-pair SpMM: used at 65..128 columns (multiples of 4: L = 32, V = 4)
-template <typename T> struct PairCfg { static constexpr bool enabled = std::is_same<T, float>::value; };
-static bool pair_cols_ok(int64_t k) { return k > 64 && k <= 128 && k % 4 == 0; }
+template <> struct GrpCfg<cfloat> {
+  static constexpr bool enabled = false;  // complex64 takes the row-pair SpMM below
+  static constexpr int G = 2;
+  static constexpr int C = 8;
+};
+// Row-pair SpMM: FP32 at 65..128 columns (multiples of 4: L = 32, V = 4);
+// complex64 at 128 columns in two 64-column slices (V = 2, S = 2)
+template <typename T> struct PairCfg {
+  static constexpr bool enabled = std::is_same<T, float>::value || std::is_same<T, cfloat>::value;
+  static constexpr int V = std::is_same<T, float>::value ? 4 : 2;
+  static constexpr int S = std::is_same<T, float>::value ? 1 : 2;
+};
+template <typename T> static bool pair_cols_ok(int64_t k) {
+  if (std::is_same<T, float>::value) return k > 64 && k <= 128 && k % 4 == 0;
+  return k == 128;
+}
 constexpr int kGrpWarps = 4;     // warps per block
 constexpr int kGrpVals = 256;    // staged matrix values per group (else read from global)
 constexpr int kWaitSpins = 1 << 22;
@@ -619,40 +632,45 @@ constexpr size_t grp_smem_bytes() {
 // Chunks of 32 union entries are staged in shared memory as (x row offset,
 // coefficient of row 0, coefficient of row 1), padded to a multiple of U with
 // the last offset at coefficient 0.  EPI as spmm_kernel (PQDOT only here).
-template <int EPI>
-__global__ void __launch_bounds__(kBlk, BpsSpmm<float>::value)
-spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const float* __restrict__ val, GroupPlan gp,
-                 const float* __restrict__ X, float* __restrict__ Y, void* __restrict__ part_,
+// T = complex64: S = 2 column slices of 64; a task is (pair, slice) and a
+// warp always sees the same slice (task % S = warp % S, groups a multiple of
+// S), as block_colreduce requires.
+template <typename T, int EPI>
+__global__ void __launch_bounds__(kBlk, BpsSpmm<T>::value)
+spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const T* __restrict__ val, GroupPlan gp,
+                 const T* __restrict__ X, T* __restrict__ Y, void* __restrict__ part_,
                  const int32_t* __restrict__ live) {
   if (live && *live == 0) return;  // every column converged: a no-op iteration
-  constexpr int V = 4, U = 8;
-  typedef double A;
+  constexpr int V = PairCfg<T>::V, S = PairCfg<T>::S, U = 8;
+  typedef typename Scalar<T>::acc A;
   static_assert(EPI == EPI_PQDOT, "row-pair SpMM: p.Ap epilogue only");
   __shared__ A sm[kBlk * V];
   __shared__ __align__(16) int32_t s_off[kBlk];
-  __shared__ __align__(16) float s_va[kBlk];
-  __shared__ __align__(16) float s_vb[kBlk];
+  __shared__ __align__(16) T s_va[kBlk];
+  __shared__ __align__(16) T s_vb[kBlk];
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  const int64_t c0 = (int64_t)lane * V;
+  const int64_t task0 = blockIdx.x * (int64_t)(kBlk / 32) + (threadIdx.x >> 5);
+  const int64_t c0 = (task0 % S) * (int64_t)(32 * V) + (int64_t)lane * V;
   const bool on = c0 < k;
   const int64_t groups = (int64_t)gridDim.x * (kBlk / 32);
   int32_t* const wo = s_off + (threadIdx.x & ~31);
-  float* const wa = s_va + (threadIdx.x & ~31);
-  float* const wb = s_vb + (threadIdx.x & ~31);
-  const float* const xl = X + c0;
+  T* const wa = s_va + (threadIdx.x & ~31);
+  T* const wb = s_vb + (threadIdx.x & ~31);
+  const T* const xl = X + c0;
   alignas(16) A acc[V];
 #pragma unroll
-  for (int j = 0; j < V; ++j) acc[j] = 0.0;
-  for (int64_t t = blockIdx.x * (int64_t)(kBlk / 32) + (threadIdx.x >> 5); t < gp.ng; t += groups) {
+  for (int j = 0; j < V; ++j) acc[j] = acc_zero<A>();
+  for (int64_t task = task0; task < gp.ng * S; task += groups) {
+    const int64_t t = task / S;
     const int64_t r0 = 2 * t;
     const bool has1 = r0 + 1 < n;
     const int32_t ub = gp.gptr[t], ue = gp.gptr[t + 1];
     const int32_t ba = indptr[r0], bb = indptr[r0 + 1];  // value ranges of rows r0 and r0 + 1
     int32_t ca = 0, cb = 0;                              // entries of each row consumed so far
-    alignas(16) float ya[V], yb[V];
+    alignas(16) T ya[V], yb[V];
 #pragma unroll
-    for (int j = 0; j < V; ++j) ya[j] = yb[j] = 0.f;
+    for (int j = 0; j < V; ++j) ya[j] = yb[j] = s_zero(T());
     for (int32_t u0 = ub; u0 < ue; u0 += 32) {
       const int cnt = min(32, ue - u0);
       const int cntp = (cnt + U - 1) / U * U;
@@ -660,8 +678,8 @@ spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const
       const int32_t col = in ? gp.ucol[u0 + lane] : 0;
       const uint32_t m = in ? gp.umask[u0 + lane] : 0u;
       const unsigned bma = __ballot_sync(0xffffffffu, m & 1u), bmb = __ballot_sync(0xffffffffu, m & 2u);
-      const float va = (m & 1u) ? val[ba + ca + __popc(bma & lt)] : 0.f;
-      const float vb = (m & 2u) ? val[bb + cb + __popc(bmb & lt)] : 0.f;
+      const T va = (m & 1u) ? val[ba + ca + __popc(bma & lt)] : s_zero(T());
+      const T vb = (m & 2u) ? val[bb + cb + __popc(bmb & lt)] : s_zero(T());
       ca += __popc(bma);
       cb += __popc(bmb);
       const int32_t last = __shfl_sync(0xffffffffu, col, cnt - 1);
@@ -675,38 +693,38 @@ spmm_pair_kernel(int64_t n, int64_t k, const int32_t* __restrict__ indptr, const
         alignas(16) int32_t oo[U];
         ldv_s<int32_t, U>(wo + j, oo);
         if (on) {
-          alignas(16) float xv[U][V];
+          alignas(16) T xv[U][V];
 #pragma unroll
-          for (int u = 0; u < U; ++u) ldv<float, V>(xl + (uint32_t)oo[u], xv[u]);
-          alignas(16) float aa[U], bbv[U];
-          ldv_s<float, U>(wa + j, aa);
-          ldv_s<float, U>(wb + j, bbv);
+          for (int u = 0; u < U; ++u) ldv<T, V>(xl + (uint32_t)oo[u], xv[u]);
+          alignas(16) T aa[U], bbv[U];
+          ldv_s<T, U>(wa + j, aa);
+          ldv_s<T, U>(wb + j, bbv);
 #pragma unroll
           for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int q = 0; q < V; ++q) {
-              ya[q] = fmaf(aa[u], xv[u][q], ya[q]);
-              yb[q] = fmaf(bbv[u], xv[u][q], yb[q]);
+              ya[q] = s_fma(aa[u], xv[u][q], ya[q]);
+              yb[q] = s_fma(bbv[u], xv[u][q], yb[q]);
             }
         }
       }
       __syncwarp();  // the slot is rewritten by the next chunk
     }
     if (on) {
-      alignas(16) float pv[V];
-      ldv<float, V>(X + r0 * k + c0, pv);
+      alignas(16) T pv[V];
+      ldv<T, V>(X + r0 * k + c0, pv);
 #pragma unroll
       for (int j = 0; j < V; ++j) acc[j] = acc_fma(pv[j], ya[j], acc[j]);
-      stv<float, V>(Y + r0 * k + c0, ya);
+      stv<T, V>(Y + r0 * k + c0, ya);
       if (has1) {
-        ldv<float, V>(X + (r0 + 1) * k + c0, pv);
+        ldv<T, V>(X + (r0 + 1) * k + c0, pv);
 #pragma unroll
         for (int j = 0; j < V; ++j) acc[j] = acc_fma(pv[j], yb[j], acc[j]);
-        stv<float, V>(Y + (r0 + 1) * k + c0, yb);
+        stv<T, V>(Y + (r0 + 1) * k + c0, yb);
       }
     }
   }
-  block_colreduce<A, 32, V>(acc, reinterpret_cast<A*>(part_), k, sm);
+  block_colreduce<A, 32, V, S>(acc, reinterpret_cast<A*>(part_), k, sm);
 }
 
 // ------------------------------------------------------- CG vector kernels
@@ -1438,13 +1456,14 @@ static int spmm_grp(const rb_csr& A, const T* val, const GroupPlan& gp, const T*
   }
 }
 
-template <int EPI>
-static int spmm_pair(const rb_csr& A, const float* val, const GroupPlan& gp, const float* X, float* Y, void* part,
+template <typename T, int EPI>
+static int spmm_pair(const rb_csr& A, const T* val, const GroupPlan& gp, const T* X, T* Y, void* part,
                      int64_t k, unsigned* grid_out, cudaStream_t st, const int32_t* live) {
-  if (!pair_cols_ok(k) || A.n * k >= (int64_t(1) << 31)) return fail(RB_EARG, "row-pair SpMM: %lld columns", (long long)k);
+  if (!pair_cols_ok<T>(k) || A.n * k >= (int64_t(1) << 31))
+    return fail(RB_EARG, "row-pair SpMM: %lld columns", (long long)k);
   const unsigned grid = (unsigned)std::max<int64_t>(
-      1, std::min<int64_t>(num_sms() * BpsSpmm<float>::value, ceil_div(gp.ng, kBlk / 32)));
-  spmm_pair_kernel<EPI><<<grid, kBlk, 0, st>>>(A.n, k, A.indptr, val, gp, X, Y, part, live);
+      1, std::min<int64_t>(num_sms() * BpsSpmm<T>::value, ceil_div(gp.ng * PairCfg<T>::S, kBlk / 32)));
+  spmm_pair_kernel<T, EPI><<<grid, kBlk, 0, st>>>(A.n, k, A.indptr, val, gp, X, Y, part, live);
   RB_LAUNCH_CHECK();
   *grid_out = grid;
   return RB_OK;
@@ -1657,7 +1676,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       unsigned nb = shs.grid;
       if (gp) {
         if constexpr (PairCfg<T>::enabled) {
-          RB_TRY((spmm_pair<EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st, live)));
+          RB_TRY((spmm_pair<T, EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st, live)));
         } else {
           RB_TRY((spmm_grp<T, EPI_PQDOT>(A, val, *gp, P, Q, nullptr, part_a, k, counter + 2, &nb, st, live)));
         }
@@ -1868,7 +1887,7 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
   }
   GroupPlan gp{nullptr, nullptr, nullptr, 0};
   const bool plan = (GrpCfg<T>::enabled && grp_cols_ok(kb)) ||
-                    (PairCfg<T>::enabled && pair_cols_ok(kb) && n * kb < (int64_t(1) << 31));
+                    (PairCfg<T>::enabled && pair_cols_ok<T>(kb) && n * kb < (int64_t(1) << 31));
   if (plan && n > 0)
     RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask, b.scan_work, b.scan_bytes, &gp, st));
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * kb, 256), 148 * 16);
