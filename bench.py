@@ -220,9 +220,9 @@ def run_b200(args):
     # the product's own bytes: the CSR matrix (FP32 values, int32 indices) and
     # x and y once each, whatever plan the kernel walks
     spmm_bytes = nnz * (4 + 4) + 4 * (n + 1) + 2 * k * n * 4
-    # x, r, p, q read + x, r written (FP32), dinv and the aggregate row list
-    # read, the restricted residual (nc x k) written
-    upd_bytes = 6 * k * n * 4 + 8 * n + 4 * k * infos[-1]["coarse_nc"]
+    # r, q read + r written (FP32), dinv and the aggregate row list read, the
+    # restricted residual (nc x k) written (x += a p is in the p-update)
+    upd_bytes = 3 * k * n * 4 + 8 * n + 4 * k * infos[-1]["coarse_nc"]
     sp_ms = sum(i["spmm_ms"] for i in pinfos) / max(1, sum(i["spmm_launches"] for i in pinfos))
     up_ms = sum(i["update_ms"] for i in pinfos) / max(1, sum(i["update_launches"] for i in pinfos))
     peak, peak_kind = peaks()
@@ -293,7 +293,7 @@ def run_b200(args):
                      "algorithmic_bytes": spmm_bytes, "launch_ms": round(sp_ms, 4),
                      "traffic": traffic.get("spmm_pair_kernel<EPI_PQDOT>"),
                      "traffic_source": "ncu capture, profiles/forward_3Mtet_128rhs_launches_and_kernels.md"},
-        "roofline_update": {"kernel": "cg_update_agg_kernel<float> (x, r update + r.z, r.r, coarse restriction)",
+        "roofline_update": {"kernel": "cg_update_agg_kernel<float> (r update + r.z, r.r, coarse restriction)",
                             "achieved": round(up_gbs, 1) if up_gbs else None,
                             "unit": "GB/s", "frac": round(up_gbs / peak, 4) if up_gbs else None,
                             "algorithmic_bytes": upd_bytes, "launch_ms": round(up_ms, 4),

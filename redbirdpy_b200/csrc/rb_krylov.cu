@@ -751,7 +751,7 @@ struct ColState {
   int32_t active;  // column still iterating
   int32_t status;  // 0 running/converged, 2 breakdown
   int32_t iters;
-  int32_t pad;
+  int32_t upd;     // x += alpha p in this iteration's p-update (alpha set by fin_alpha)
 };
 
 template <typename T> __device__ __forceinline__ T from_c(cdouble v);
@@ -811,13 +811,13 @@ cg_init_kernel(int64_t n, int64_t k, const T* __restrict__ dinv, const T* __rest
   block_colreduce<double, L, V>(arr, part_rr, k, smr);
 }
 
-// x += a p; r -= a q; z = Dinv r; acc rz += r.z, rr += |r|^2
+// r -= a q; z = Dinv r; acc rz += r.z, rr += |r|^2.  (x += a p waits for
+// the p-update, which reads p anyway: 3 vector passes here instead of 6.)
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
-                 T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
-                 typename Scalar<T>::acc* __restrict__ part_rz, double* __restrict__ part_rr,
-                 const int32_t* __restrict__ live) {
+                 T* __restrict__ R, const T* __restrict__ Q, typename Scalar<T>::acc* __restrict__ part_rz,
+                 double* __restrict__ part_rr, const int32_t* __restrict__ live) {
   if (live && *live == 0) return;  // every column converged: a no-op iteration
   typedef typename Scalar<T>::acc A;
   __shared__ A sm[kBlk * V];
@@ -840,62 +840,86 @@ cg_update_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T*
   for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     if (!on) continue;
     const T d = dinv[row];
-    alignas(16) T x[V], r[V], p[V], q[V];
-    ldv<T, V>(Xs + row * k + c0, x);
+    alignas(16) T r[V], q[V];
     ldv<T, V>(R + row * k + c0, r);
-    ldv<T, V>(P + row * k + c0, p);
     ldv<T, V>(Q + row * k + c0, q);
 #pragma unroll
     for (int j = 0; j < V; ++j) {
-      if (act[j]) {  // frozen columns keep x and r untouched (p may hold NaN after a breakdown)
-        x[j] = s_fma(al[j], p[j], x[j]);
-        r[j] = s_sub(r[j], s_mul(al[j], q[j]));
-      }
+      if (act[j]) r[j] = s_sub(r[j], s_mul(al[j], q[j]));  // frozen columns keep r untouched
       const T z = s_mul(d, r[j]);
       arz[j] = acc_fma(r[j], z, arz[j]);
       arr[j] += s_abs2(r[j]);
     }
-    stv<T, V>(Xs + row * k + c0, x);
     stv<T, V>(R + row * k + c0, r);
   }
   block_colreduce<A, L, V>(arz, part_rz, k, sm);
   block_colreduce<double, L, V>(arr, part_rr, k, smr);
 }
 
-// p = z + beta p, z = Dinv r (+ ec[agg[row]] with a coarse space)  (active columns only)
+// x += alpha p (columns whose alpha this iteration set: cs.upd), then
+// p = z + beta p, z = Dinv r (+ ec[agg[row]] with a coarse space) (columns
+// still active)
+template <typename T, int V>
+struct PupCols {
+  alignas(16) T al[V], be[V];
+  bool act[V], upd[V];
+  bool any_act = false, any_upd = false;
+  __device__ __forceinline__ void load(const ColState* __restrict__ cs, int64_t c0) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      act[j] = cs[c0 + j].active;
+      upd[j] = cs[c0 + j].upd;
+      al[j] = upd[j] ? from_c<T>(cs[c0 + j].alpha) : s_zero(T());
+      be[j] = from_c<T>(cs[c0 + j].beta);
+      any_act |= act[j];
+      any_upd |= upd[j];
+    }
+  }
+  __device__ __forceinline__ void row(T* __restrict__ Xrow, T* __restrict__ Prow, const T* __restrict__ Rrow, T d,
+                                      const T (&e)[V]) const {
+    alignas(16) T p[V];
+    ldv<T, V>(Prow, p);
+    if (any_upd) {
+      alignas(16) T x[V];
+      ldv<T, V>(Xrow, x);
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if (upd[j]) x[j] = s_fma(al[j], p[j], x[j]);
+      stv<T, V>(Xrow, x);
+    }
+    if (any_act) {
+      alignas(16) T r[V];
+      ldv<T, V>(Rrow, r);
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if (act[j]) p[j] = s_fma(be[j], p[j], s_fma(d, r[j], e[j]));
+      stv<T, V>(Prow, p);
+    }
+  }
+};
+
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
-                  const T* __restrict__ R, T* __restrict__ P, const int32_t* __restrict__ agg,
+                  const T* __restrict__ R, T* __restrict__ P, T* __restrict__ Xs, const int32_t* __restrict__ agg,
                   const T* __restrict__ ec) {
   const int lane = threadIdx.x % L;
   const int64_t c0 = (int64_t)lane * V;
   if (c0 >= k) return;
   const int64_t groups = (int64_t)gridDim.x * (kBlk / L);
-  alignas(16) T be[V];
-  bool act[V], any = false;
-#pragma unroll
-  for (int j = 0; j < V; ++j) {
-    act[j] = cs[c0 + j].active;
-    be[j] = from_c<T>(cs[c0 + j].beta);
-    any |= act[j];
-  }
-  if (!any) return;
+  PupCols<T, V> pc;
+  pc.load(cs, c0);
+  if (!pc.any_act && !pc.any_upd) return;
   for (int64_t row = blockIdx.x * (int64_t)(kBlk / L) + threadIdx.x / L; row < n; row += groups) {
     const T d = dinv[row];
-    alignas(16) T r[V], p[V], e[V];
-    ldv<T, V>(R + row * k + c0, r);
-    ldv<T, V>(P + row * k + c0, p);
+    alignas(16) T e[V];
     if (agg) {
       ldv<T, V>(ec + (int64_t)agg[row] * k + c0, e);
     } else {
 #pragma unroll
       for (int j = 0; j < V; ++j) e[j] = s_zero(T());
     }
-#pragma unroll
-    for (int j = 0; j < V; ++j)
-      if (act[j]) p[j] = s_fma(be[j], p[j], s_fma(d, r[j], e[j]));
-    stv<T, V>(P + row * k + c0, p);
+    pc.row(Xs + row * k + c0, P + row * k + c0, R + row * k + c0, d, e);
   }
 }
 
@@ -936,7 +960,7 @@ __device__ __forceinline__ void block_colsum_row(const A (&acc)[V], T* __restric
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
-                     T* __restrict__ Xs, T* __restrict__ R, const T* __restrict__ P, const T* __restrict__ Q,
+                     T* __restrict__ R, const T* __restrict__ Q,
                      const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
                      T* __restrict__ rc, typename Scalar<T>::acc* __restrict__ part_rz,
                      double* __restrict__ part_rr, const int32_t* __restrict__ live) {
@@ -971,23 +995,17 @@ cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, con
       if (q + G < q1) nrow = agg_rows[q + G];  // next row's index in flight
       if (!on) continue;
       const T d = dinv[row];
-      alignas(16) T x[V], r[V], p[V], qv[V];
-      ldv<T, V>(Xs + row * k + c0, x);
+      alignas(16) T r[V], qv[V];
       ldv<T, V>(R + row * k + c0, r);
-      ldv<T, V>(P + row * k + c0, p);
       ldv<T, V>(Q + row * k + c0, qv);
 #pragma unroll
       for (int j = 0; j < V; ++j) {
-        if (act[j]) {
-          x[j] = s_fma(al[j], p[j], x[j]);
-          r[j] = s_sub(r[j], s_mul(al[j], qv[j]));
-        }
+        if (act[j]) r[j] = s_sub(r[j], s_mul(al[j], qv[j]));
         const T z = s_mul(d, r[j]);
         arz[j] = acc_fma(r[j], z, arz[j]);
         arr[j] += s_abs2(r[j]);
         rs[j] = s_add(rs[j], r[j]);
       }
-      stv<T, V>(Xs + row * k + c0, x);
       stv<T, V>(R + row * k + c0, r);
     }
     {
@@ -1004,21 +1022,16 @@ cg_update_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, con
 template <typename T, int L, int V>
 __global__ void __launch_bounds__(kBlk, Bps<T>::value)
 cg_pupdate_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, const T* __restrict__ dinv,
-                      const T* __restrict__ R, T* __restrict__ P, const int32_t* __restrict__ agg_ptr,
-                      const int32_t* __restrict__ agg_rows, const T* __restrict__ ec) {
+                      const T* __restrict__ R, T* __restrict__ P, T* __restrict__ Xs,
+                      const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
+                      const T* __restrict__ ec) {
   constexpr int G = kBlk / L;
   const int lane = threadIdx.x % L, grp = threadIdx.x / L;
   const int64_t c0 = (int64_t)lane * V;
   if (c0 >= k) return;
-  alignas(16) T be[V];
-  bool act[V], any = false;
-#pragma unroll
-  for (int j = 0; j < V; ++j) {
-    act[j] = cs[c0 + j].active;
-    be[j] = from_c<T>(cs[c0 + j].beta);
-    any |= act[j];
-  }
-  if (!any) return;
+  PupCols<T, V> pc;
+  pc.load(cs, c0);
+  if (!pc.any_act && !pc.any_upd) return;
   for (int64_t I = blockIdx.x; I < nc; I += gridDim.x) {
     alignas(16) T e[V];
     ldv<T, V>(ec + I * k + c0, e);
@@ -1028,14 +1041,7 @@ cg_pupdate_agg_kernel(int64_t nc, int64_t k, const ColState* __restrict__ cs, co
     for (; q < q1; q += G) {
       const int64_t row = nrow;
       if (q + G < q1) nrow = agg_rows[q + G];
-      const T d = dinv[row];
-      alignas(16) T r[V], p[V];
-      ldv<T, V>(R + row * k + c0, r);
-      ldv<T, V>(P + row * k + c0, p);
-#pragma unroll
-      for (int j = 0; j < V; ++j)
-        if (act[j]) p[j] = s_fma(be[j], p[j], s_fma(d, r[j], e[j]));
-      stv<T, V>(P + row * k + c0, p);
+      pc.row(Xs + row * k + c0, P + row * k + c0, R + row * k + c0, dinv[row], e);
     }
   }
 }
@@ -1090,6 +1096,7 @@ __global__ void fin_init_kernel(int64_t k, int nb, const A* part_rz, const doubl
   s.tol2 = os ? os[c].itol2 : -1.0;
   s.alpha = make_double2(0, 0);
   s.beta = make_double2(0, 0);
+  s.upd = 0;
   cs[c] = s;
   if (s.active) atomicAdd(live, 1);
 }
@@ -1127,7 +1134,11 @@ __global__ void __launch_bounds__(kFinThreads) fin_alpha_kernel(int64_t k, int n
                                                                int32_t* __restrict__ clear) {
   if (clear && blockIdx.x == 0 && threadIdx.x == 0) *clear = 0;
   const int64_t c = blockIdx.x;
-  if (c >= k || !cs[c].active) return;  // uniform over the block
+  if (c >= k) return;
+  if (!cs[c].active) {  // uniform over the block; no x update in this iteration's p-update
+    if (threadIdx.x == 0) cs[c].upd = 0;
+    return;
+  }
   const cdouble pq = block_sum_part<A>(part_pq, nb, k, c);
   if (threadIdx.x) return;
   ColState s = cs[c];
@@ -1136,8 +1147,10 @@ __global__ void __launch_bounds__(kFinThreads) fin_alpha_kernel(int64_t k, int n
     s.active = 0;
     s.status = 2;
     s.alpha = make_double2(0, 0);
+    s.upd = 0;
   } else {
     s.alpha = cdiv(s.rz, s.pq);
+    s.upd = 1;
   }
   cs[c] = s;
 }
@@ -1688,13 +1701,13 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       if (co && AggOrder<T>::value) {
         // aggregate order: the update also restricts the new r to rc
 #define RB_UPD(L_, V_)                                                                                           \
-  cg_update_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, Xs, R, P, Q, co->agg_ptr,      \
-                                                         co->agg_rows, co->rc, (Acc*)part_a, part_b, live)
+  cg_update_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, Q, co->agg_ptr, co->agg_rows, \
+                                                         co->rc, (Acc*)part_a, part_b, live)
         RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       } else {
 #define RB_UPD(L_, V_)                                                                                           \
-  cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, Xs, R, P, Q, (Acc*)part_a, part_b, live)
+  cg_update_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, Q, (Acc*)part_a, part_b, live)
         RB_DISPATCH_LV(sh, RB_UPD);
 #undef RB_UPD
       }
@@ -1708,12 +1721,12 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
                                                                next, part_c, kCdotGrid);
       if (co && AggOrder<T>::value) {
 #define RB_PUP(L_, V_)                                                                                   \
-  cg_pupdate_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, P, co->agg_ptr,   \
+  cg_pupdate_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, P, Xs, co->agg_ptr, \
                                                           co->agg_rows, ec)
         RB_DISPATCH_LV(sh, RB_PUP);
 #undef RB_PUP
       } else {
-#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P, agg, ec)
+#define RB_PUP(L_, V_) cg_pupdate_kernel<T, L_, V_><<<sh.grid, kBlk, 0, st>>>(n, k, cs, dinv, R, P, Xs, agg, ec)
         RB_DISPATCH_LV(sh, RB_PUP);
 #undef RB_PUP
       }
