@@ -937,6 +937,11 @@ cg_pupdate_kernel(int64_t n, int64_t k, const ColState* __restrict__ cs, const T
 // sums its rows of the aggregate in the vector type (about 30 rows), the
 // groups are added in FP64 and the result rounded to the vector type.
 template <typename T> struct AggOrder { static constexpr bool value = true; };
+// The p-update needs no restriction; it takes the aggregate order only where
+// that measured faster: complex64 (214.5 against 217.9 ms for the FD solve);
+// FP32 streams better in row order, reading ec[agg[row]] from L2 (CW solve
+// 94.2 against 96.6 ms).
+template <typename T> struct PupAggOrder { static constexpr bool value = Scalar<T>::is_complex; };
 template <typename A, int L, int V, typename T>
 __device__ __forceinline__ void block_colsum_row(const A (&acc)[V], T* __restrict__ out, int64_t k, A* sm) {
   const int lane = threadIdx.x % L, grp = threadIdx.x / L;
@@ -1719,7 +1724,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       RB_TRY(tm.record(st));
       fin_beta_kernel<Acc><<<(unsigned)k, kFinThreads, 0, st>>>(k, (int)ugrid, (const Acc*)part_a, part_b, cs, tol2,
                                                                next, part_c, kCdotGrid);
-      if (co && AggOrder<T>::value) {
+      if (co && PupAggOrder<T>::value) {
 #define RB_PUP(L_, V_)                                                                                   \
   cg_pupdate_agg_kernel<T, L_, V_><<<agrid, kBlk, 0, st>>>(co->nc, k, cs, dinv, R, P, Xs, co->agg_ptr, \
                                                           co->agg_rows, ec)
