@@ -46,6 +46,8 @@ __device__ __forceinline__ double scale_r(double b, double v) { return b * v; }
 __device__ __forceinline__ cfloat scale_r(float b, cfloat v) { return make_float2(b * v.x, b * v.y); }
 __device__ __forceinline__ cdouble scale_r(double b, cdouble v) { return make_double2(b * v.x, b * v.y); }
 
+__device__ __forceinline__ int tid_warp() { return (int)(threadIdx.x >> 5); }
+
 struct JacArgs {
   const int32_t* indptr;
   const int32_t* indices;
@@ -79,10 +81,11 @@ template <typename C> __host__ __device__ inline int jac_c_stride(int rmax, int 
 
 // smem layout, TN nodes, each region starting on a 16-byte boundary:
 //   phi [TN][phi stride] C | Bm [TN][rmax][rmax] R | Cm [TN][C stride] C |
-//   W [TN][emax][16] R | EN [TN][emax] int4 | nb [TN][rmax] int | rn, ek [TN] int
+//   W [TN][emax][16] R | EN [TN][emax] int4 | nb [TN][rmax] int | rn, ek [TN] int |
+//   LP [TN][emax][4] int16 (position of each tet node in the node's row)
 __host__ __device__ inline size_t al16(size_t b) { return (b + 15) / 16 * 16; }
 struct JacSmem {
-  size_t phi, B, C, W, EN, nb, total;
+  size_t phi, B, C, W, EN, nb, lp, total;
 };
 template <typename C>
 __host__ __device__ inline JacSmem jac_layout(int TN, int rmax, int nc, int ndet, int emax) {
@@ -94,7 +97,8 @@ __host__ __device__ inline JacSmem jac_layout(int TN, int rmax, int nc, int ndet
   L.W = L.C + al16((size_t)TN * jac_c_stride<C>(rmax, ndet) * sizeof(C));
   L.EN = L.W + al16((size_t)TN * emax * 16 * sizeof(R));
   L.nb = L.EN + al16((size_t)TN * emax * sizeof(int4));
-  L.total = L.nb + al16((size_t)TN * rmax * sizeof(int) + TN * sizeof(int) * 2);
+  L.lp = L.nb + al16((size_t)TN * rmax * sizeof(int) + TN * sizeof(int) * 2);
+  L.total = L.lp + al16((size_t)TN * emax * 4 * sizeof(int16_t));
   return L;
 }
 template <typename C>
@@ -140,6 +144,9 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   int* snb = reinterpret_cast<int*>(smem + L.nb);
   int* srn = snb + TN * rmax;
   int* sek = srn + TN;
+  int16_t* slp = reinterpret_cast<int16_t*>(smem + L.lp);
+  const int warp = tid_warp(), lane = threadIdx.x & 31;
+  constexpr int kWarps = kJacThreads / 32;
 
   const int64_t n0 = (int64_t)blockIdx.x * TN;
   const int tid = threadIdx.x;
@@ -183,48 +190,66 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
       }
   }
   __syncthreads();
-  // staged phi rows of the neighbours, converted to the compute type
-  for (int64_t i = tid; i < (int64_t)TN * rmax * nc; i += kJacThreads) {
-    const int slot = (int)(i / nc), c = (int)(i % nc);
+  // staged phi rows of the neighbours, converted to the compute type: a warp
+  // per (node, neighbour) slot, lanes over the columns
+  for (int slot = warp; slot < TN * rmax; slot += kWarps) {
+    const int t = slot / rmax, q = slot - t * rmax;
     const int nb = snb[slot];
-    C v;
-    if (nb >= 0) v = cvt<C, In>(phi[(int64_t)nb * a.ld + a.cols[c]]);
-    else v = s_zero(C());
-    sphi[(size_t)(slot / rmax) * SP + (size_t)(slot % rmax) * nc + c] = v;
+    C* dst = sphi + (size_t)t * SP + (size_t)q * nc;
+    for (int c = lane; c < nc; c += 32) dst[c] = nb >= 0 ? cvt<C, In>(phi[(int64_t)nb * a.ld + a.cols[c]]) : s_zero(C());
   }
-  // 2. B_n[a][b] = sum over the node's tets of w_e at the local positions
-  for (int i = tid; i < TN * rmax * rmax; i += kJacThreads) {
-    const int t = i / (rmax * rmax), ab = i % (rmax * rmax);
-    const int ia = ab / rmax, ib = ab % rmax;
-    R s = 0;
-    if (ia < srn[t] && ib < srn[t]) {
-      const int na = snb[t * rmax + ia], nbb = snb[t * rmax + ib];
-      for (int q = 0; q < sek[t]; ++q) {
-        const int4 en = sEN[t * emax + q];
-        const int32_t nd4[4] = {en.x, en.y, en.z, en.w};
-        int pa = -1, pb = -1;
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          if (nd4[m] == na) pa = m;
-          if (nd4[m] == nbb) pb = m;
-        }
-        if (pa >= 0 && pb >= 0) s += sW[((size_t)t * emax + q) * 16 + pa * 4 + pb];
-      }
+  // position of each tet node in its node's row (every tet node is a neighbour)
+  for (int i = tid; i < TN * emax * 4; i += kJacThreads) {
+    const int tq = i >> 2, m = i & 3;
+    const int t = tq / emax, q = tq - t * emax;
+    int pos = -1;
+    if (q < sek[t]) {
+      const int4 en = sEN[tq];
+      const int node = m == 0 ? en.x : m == 1 ? en.y : m == 2 ? en.z : en.w;
+      for (int b = 0; b < srn[t]; ++b)
+        if (snb[t * rmax + b] == node) pos = b;
     }
-    sB[i] = s;
+    slp[i] = (int16_t)pos;
   }
   __syncthreads();
-  // 3. C_n[a][d] = sum_b B_n[a][b] phi[b][det d]
-  for (int i = tid; i < TN * rmax * nd; i += kJacThreads) {
-    const int t = i / (rmax * nd), r = i % (rmax * nd);
-    const int ia = r / nd, d = r % nd;
-    C s = s_zero(C());
+  // 2. B_n[a][b] = sum over the node's tets (ascending) of w_e at the local
+  // positions: a thread per row a walks the tets holding it and adds its 4
+  // coefficients into the row (per entry the same order as summing over the
+  // tets for each (a, b) separately)
+  for (int row = tid; row < TN * rmax; row += kJacThreads) {
+    const int t = row / rmax, ia = row - t * rmax;
+    R* Brow = sB + (size_t)row * rmax;
+    for (int ib = 0; ib < rmax; ++ib) Brow[ib] = 0;
     if (ia < srn[t]) {
-      const R* Brow = sB + ((size_t)t * rmax + ia) * rmax;
-      const C* P = sphi + (size_t)t * SP + a.det0 + d;
-      for (int b = 0; b < srn[t]; ++b) s = s_add(s, scale_r(Brow[b], P[(size_t)b * nc]));
+      for (int q = 0; q < sek[t]; ++q) {
+        const int16_t* lp = slp + ((size_t)t * emax + q) * 4;
+        int pa = -1;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+          if (lp[m] == ia) pa = m;
+        if (pa < 0) continue;
+        const R* W = sW + ((size_t)t * emax + q) * 16 + pa * 4;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+          if (lp[m] >= 0) Brow[lp[m]] += W[m];  // (a tet node outside the row would be a broken pattern)
+      }
     }
-    sC[(size_t)t * SC + r] = s;
+  }
+  __syncthreads();
+  // 3. C_n[a][d] = sum_b B_n[a][b] phi[b][det d]: a warp per (node, row a),
+  // lanes over the detectors
+  for (int slot = warp; slot < TN * rmax; slot += kWarps) {
+    const int t = slot / rmax, ia = slot - t * rmax;
+    const int nr = srn[t];
+    const R* Brow = sB + (size_t)slot * rmax;
+    const C* P = sphi + (size_t)t * SP + a.det0;
+    C* Cout = sC + (size_t)t * SC + (size_t)ia * nd;
+    for (int d = lane; d < nd; d += 32) {
+      C s = s_zero(C());
+      if (ia < nr)
+        for (int b = 0; b < nr; ++b) s = s_add(s, scale_r(Brow[b], P[(size_t)b * nc + d]));
+      Cout[d] = s;
+    }
   }
   __syncthreads();
   // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]
