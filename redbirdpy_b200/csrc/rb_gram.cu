@@ -43,6 +43,7 @@ constexpr uint32_t kGTmemCols = 512;  // two 128 x 256 FP32 accumulators (rows 0
 // split form (tf32x3) drains every 4096 K; the plain TF32 form every 16384 K
 // (~1e-4, below what its rounded inputs allow), so that its MMAs wait on
 // four times fewer drains.
+constexpr int kGItems = 4;  // item indices the producer may claim ahead of the epilogue
 constexpr int kGChunk = 128;
 constexpr int kGChunkTf32 = 512;
 constexpr int kGChunkBf16 = 256;  // the same 16384 K with 64 BF16 elements per K-block
@@ -54,6 +55,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
@@ -133,31 +138,61 @@ __device__ __host__ __forceinline__ int64_t gram_col_tiles(int64_t bj, int64_t n
   return need < nbi ? need : nbi;
 }
 
+// tile t of the upper triangle -> its row offsets (i0 in H's rows, j0 in its
+// columns): tiles are numbered down each tile column, column after column
+__device__ __forceinline__ void gram_tile(int64_t t, int64_t nbi, int64_t nbj, int& i0, int& j0) {
+  int64_t bj = 0;
+  while (bj < nbj - 1 && t >= gram_col_tiles(bj, nbi)) t -= gram_col_tiles(bj++, nbi);
+  i0 = (int)(t * kGM);
+  j0 = (int)(bj * kGN);
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool aborted(const int* err) { return *(volatile const int*)err != 0; }
+
+// Persistent form: one CTA per SM claims work items (tile t, K segment s of
+// kspan) from a global counter in segment-major order, item = s * tiles + t,
+// and hands each index to its MMA lane and epilogue warps through a small
+// shared-memory ring.  Claiming instead of a fixed deal lets an SM that runs
+// slower take fewer items (a fixed round-robin deal measured 270 ms against
+// 223 ms at 8192 x 1,040,502), and short items leave a short last round
+// (2112 items per launch instead of 528 tiles in 4 waves, the last one 57%
+// full: 238 ms).  The FP64 partial sums of tile t for segment s are added to
+// H only after those of segment s - 1: each epilogue warp publishes its rows
+// with a fenced increment of done[t] and waits for done[t] >= 4 s before its
+// first add.  Item i depends only on item i - tiles, claimed earlier, and all
+// CTAs are resident (cooperative launch, one CTA per SM), so the waits always
+// end; they are bounded all the same.  With nseg == 1 (one item per tile,
+// used when the tile count outgrows the progress counters) nothing waits.
+//
 // BF16: J stored as BF16 (64 elements per 128-byte stage row), one pass
 template <bool BF16>
 __global__ void __launch_bounds__(kGThreads, 1)
 gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_lo, int segs,
-                 int64_t M, int64_t kbeg, int64_t kend, int accumulate, double* __restrict__ H, int64_t ldh,
-                 double alpha, int* __restrict__ err) {
-  // K range [kbeg, kend) of this launch; accumulate: add to H instead of
-  // writing its first partial sums
-  const int64_t K = kend - kbeg;
+                 int64_t M, int64_t kbeg, int64_t K, int64_t kspan, int64_t tiles, int accumulate,
+                 double* __restrict__ H, int64_t ldh, double alpha, int* __restrict__ done,
+                 unsigned long long* __restrict__ next, int* __restrict__ err) {
+  // K range [kbeg, kbeg + K) of this launch in segments of kspan; accumulate:
+  // add segment 0 to H instead of writing it
   extern __shared__ __align__(1024) unsigned char gsm_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kGStages * kGStageBytes);
   uint64_t* empty = full + kGStages;
   uint64_t* tfull = empty + kGStages;  // accumulators ready for the epilogue
   uint64_t* tempty = tfull + 1;        // accumulators drained by the epilogue
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+  uint64_t* mdone = tempty + 1;        // every MMA of this CTA complete (exit)
+  uint64_t* ifull = mdone + 1;         // item ring: index written by the producer
+  uint64_t* iempty = ifull + kGItems;  // item ring: read by the MMA lane and the 4 epilogue warps
+  int64_t* sitem = reinterpret_cast<int64_t*>(iempty + kGItems);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sitem + kGItems);
 
-  // tile (bi, bj): walk the tile columns until this block's index falls inside
   const int64_t nbi = (M + kGM - 1) / kGM, nbj = (M + kGN - 1) / kGN;
-  int64_t t = blockIdx.x, bj = 0;
-  while (bj < nbj && t >= gram_col_tiles(bj, nbi)) t -= gram_col_tiles(bj++, nbi);
-  if (bj >= nbj) return;
-  const int64_t bi = t;
-  const int i0 = (int)(bi * kGM), j0 = (int)(bj * kGN);
-
+  const int64_t nseg = (K + kspan - 1) / kspan;
+  const int64_t items = tiles * nseg;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kGStages; ++s) {
@@ -166,6 +201,11 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     }
     mbar_init(smem_u32(tfull), 1);
     mbar_init(smem_u32(tempty), 4 * 32);
+    mbar_init(smem_u32(mdone), 1);
+    for (int s = 0; s < kGItems; ++s) {
+      mbar_init(smem_u32(&ifull[s]), 1);
+      mbar_init(smem_u32(&iempty[s]), 1 + 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -179,56 +219,104 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   // segs == 1: H = J J^T.  segs == 3 (split precision, J = hi + lo):
   // H = hi hi^T + hi lo^T + lo hi^T, one K sweep per product, one accumulator
   constexpr int kE = BF16 ? 2 * kGK : kGK;  // elements per 128-byte stage row
-  const int nk1 = (int)((K + kE - 1) / kE);
-  const int nk = nk1 * segs;
   const int chunk = BF16 ? kGChunkBf16 : (segs == 1) ? kGChunkTf32 : kGChunk;  // K-blocks between drains
+  // K-blocks of one pass over segment s
+  auto seg_blocks = [&](int64_t s) -> int {
+    const int64_t k0 = s * kspan, k1 = (k0 + kspan < K) ? k0 + kspan : K;
+    return (int)((k1 - k0 + kE - 1) / kE);
+  };
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % kGStages;
-        if (kb >= kGStages && !mbar_wait(smem_u32(&empty[s]), ((kb / kGStages) - 1) & 1, err, 1)) break;
-        const uint32_t a = smem_u32(sm + s * kGStageBytes);
-        const uint32_t b = a + kGABytes;
-        const uint32_t bar = smem_u32(&full[s]);
-        const int seg = kb / nk1, kx = (int)kbeg + (kb - seg * nk1) * kE;
-        const CUtensorMap* ma = (seg == 2) ? &tmap_lo : &tmap;
-        const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
-        mbar_expect_tx(bar, kGStageBytes);
-        tma_load_2d(a, ma, bar, kx, i0);
-        tma_load_2d(a + kGBoxBytes, ma, bar, kx, i0 + kGMH);
-        tma_load_2d(b, mb, bar, kx, j0);
-        tma_load_2d(b + kGBoxBytes, mb, bar, kx, j0 + kGMH);
+      uint32_t g = 0;  // stages issued by this CTA
+      bool ok = true;
+      for (uint32_t n = 0; ok; ++n) {
+        // claim the next item and hand its index to the other roles
+        const int slot = (int)(n % kGItems);
+        if (n >= (uint32_t)kGItems && !mbar_wait(smem_u32(&iempty[slot]), ((n / kGItems) - 1) & 1, err, 8)) break;
+        const int64_t item = aborted(err) ? items : (int64_t)atomicAdd(next, 1ull);
+        sitem[slot] = item < items ? item : items;
+        mbar_arrive(smem_u32(&ifull[slot]));
+        if (item >= items) break;
+        const int64_t s = item / tiles;
+        int i0, j0;
+        gram_tile(item - s * tiles, nbi, nbj, i0, j0);
+        const int nk1 = seg_blocks(s), nk = nk1 * segs;
+        for (int kb = 0; kb < nk; ++kb) {
+          const int st = (int)(g % kGStages);
+          if (g >= (uint32_t)kGStages && !mbar_wait(smem_u32(&empty[st]), ((g / kGStages) - 1) & 1, err, 1)) {
+            ok = false;
+            break;
+          }
+          const uint32_t a = smem_u32(sm + st * kGStageBytes);
+          const uint32_t b = a + kGABytes;
+          const uint32_t bar = smem_u32(&full[st]);
+          const int seg = kb / nk1;
+          const int kx = (int)(kbeg + s * kspan) + (kb - seg * nk1) * kE;
+          const CUtensorMap* ma = (seg == 2) ? &tmap_lo : &tmap;
+          const CUtensorMap* mb = (seg == 1) ? &tmap_lo : &tmap;
+          mbar_expect_tx(bar, kGStageBytes);
+          tma_load_2d(a, ma, bar, kx, i0);
+          tma_load_2d(a + kGBoxBytes, ma, bar, kx, i0 + kGMH);
+          tma_load_2d(b, mb, bar, kx, j0);
+          tma_load_2d(b + kGBoxBytes, mb, bar, kx, j0 + kGMH);
+          ++g;
+        }
       }
+      // the copies still in flight land before the CTA exits
+      for (uint32_t h = g > (uint32_t)kGStages ? g - kGStages : 0u; h < g; ++h)
+        mbar_wait(smem_u32(&full[h % kGStages]), (h / kGStages) & 1, err, 5);
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % kGStages;
-        const int c = kb / chunk;
-        const bool first = (kb % chunk) == 0;
-        const bool last = (kb % chunk) == chunk - 1 || kb == nk - 1;
-        // a new chunk waits until the epilogue drained the previous one
-        if (first && c >= 1 && !mbar_wait(smem_u32(tempty), (c - 1) & 1, err, 4)) break;
-        if (!mbar_wait(smem_u32(&full[s]), (kb / kGStages) & 1, err, 2)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a = smem_u32(sm + s * kGStageBytes);
-        const uint32_t b = a + kGABytes;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {  // 32 bytes of K per MMA: 8 TF32 or 16 BF16 elements
-          const uint64_t bd = umma_desc_sw128(b + 32 * k);
-          const uint32_t acc = !(first && k == 0);
-          if constexpr (BF16) {
-            umma_bf16(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
-            umma_bf16(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
-          } else {
-            umma_tf32(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
-            umma_tf32(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+      uint32_t g = 0, cc = 0;  // stages consumed, accumulator chunks committed
+      bool ok = true;
+      for (uint32_t n = 0; ok; ++n) {
+        const int slot = (int)(n % kGItems);
+        if (!mbar_wait(smem_u32(&ifull[slot]), (n / kGItems) & 1, err, 9)) break;
+        const int64_t item = sitem[slot];
+        mbar_arrive(smem_u32(&iempty[slot]));
+        if (item >= items) break;
+        const int nk = seg_blocks(item / tiles) * segs;
+        for (int kb = 0; kb < nk; ++kb) {
+          const int st = (int)(g % kGStages);
+          const bool first = (kb % chunk) == 0;
+          const bool last = (kb % chunk) == chunk - 1 || kb == nk - 1;
+          // a new chunk waits until the epilogue drained the previous one
+          if (first && cc >= 1 && !mbar_wait(smem_u32(tempty), (cc - 1) & 1, err, 4)) {
+            ok = false;
+            break;
           }
+          if (!mbar_wait(smem_u32(&full[st]), (g / kGStages) & 1, err, 2)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a = smem_u32(sm + st * kGStageBytes);
+          const uint32_t b = a + kGABytes;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {  // 32 bytes of K per MMA: 8 TF32 or 16 BF16 elements
+            const uint64_t bd = umma_desc_sw128(b + 32 * k);
+            const uint32_t acc = !(first && k == 0);
+            if constexpr (BF16) {
+              umma_bf16(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
+              umma_bf16(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+            } else {
+              umma_tf32(tmem, umma_desc_sw128(a + 32 * k), bd, acc);
+              umma_tf32(tmem + kGN, umma_desc_sw128(a + kGBoxBytes + 32 * k), bd, acc);
+            }
+          }
+          umma_commit(smem_u32(&empty[st]));
+          if (last) {
+            umma_commit(smem_u32(tfull));
+            ++cc;
+          }
+          ++g;
         }
-        umma_commit(smem_u32(&empty[s]));
-        if (last) umma_commit(smem_u32(tfull));
       }
+      // every MMA issued completes before the accumulators are freed
+      umma_commit(smem_u32(mdone));
+      mbar_wait(smem_u32(mdone), 0, err, 6);
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 of both accumulators
@@ -236,42 +324,87 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     // the FP64 output rows
     const int q = warp & 3;
     const int row = 32 * q + lane;
-    const int nchunk = (nk + chunk - 1) / chunk;
-    for (int c = 0; c < nchunk; ++c) {
-      // warp-uniform outcome: tcgen05.ld below needs the whole warp
-      const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(tfull), c & 1, err, 3));
-      if (!got) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
-        const int64_t gi = (int64_t)i0 + h * kGMH + row;
-#pragma unroll 1
-        for (int c0 = 0; c0 < kGN; c0 += 32) {
-          uint32_t v[32];
-          const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * kGN + c0);
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-              : "r"(taddr));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          if (gi < M) {
-            double* dst = H + gi * ldh + j0 + c0;
-#pragma unroll
-            for (int u = 0; u < 32; ++u)
-              if ((int64_t)j0 + c0 + u < M) {
-                const double x = alpha * (double)__uint_as_float(v[u]);
-                dst[u] = (c == 0 && !accumulate) ? x : dst[u] + x;
-              }
-          }
+    uint32_t cc = 0;  // accumulator chunks drained
+    bool ok = true;
+    for (uint32_t n = 0; ok; ++n) {
+      const int slot = (int)(n % kGItems);
+      int64_t item = items;
+      if (lane == 0) {
+        if (mbar_wait(smem_u32(&ifull[slot]), (n / kGItems) & 1, err, 10)) {
+          item = sitem[slot];
+          mbar_arrive(smem_u32(&iempty[slot]));
         }
       }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(tempty)) : "memory");
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if (item >= items) break;
+      const int64_t s = item / tiles, t = item - s * tiles;
+      int i0, j0;
+      gram_tile(t, nbi, nbj, i0, j0);
+      const int nk = seg_blocks(s) * segs;
+      const int nchunk = (nk + chunk - 1) / chunk;
+      if (s > 0) {
+        // the four epilogue warps of segment s - 1 have added their rows
+        bool seen = true;
+        if (lane == 0) {
+          const int want = 4 * (int)s;
+          long long i = 0;
+          while (ld_acquire(done + t) < want && ++i < kGWaitLimit) __nanosleep(64);
+          seen = i < kGWaitLimit;
+          if (!seen) atomicExch(err, 7);
+        }
+        if (!__shfl_sync(0xffffffffu, (int)seen, 0)) break;
+        (void)ld_acquire(done + t);  // every lane orders its reads of H after the flag
+      }
+      for (int c = 0; c < nchunk; ++c, ++cc) {
+        // warp-uniform outcome: tcgen05.ld below needs the whole warp
+        const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(tfull), cc & 1, err, 3));
+        if (!got) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const bool write = (c == 0 && s == 0 && !accumulate);
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int64_t gi = (int64_t)i0 + h * kGMH + row;
+#pragma unroll 1
+          for (int c0 = 0; c0 < kGN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * kGN + c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (gi < M) {
+              double* dst = H + gi * ldh + j0 + c0;
+#pragma unroll
+              for (int u = 0; u < 32; ++u)
+                if ((int64_t)j0 + c0 + u < M) {
+                  const double x = alpha * (double)__uint_as_float(v[u]);
+                  dst[u] = write ? x : dst[u] + x;
+                }
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(tempty)) : "memory");
+      }
+      if (!ok) break;
+      if (nseg > 1) {
+        // publish this warp's rows of tile t through segment s
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence();
+          atomicAdd(done + t, 1);
+        }
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -331,7 +464,11 @@ static int make_map(CUtensorMap* map, const void* J, int64_t M, int64_t K, int64
 
 extern "C" {
 
-size_t rb_gram_work_bytes(void) { return 256; }
+// workspace: the error word, the item counter (byte 128), then one progress
+// counter per tile from byte 256 (up to
+// kGFlags tiles: M up to about 92,000 rows in one persistent launch)
+constexpr int64_t kGFlags = 65536;
+size_t rb_gram_work_bytes(void) { return 256 + (size_t)kGFlags * sizeof(int); }
 
 static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_t K, int64_t ldj, double alpha,
                     double* H, int64_t ldh, void* work, size_t work_bytes, void* stream) {
@@ -345,28 +482,63 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
   CUtensorMap map, map_lo;
   RB_TRY(make_map(&map, J, M, K, ldj, bf16));
   RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj, bf16));
-  const int segs = Jlo ? 3 : 1;
+  int segs = Jlo ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   int* err = reinterpret_cast<int*>(work);
+  unsigned long long* next = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(work) + 128);
+  int* done = reinterpret_cast<int*>(static_cast<unsigned char*>(work) + 256);
   RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
   const int64_t nbi = ceil_div(M, kGM), nbj = ceil_div(M, kGN);
   int64_t tiles = 0;
   for (int64_t bj = 0; bj < nbj; ++bj) tiles += gram_col_tiles(bj, nbi);
-  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-  RB_CUDA_TRY(cudaFuncSetAttribute(gram_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-  // K in ranges of 65536 per launch (a multiple of every stage row): a
-  // launch's CTAs stay close to each other in K, so more of the slab of J they
-  // share is still in L2 (measured 5-6% faster than one launch at K = 10^6)
-  const int64_t kspan = 65536;
-  for (int64_t kb = 0; kb < K; kb += kspan) {
-    const int64_t ke = std::min<int64_t>(K, kb + kspan);
-    if (bf16)
-      gram_tf32_kernel<true><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, kb, ke, kb > 0, H, ldh,
-                                                                          alpha, err);
-    else
-      gram_tf32_kernel<false><<<(unsigned)tiles, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, kb, ke, kb > 0, H,
-                                                                           ldh, alpha, err);
-    RB_LAUNCH_CHECK();
+  const void* fn = bf16 ? reinterpret_cast<const void*>(&gram_tf32_kernel<true>)
+                        : reinterpret_cast<const void*>(&gram_tf32_kernel<false>);
+  RB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  int dev = 0, sms = 0, per_sm = 0;
+  RB_CUDA_TRY(cudaGetDevice(&dev));
+  RB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGThreads, kGSmem));
+  if (per_sm < 1 || sms < 1) return fail(RB_ECUDA, "rb_gram: the tile kernel does not fit on an SM");
+  const int64_t resident = (int64_t)sms * per_sm;
+  // K in launches of 65536: a launch boundary brings every CTA back to the
+  // same K, so the slab of J they share stays in L2 (one launch over all of K
+  // let the CTAs drift apart: 276 against 238 ms at 8192 x 1,040,502).  Inside
+  // a launch the items are (tile, 16384 K) pairs, one accumulator chunk of the
+  // single-pass forms, so the last round is short: 2112 items on 148 SMs
+  // instead of 528 tiles in 4 waves with the last one 57% full.
+  const int64_t kseg = 65536, kitem = 16384;  // multiples of every stage row
+  int64_t kspan = kitem, kbeg = 0, klen = 0;
+  int accumulate = 0;
+  if (tiles <= kGFlags) {
+    for (kbeg = 0; kbeg < K; kbeg += kseg) {
+      klen = std::min<int64_t>(kseg, K - kbeg);
+      accumulate = kbeg > 0;
+      RB_CUDA_TRY(cudaMemsetAsync(next, 0, 128 + (size_t)tiles * sizeof(int), st));  // item counter, progress
+      const int64_t items = tiles * ceil_div(klen, kspan);
+      const dim3 grid((unsigned)std::min<int64_t>(items, resident)), block(kGThreads);
+      void* args[] = {(void*)&map,  (void*)&map_lo, (void*)&segs,       (void*)&M,   (void*)&kbeg,
+                      (void*)&klen, (void*)&kspan,  (void*)&tiles,      (void*)&accumulate, (void*)&H,
+                      (void*)&ldh,  (void*)&alpha,  (void*)&done,       (void*)&next, (void*)&err};
+      // cooperative: every CTA resident, so the per-tile ordering waits end
+      RB_CUDA_TRY(cudaLaunchCooperativeKernel(fn, grid, block, args, (size_t)kGSmem, st));
+    }
+  } else {
+    // more tiles than progress counters: items are whole tiles of one launch
+    // (no ordering between CTAs needed)
+    kspan = kseg;
+    const dim3 grid((unsigned)std::min<int64_t>(tiles, resident));
+    for (kbeg = 0; kbeg < K; kbeg += kseg) {
+      klen = std::min<int64_t>(kseg, K - kbeg);
+      accumulate = kbeg > 0;
+      RB_CUDA_TRY(cudaMemsetAsync(next, 0, sizeof(unsigned long long), st));
+      if (bf16)
+        gram_tf32_kernel<true><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, kbeg, klen, kspan, tiles,
+                                                                 accumulate, H, ldh, alpha, done, next, err);
+      else
+        gram_tf32_kernel<false><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, kbeg, klen, kspan, tiles,
+                                                                  accumulate, H, ldh, alpha, done, next, err);
+      RB_LAUNCH_CHECK();
+    }
   }
   dim3 mg((unsigned)ceil_div(M, 32), (unsigned)ceil_div(M, 32));
   mirror_upper_kernel<<<mg, dim3(32, 8), 0, st>>>(H, M, ldh);

@@ -52,6 +52,30 @@ def test_gram_long_k_accuracy():
         assert err < tol, (precision, err)
 
 
+@pytest.mark.parametrize("precision,tol", [("tf32", 3e-3), ("tf32x3", 6e-5), ("bf16", 1e-3)])
+def test_gram_segments_in_order(precision, tol):
+    """Several tiles and three K segments of 65536: the persistent launch adds
+    segment s of a tile only after segment s - 1 (items running at once wait
+    on each other); the result is the same on every run."""
+    rng = np.random.default_rng(7)
+    M, K = 520, 140001
+    A = rng.standard_normal((M, K)) * np.exp(-np.linspace(0, 4, K))[None, :]
+    if precision == "bf16":
+        J, Kc, Ar = _bf16_rows(A)
+        args = ()
+    else:
+        J, Kc = rbb.recon._device_rows(A)
+        Ar = A.astype(np.float32).astype(np.float64)
+        args = (precision,)
+    H1, _ = engine.gram(J.clone(), Kc, 1.0, *args)
+    H2, _ = engine.gram(J.clone(), Kc, 1.0, *args)
+    H1, H2 = H1.cpu().numpy(), H2.cpu().numpy()
+    ref = Ar @ Ar.T
+    assert np.abs(H1 - ref).max() / np.abs(ref).max() < tol
+    assert np.array_equal(H1, H2)
+    assert np.array_equal(H1, H1.T)
+
+
 def test_reginv_matches_reference(golden):
     g = golden("dense_recon")
     for got, ref in ((rbb.reginvunder(g["Ju"], g["ru"], 0.1), g["under"]),
