@@ -324,6 +324,20 @@ int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj,
             double* H, int64_t ldh, void* work, size_t work_bytes, void* stream);
 int rb_gram_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
                  void* work, size_t work_bytes, void* stream);
+/* Optional staging buffer (same results, bit for bit): the tiles are formed
+ * from column slabs of J (65536 wide) copied into a compact buffer first.
+ * Long rows (a row stride of megabytes) spread one slab over a page per row;
+ * the compact slab halves the time of a slab's products at 8192 x 1,040,502.
+ * rb_gram_stage_bytes returns the bytes to pass (0: staging does not pay for
+ * this shape; the staged calls then run as the plain ones).  elem_bytes is 4
+ * (FP32) or 2 (BF16); split != 0 when Jlo is given. */
+size_t rb_gram_stage_bytes(int64_t M, int64_t K, int64_t ldj, int32_t elem_bytes, int32_t split);
+int rb_gram_staged(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha,
+                   double* H, int64_t ldh, void* stage, size_t stage_bytes, void* work, size_t work_bytes,
+                   void* stream);
+int rb_gram_bf16_staged(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H,
+                        int64_t ldh, void* stage, size_t stage_bytes, void* work, size_t work_bytes,
+                        void* stream);
 int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* stream);
 int rb_reginv_prepare(double* H, int64_t M, int64_t ldh, double lambda, double* di, void* stream);
 size_t rb_cholesky_work_bytes(void);

@@ -92,6 +92,9 @@ _SIGS = {
     "rb_gram_work_bytes": (_sz, []),
     "rb_gram": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp]),
     "rb_gram_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp]),
+    "rb_gram_stage_bytes": (_sz, [_i64, _i64, _i64, _i32, _i32]),
+    "rb_gram_staged": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp, _sz, _vp]),
+    "rb_gram_bf16_staged": (ctypes.c_int, [_vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp, _sz, _vp]),
     "rb_split_tf32": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
     "rb_reginv_prepare": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _vp, _vp]),
     "rb_cholesky_work_bytes": (_sz, []),

@@ -412,6 +412,30 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGTmemCols));
 }
 
+// S[r][0 .. nb) = J[r][b0 .. b0 + nb) in bytes (16-byte pieces, nb a multiple
+// of 16): the column slab of one launch, copied into a compact buffer; rows
+// on grid y, 16-byte pieces of a row on grid x, four per thread in flight
+__global__ void __launch_bounds__(256) slab_copy_kernel(const unsigned char* __restrict__ J, int64_t ldj_b, int64_t b0,
+                                                        int64_t nb, unsigned char* __restrict__ S, int64_t lds_b,
+                                                        int64_t M) {
+  const int64_t per_row = nb >> 4;
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = blockIdx.y; r < M; r += gridDim.y) {
+    const int4* __restrict__ src = reinterpret_cast<const int4*>(J + r * ldj_b + b0);
+    int4* __restrict__ dst = reinterpret_cast<int4*>(S + r * lds_b);
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; c + 3 * step < per_row; c += 4 * step) {
+      const int4 v0 = __ldcs(src + c), v1 = __ldcs(src + c + step), v2 = __ldcs(src + c + 2 * step),
+                 v3 = __ldcs(src + c + 3 * step);
+      dst[c] = v0;
+      dst[c + step] = v1;
+      dst[c + 2 * step] = v2;
+      dst[c + 3 * step] = v3;
+    }
+    for (; c < per_row; c += step) dst[c] = __ldcs(src + c);
+  }
+}
+
 // H[j][i] = H[i][j] for i < j (upper triangle -> lower)
 __global__ void mirror_upper_kernel(double* __restrict__ H, int64_t M, int64_t ldh) {
   __shared__ double tile[32][33];
@@ -470,8 +494,21 @@ extern "C" {
 constexpr int64_t kGFlags = 65536;
 size_t rb_gram_work_bytes(void) { return 256 + (size_t)kGFlags * sizeof(int); }
 
+// K per launch: a launch boundary brings every CTA back to the same K, so the
+// slab of J they share stays in L2 (one launch over all of K let the CTAs
+// drift apart: 276 against 238 ms at 8192 x 1,040,502)
+constexpr int64_t kGSeg = 65536;
+// rows longer than this (bytes) are staged slab by slab when a buffer is given
+constexpr int64_t kGStageRow = 1 << 20;
+
+size_t rb_gram_stage_bytes(int64_t M, int64_t K, int64_t ldj, int32_t elem_bytes, int32_t split) {
+  if (M < 1 || K < 1 || (elem_bytes != 2 && elem_bytes != 4) || ldj * elem_bytes <= kGStageRow) return 0;
+  return (size_t)M * kGSeg * elem_bytes * (split ? 2 : 1) + 256;
+}
+
 static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_t K, int64_t ldj, double alpha,
-                    double* H, int64_t ldh, void* work, size_t work_bytes, void* stream) {
+                    double* H, int64_t ldh, void* stage, size_t stage_bytes, void* work, size_t work_bytes,
+                    void* stream) {
   if (!J || !H || !work || M < 1 || K < 1 || ldj < K || ldh < M)
     return fail(RB_EARG, "rb_gram: bad arguments");
   if (work_bytes < rb_gram_work_bytes()) return fail(RB_EARG, "rb_gram: workspace too small");
@@ -479,9 +516,18 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
   if ((reinterpret_cast<uintptr_t>(J) & 15) || (Jlo && (reinterpret_cast<uintptr_t>(Jlo) & 15)) || (ldj % lda))
     return fail(RB_EARG, "rb_gram: J must be 16-byte aligned with a row stride that is a multiple of 16 bytes");
   if (M > (int64_t)1 << 30 || K > (int64_t)1 << 30) return fail(RB_ESIZE, "rb_gram: matrix too large");
+  const int eb = bf16 ? 2 : 4;
+  const size_t need = rb_gram_stage_bytes(M, K, ldj, eb, Jlo != nullptr);
+  const bool staged = stage && need > 0;
+  if (staged && (stage_bytes < need || (reinterpret_cast<uintptr_t>(stage) & 15)))
+    return fail(RB_EARG, "rb_gram: staging buffer too small or not 16-byte aligned");
+  unsigned char* S = static_cast<unsigned char*>(stage);
+  unsigned char* Slo = staged && Jlo ? S + (size_t)M * kGSeg * eb : nullptr;
   CUtensorMap map, map_lo;
-  RB_TRY(make_map(&map, J, M, K, ldj, bf16));
-  RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj, bf16));
+  if (!staged) {
+    RB_TRY(make_map(&map, J, M, K, ldj, bf16));
+    RB_TRY(make_map(&map_lo, Jlo ? Jlo : J, M, K, ldj, bf16));
+  }
   int segs = Jlo ? 3 : 1;
   cudaStream_t st = as_stream(stream);
   int* err = reinterpret_cast<int*>(work);
@@ -500,23 +546,42 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
   RB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGThreads, kGSmem));
   if (per_sm < 1 || sms < 1) return fail(RB_ECUDA, "rb_gram: the tile kernel does not fit on an SM");
   const int64_t resident = (int64_t)sms * per_sm;
-  // K in launches of 65536: a launch boundary brings every CTA back to the
-  // same K, so the slab of J they share stays in L2 (one launch over all of K
-  // let the CTAs drift apart: 276 against 238 ms at 8192 x 1,040,502).  Inside
-  // a launch the items are (tile, 16384 K) pairs, one accumulator chunk of the
-  // single-pass forms, so the last round is short: 2112 items on 148 SMs
-  // instead of 528 tiles in 4 waves with the last one 57% full.
-  const int64_t kseg = 65536, kitem = 16384;  // multiples of every stage row
-  int64_t kspan = kitem, kbeg = 0, klen = 0;
+  // Inside a launch the items are (tile, 16384 K) pairs, one accumulator
+  // chunk of the single-pass forms, so the last round is short: 2112 items on
+  // 148 SMs instead of 528 tiles in 4 waves with the last one 57% full.
+  const int64_t kseg = kGSeg, kitem = 16384;  // multiples of every stage row
+  int64_t kspan = kitem, kbeg = 0, klen = 0, koff = 0;
   int accumulate = 0;
+  // staged: copy the launch's slab of J (and Jlo) into the compact buffer and
+  // map that instead; the kernel's K offset is then 0
+  auto stage_slab = [&]() -> int {
+    if (!staged) {
+      koff = kbeg;
+      return RB_OK;
+    }
+    const int64_t nb = (klen * eb + 15) / 16 * 16;
+    const dim3 g((unsigned)std::max<int64_t>(1, ceil_div(nb / 16, 256 * 4)), (unsigned)std::min<int64_t>(M, 65535));
+    slab_copy_kernel<<<g, 256, 0, st>>>(static_cast<const unsigned char*>(J), ldj * eb, kbeg * eb, nb, S, kseg * eb, M);
+    RB_LAUNCH_CHECK();
+    if (Jlo) {
+      slab_copy_kernel<<<g, 256, 0, st>>>(static_cast<const unsigned char*>(Jlo), ldj * eb, kbeg * eb, nb, Slo,
+                                          kseg * eb, M);
+      RB_LAUNCH_CHECK();
+    }
+    RB_TRY(make_map(&map, S, M, klen, kseg, bf16));
+    RB_TRY(make_map(&map_lo, Jlo ? Slo : S, M, klen, kseg, bf16));
+    koff = 0;
+    return RB_OK;
+  };
   if (tiles <= kGFlags) {
     for (kbeg = 0; kbeg < K; kbeg += kseg) {
       klen = std::min<int64_t>(kseg, K - kbeg);
       accumulate = kbeg > 0;
+      RB_TRY(stage_slab());
       RB_CUDA_TRY(cudaMemsetAsync(next, 0, 128 + (size_t)tiles * sizeof(int), st));  // item counter, progress
       const int64_t items = tiles * ceil_div(klen, kspan);
       const dim3 grid((unsigned)std::min<int64_t>(items, resident)), block(kGThreads);
-      void* args[] = {(void*)&map,  (void*)&map_lo, (void*)&segs,       (void*)&M,   (void*)&kbeg,
+      void* args[] = {(void*)&map,  (void*)&map_lo, (void*)&segs,       (void*)&M,   (void*)&koff,
                       (void*)&klen, (void*)&kspan,  (void*)&tiles,      (void*)&accumulate, (void*)&H,
                       (void*)&ldh,  (void*)&alpha,  (void*)&done,       (void*)&next, (void*)&err};
       // cooperative: every CTA resident, so the per-tile ordering waits end
@@ -530,12 +595,13 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
     for (kbeg = 0; kbeg < K; kbeg += kseg) {
       klen = std::min<int64_t>(kseg, K - kbeg);
       accumulate = kbeg > 0;
+      RB_TRY(stage_slab());
       RB_CUDA_TRY(cudaMemsetAsync(next, 0, sizeof(unsigned long long), st));
       if (bf16)
-        gram_tf32_kernel<true><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, kbeg, klen, kspan, tiles,
+        gram_tf32_kernel<true><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, 1, M, koff, klen, kspan, tiles,
                                                                  accumulate, H, ldh, alpha, done, next, err);
       else
-        gram_tf32_kernel<false><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, kbeg, klen, kspan, tiles,
+        gram_tf32_kernel<false><<<grid, kGThreads, kGSmem, st>>>(map, map_lo, segs, M, koff, klen, kspan, tiles,
                                                                   accumulate, H, ldh, alpha, done, next, err);
       RB_LAUNCH_CHECK();
     }
@@ -552,12 +618,22 @@ static int gram_run(const void* J, const void* Jlo, bool bf16, int64_t M, int64_
 
 int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
             void* work, size_t work_bytes, void* stream) {
-  return gram_run(J, Jlo, false, M, K, ldj, alpha, H, ldh, work, work_bytes, stream);
+  return gram_run(J, Jlo, false, M, K, ldj, alpha, H, ldh, nullptr, 0, work, work_bytes, stream);
+}
+
+int rb_gram_staged(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha, double* H,
+                   int64_t ldh, void* stage, size_t stage_bytes, void* work, size_t work_bytes, void* stream) {
+  return gram_run(J, Jlo, false, M, K, ldj, alpha, H, ldh, stage, stage_bytes, work, work_bytes, stream);
 }
 
 int rb_gram_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh, void* work,
                  size_t work_bytes, void* stream) {
-  return gram_run(J, nullptr, true, M, K, ldj, alpha, H, ldh, work, work_bytes, stream);
+  return gram_run(J, nullptr, true, M, K, ldj, alpha, H, ldh, nullptr, 0, work, work_bytes, stream);
+}
+
+int rb_gram_bf16_staged(const void* J, int64_t M, int64_t K, int64_t ldj, double alpha, double* H, int64_t ldh,
+                        void* stage, size_t stage_bytes, void* work, size_t work_bytes, void* stream) {
+  return gram_run(J, nullptr, true, M, K, ldj, alpha, H, ldh, stage, stage_bytes, work, work_bytes, stream);
 }
 
 }  // extern "C"

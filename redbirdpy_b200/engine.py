@@ -675,19 +675,25 @@ def gram(J, K, alpha=1.0, precision="tf32"):
     M, ldj = J.shape
     H = torch.empty((M, M), dtype=torch.float64, device=J.device)
     lo = None
-    if J.dtype == torch.bfloat16:
-        wb = _lib.lib().rb_gram_work_bytes()
-        work = torch.empty(wb, dtype=torch.uint8, device=J.device)
-        call("rb_gram_bf16", ptr(J), M, K, ldj, float(alpha), ptr(H), M, ptr(work), wb, stream())
-        return H, None
-    if precision == "tf32x3":
-        lo = torch.empty_like(J)
-        call("rb_split_tf32", ptr(J), ptr(lo), M, K, ldj, stream())
-    elif precision != "tf32":
-        raise ValueError(f"unknown gram precision {precision}")
     wb = _lib.lib().rb_gram_work_bytes()
     work = torch.empty(wb, dtype=torch.uint8, device=J.device)
-    call("rb_gram", ptr(J), ptr(lo), M, K, ldj, float(alpha), ptr(H), M, ptr(work), wb, stream())
+    bf16 = J.dtype == torch.bfloat16
+    if not bf16:
+        if precision == "tf32x3":
+            lo = torch.empty_like(J)
+            call("rb_split_tf32", ptr(J), ptr(lo), M, K, ldj, stream())
+        elif precision != "tf32":
+            raise ValueError(f"unknown gram precision {precision}")
+    # long rows: the products are formed from compact copies of J's column
+    # slabs (same result; 2x faster slabs at a row stride of megabytes)
+    sb = _lib.lib().rb_gram_stage_bytes(M, K, ldj, 2 if bf16 else 4, int(lo is not None))
+    stage = torch.empty(sb, dtype=torch.uint8, device=J.device) if sb else None
+    sp = ptr(stage) if stage is not None else None
+    if bf16:
+        call("rb_gram_bf16_staged", ptr(J), M, K, ldj, float(alpha), ptr(H), M, sp, sb, ptr(work), wb, stream())
+    else:
+        call("rb_gram_staged", ptr(J), ptr(lo), M, K, ldj, float(alpha), ptr(H), M, sp, sb, ptr(work), wb,
+             stream())
     return H, lo
 
 

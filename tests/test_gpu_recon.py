@@ -76,6 +76,42 @@ def test_gram_segments_in_order(precision, tol):
     assert np.array_equal(H1, H1.T)
 
 
+@pytest.mark.parametrize("precision", ["tf32", "tf32x3", "bf16"])
+def test_gram_staged_slabs_bit_identical(precision):
+    """Rows longer than 1 MB take the staged path (compact copies of each
+    65536-column slab): the same bits as the products formed in place, and
+    within the tolerance of the FP64 product."""
+    from redbirdpy_b200 import _lib
+    rng = np.random.default_rng(11)
+    M, K = (200, 600001) if precision == "bf16" else (300, 300001)  # rows of 1.2 MB
+    A = rng.standard_normal((M, K)) * np.exp(-np.linspace(0, 4, K))[None, :]
+    if precision == "bf16":
+        J, Kc, Ar = _bf16_rows(A)
+        args = ()
+    else:
+        J, Kc = rbb.recon._device_rows(A)
+        Ar = A.astype(np.float32).astype(np.float64)
+        args = (precision,)
+    ldj = J.shape[1]
+    assert _lib.lib().rb_gram_stage_bytes(M, Kc, ldj, 2 if precision == "bf16" else 4,
+                                          int(precision == "tf32x3")) > 0
+    Hs, lo = engine.gram(J, Kc, 1.0, *args)  # staged (J is left as hi for tf32x3)
+    wb = _lib.lib().rb_gram_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    Hp = torch.empty_like(Hs)
+    if precision == "bf16":
+        engine.call("rb_gram_bf16", engine.ptr(J), M, Kc, ldj, 1.0, engine.ptr(Hp), M, engine.ptr(work), wb,
+                    engine.stream())
+    else:
+        engine.call("rb_gram", engine.ptr(J), engine.ptr(lo), M, Kc, ldj, 1.0, engine.ptr(Hp), M,
+                    engine.ptr(work), wb, engine.stream())
+    Hs, Hp = Hs.cpu().numpy(), Hp.cpu().numpy()
+    assert np.array_equal(Hs, Hp)
+    ref = Ar @ Ar.T
+    tol = {"tf32": 3e-3, "tf32x3": 6e-5, "bf16": 1e-3}[precision]
+    assert np.abs(Hs - ref).max() / np.abs(ref).max() < tol
+
+
 def test_reginv_matches_reference(golden):
     g = golden("dense_recon")
     for got, ref in ((rbb.reginvunder(g["Ju"], g["ru"], 0.1), g["under"]),
