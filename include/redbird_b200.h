@@ -315,9 +315,12 @@ int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, co
  *                              BF16 A and B), ldj % 8 == 0: half the bytes and
  *                              twice the tensor rate of TF32.
  *   H += lambda I, normalise   rb_reginv_prepare (_normalize_diag, recon.py:784-789)
- *   H = L L^T                  rb_cholesky (FP64, in place, lower)
- *   L L^T x = b                rb_chol_solve (in place on x)
- *   out = alpha J^T y + beta out   rb_gemv_t
+ *   H = L L^T                  rb_cholesky (FP64, in place, lower; the strict
+ *                              upper triangle of each 64 x 64 diagonal block
+ *                              receives that block's inverse, transposed)
+ *   L L^T x = b                rb_chol_solve (in place on x; L as rb_cholesky
+ *                              leaves it, diagonal-block inverses included)
+ *   out = alpha J^T y + beta out   rb_gemv_t (J aligned as for rb_gram; ldj % 4 == 0)
  *   sum(J^2)                   rb_sumsq (Frobenius block scale, recon.py:235) */
 size_t rb_gram_work_bytes(void);
 int rb_gram(const float* J, const float* Jlo, int64_t M, int64_t K, int64_t ldj, double alpha,

@@ -1,7 +1,8 @@
 // Dense FP64 pieces of the Gauss-Newton step (reginvunder,
 // redbirdpy/recon.py:429-509 and _normalize_diag, recon.py:784-789):
 //   H += lambda I, di = 1/sqrt(|diag H| + 1e-16), H <- di H di     (prepare)
-//   H = L L^T, blocked right-looking Cholesky (64-wide panels)      (cholesky)
+//   H = L L^T, blocked right-looking Cholesky (64-wide panels; the
+//   inverse of each diagonal block kept in its strict upper triangle)  (cholesky)
 //   L L^T x = b                                                    (chol_solve)
 //   out = alpha * J^T y   (J FP32 M x K rows, y FP64)              (gemv_t)
 //   sum(J^2)              (Frobenius block scaling, recon.py:235)   (sumsq)
@@ -52,59 +53,156 @@ __device__ __forceinline__ void load_lower(const double* __restrict__ H, int64_t
   }
 }
 
-// factor the nb x nb diagonal block at (j0, j0) in shared memory (lower)
-__global__ void potrf_diag_kernel(double* __restrict__ H, int64_t ldh, int64_t j0, int nb, int* __restrict__ err) {
-  __shared__ double A[kNB][kNB + 1];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  load_lower<kNB + 1>(H, ldh, j0, j0, nb, A);
-  __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    __shared__ double piv;
-    if (tid == 0) {
-      const double d = A[c][c];
-      if (!(d > 0.0) || !isfinite(d)) {
-        atomicExch(err, (int)(j0 + c) + 1);
-        piv = 1.0;
-      } else {
-        piv = sqrt(d);
-      }
-      A[c][c] = piv;
-    }
-    __syncthreads();
-    for (int i = c + 1 + tid; i < nb; i += nt) A[i][c] /= piv;
-    __syncthreads();
-    // trailing update of the lower part: A[i][j] -= A[i][c] A[j][c], c < j <= i
-    const int m = nb - c - 1;
-    for (int e = tid; e < m * m; e += nt) {
-      const int i = c + 1 + e / m, j = c + 1 + e % m;
-      if (j <= i) A[i][j] -= A[i][c] * A[j][c];
-    }
-    __syncthreads();
+// Factor the nb x nb diagonal block at (j0, j0) (lower, L11) and form its
+// inverse X = L11^-1.  256 threads; thread (j = tid / 4, q = tid % 4) owns
+// column j, rows q, q + 4, ..., so the 4 owners of a column are 4 lanes of
+// one warp and exchange through shuffles.  Column c is scaled by its owners
+// (the pivot comes from the lane holding the diagonal), published to shared
+// memory (two buffers, so one barrier per column), and every thread updates
+// its entries right of c.  X is formed column by column by forward
+// substitution (the 4 owners of column j sum their own rows' terms, fixed
+// order) and stored transposed in the block's strict upper triangle:
+// H[j0 + j][j0 + i] = X[i][j], i > j (the diagonal of X is 1 / L[i][i]).
+// The panel solve and rb_chol_solve then apply X as a product.
+__global__ void __launch_bounds__(256) potrf_diag_kernel(double* __restrict__ H, int64_t ldh, int64_t j0, int nb,
+                                                         int* __restrict__ err) {
+  __shared__ double col[2][kNB];
+  __shared__ double Ls[kNB][kNB + 1];
+  const int tid = threadIdx.x;
+  const int j = tid >> 2, q = tid & 3;
+  const int lane = tid & 31;
+  const unsigned quad = 0xFu << (lane & ~3);
+  double a[kNB / 4];
+#pragma unroll
+  for (int u = 0; u < kNB / 4; ++u) {
+    const int i = q + 4 * u;
+    a[u] = (i < nb && j < nb && i >= j) ? H[(j0 + i) * ldh + j0 + j] : 0.0;
   }
-  for (int e = tid; e < nb * nb; e += nt) {
-    const int i = e / nb, j = e % nb;
-    if (j <= i) H[(j0 + i) * ldh + j0 + j] = A[i][j];
+  for (int c = 0; c < nb; ++c) {
+    double* cc = col[c & 1];
+    if (j == c) {  // the 4 owners of column c (one quad of one warp)
+      double d = 0.0;
+#pragma unroll
+      for (int u = 0; u < kNB / 4; ++u)
+        if (q + 4 * u == c) d = a[u];
+      d = __shfl_sync(quad, d, (lane & ~3) | (c & 3));
+      const bool ok = d > 0.0 && isfinite(d);
+      const double piv = ok ? sqrt(d) : 1.0;
+      if (!ok && q == 0) atomicExch(err, (int)(j0 + c) + 1);
+#pragma unroll
+      for (int u = 0; u < kNB / 4; ++u) {
+        const int i = q + 4 * u;
+        if (i >= c && i < nb) {
+          a[u] = (i == c) ? piv : a[u] / piv;
+          cc[i] = a[u];
+        }
+      }
+    }
+    __syncthreads();
+    if (j > c && j < nb) {
+      const double lj = cc[j];
+#pragma unroll
+      for (int u = 0; u < kNB / 4; ++u) {
+        const int i = q + 4 * u;
+        if (i >= j && i < nb) a[u] = fma(-cc[i], lj, a[u]);
+      }
+    }
+  }
+  // L11 back to H (lower) and to shared memory for the inverse
+#pragma unroll
+  for (int u = 0; u < kNB / 4; ++u) {
+    const int i = q + 4 * u;
+    Ls[i][j] = (i >= j && i < nb && j < nb) ? a[u] : 0.0;
+    if (i >= j && i < nb && j < nb) H[(j0 + i) * ldh + j0 + j] = a[u];
+  }
+  __syncthreads();
+  // X = L11^-1, column j by the quad of column j: X[j][j] = 1 / L[j][j],
+  // X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
+  double x[kNB / 4];
+#pragma unroll
+  for (int u = 0; u < kNB / 4; ++u) x[u] = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    double part = 0.0;
+#pragma unroll
+    for (int u = 0; u < kNB / 4; ++u) {
+      const int k = q + 4 * u;
+      if (k >= j && k < i) part = fma(Ls[i][k], x[u], part);
+    }
+    part += __shfl_xor_sync(0xffffffffu, part, 1);
+    part += __shfl_xor_sync(0xffffffffu, part, 2);
+    if (i >= j && j < nb) {
+      const double xi = (i == j) ? 1.0 / Ls[i][i] : -part / Ls[i][i];
+#pragma unroll
+      for (int u = 0; u < kNB / 4; ++u)
+        if (q + 4 * u == i) x[u] = xi;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kNB / 4; ++u) {
+    const int i = q + 4 * u;
+    if (i > j && i < nb && j < nb) H[(j0 + j) * ldh + j0 + i] = x[u];
   }
 }
 
-// L21 = A21 L11^{-T}: one thread per row below the panel, row in smem
-__global__ void trsm_panel_kernel(double* __restrict__ H, int64_t ldh, int64_t M, int64_t j0, int nb) {
-  __shared__ double L[kNB][kNB + 1];
-  extern __shared__ double xs[];  // [kNB][blockDim.x]
-  const int tid = threadIdx.x, nt = blockDim.x;
-  load_lower<kNB + 1>(H, ldh, j0, j0, nb, L);
-  __syncthreads();
-  const int64_t r = j0 + nb + blockIdx.x * (int64_t)nt + tid;
-  if (r >= M) return;
-  double* row = H + r * ldh + j0;
-  // the row itself, loaded up front
-  for (int c = 0; c < nb; ++c) xs[c * nt + tid] = row[c];
-  for (int c = 0; c < nb; ++c) {
-    double s = xs[c * nt + tid];
-    for (int t = 0; t < c; ++t) s -= xs[t * nt + tid] * L[c][t];
-    xs[c * nt + tid] = s / L[c][c];
+// X^T of a factored diagonal block in shared memory: Xt[t][c] = X[c][t]
+// (t <= c; H's strict upper triangle of the block, 1 / L[c][c] on the
+// diagonal, zero below)
+__device__ __forceinline__ void load_inv_t(const double* __restrict__ H, int64_t ldh, int64_t j0, int nb,
+                                           double (*Xt)[kNB + 1]) {
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int t = e / kNB, c = e % kNB;
+    double v = 0.0;
+    if (t < nb && c < nb) {
+      if (c > t) v = H[(j0 + t) * ldh + j0 + c];
+      else if (c == t) v = 1.0 / H[(j0 + t) * ldh + j0 + t];
+    }
+    Xt[t][c] = v;
   }
-  for (int c = 0; c < nb; ++c) row[c] = xs[c * nt + tid];
+}
+
+// L21 = A21 L11^-T = A21 X^T for the rows below the panel: a CTA takes 64
+// rows (4 x 4 outputs per thread), sums t = 0..c in order, and writes its
+// rows back in place
+constexpr int kTrsmSmem = 2 * kNB * (kNB + 1) * (int)sizeof(double);  // dynamic: above the 48 KB static limit
+__global__ void __launch_bounds__(256) trsm_panel_kernel(double* __restrict__ H, int64_t ldh, int64_t M, int64_t j0,
+                                                         int nb) {
+  extern __shared__ double tsm[];
+  double(*Xt)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(tsm);
+  double(*As)[kNB + 1] = Xt + kNB;
+  const int tid = threadIdx.x;
+  const int64_t r0 = j0 + nb + blockIdx.x * (int64_t)kNB;
+  load_inv_t(H, ldh, j0, nb, Xt);
+  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+    const int i = e / kNB, t = e % kNB;
+    As[i][t] = (r0 + i < M && t < nb) ? H[(r0 + i) * ldh + j0 + t] : 0.0;
+  }
+  __syncthreads();
+  const int tr = (tid >> 4) * 4, tc = (tid & 15) * 4;
+  double acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+  const int tmax = min(nb, tc + 4);
+  for (int t = 0; t < tmax; ++t) {
+    double xa[4], xb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xa[u] = As[tr + u][t];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) xb[v] = Xt[t][tc + v];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(xa[u], xb[v], acc[u][v]);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int64_t r = r0 + tr + u;
+      const int c = tc + v;
+      if (r < M && c < nb) H[r * ldh + j0 + c] = acc[u][v];
+    }
 }
 
 // trailing update A22 -= L21 L21^T on 64 x 64 tiles of the lower triangle.
@@ -173,38 +271,31 @@ __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __res
     }
 }
 
-// forward / backward substitution on one 64-block (single CTA)
-// mode 0: solve L_kk y = x (lower), mode 1: solve L_kk^T y = x
-__global__ void tri_block_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb, double* __restrict__ x,
-                                 int mode) {
-  __shared__ double Lb[kNB][kNB + 1];
+// the diagonal-block step of the triangular solves with the block's inverse
+// X (kept by rb_cholesky in the block's strict upper triangle):
+// mode 0: v = X v (solves L_kk y = v), mode 1: v = X^T v (solves L_kk^T y = v).
+// Output i is summed by the 4 lanes of a quad (terms t = q, q + 4, ...) and
+// the quad's partial sums are added in a fixed order.
+__global__ void __launch_bounds__(256) tri_block_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
+                                                        double* __restrict__ x, int mode) {
   __shared__ double v[kNB];
   const int tid = threadIdx.x;
-  load_lower<kNB + 1>(L, ldh, k0, k0, nb, Lb);
+  const int i = tid >> 2, q = tid & 3;
   if (tid < nb) v[tid] = x[k0 + tid];
   __syncthreads();
-  if (tid < 32) {  // one warp: each step's dot product across the lanes
-    const int lane = tid;
-    if (mode == 0) {
-      for (int c = 0; c < nb; ++c) {
-        double s = 0.0;
-        for (int t = lane; t < c; t += 32) s += Lb[c][t] * v[t];
-        s = warp_sum(s);
-        if (lane == 0) v[c] = (v[c] - s) / Lb[c][c];
-        __syncwarp();
-      }
-    } else {
-      for (int c = nb - 1; c >= 0; --c) {
-        double s = 0.0;
-        for (int t = c + 1 + lane; t < nb; t += 32) s += Lb[t][c] * v[t];
-        s = warp_sum(s);
-        if (lane == 0) v[c] = (v[c] - s) / Lb[c][c];
-        __syncwarp();
-      }
+  double s = 0.0;
+  if (i < nb) {
+    if (mode == 0) {  // y[i] = sum_{t <= i} X[i][t] v[t],  X[i][t] = L[k0 + t][k0 + i] (t < i)
+      for (int t = q; t <= i; t += 4)
+        s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + t) * ldh + k0 + i], v[t], s);
+    } else {  // y[i] = sum_{t >= i} X[t][i] v[t],  X[t][i] = L[k0 + i][k0 + t] (t > i)
+      for (int t = i + q; t < nb; t += 4)
+        s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + i) * ldh + k0 + t], v[t], s);
     }
   }
-  __syncthreads();
-  if (tid < nb) x[k0 + tid] = v[tid];
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  if (i < nb && q == 0) x[k0 + i] = s;
 }
 
 // forward: x[r] -= sum_{c in block} L[r][k0+c] x[k0+c] for r >= k0+nb (warp per row)
@@ -236,24 +327,62 @@ constexpr int kGemvSlabs = 16;
 __device__ __forceinline__ double jval(float v) { return v; }
 __device__ __forceinline__ double jval(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-// J stored as FP32 or BF16 (JT)
+// four consecutive entries of a row (16-byte FP32 / 8-byte BF16 loads)
+__device__ __forceinline__ void ld4(const float* p, double (&v)[4]) {
+  const float4 x = __ldcs(reinterpret_cast<const float4*>(p));
+  v[0] = x.x;
+  v[1] = x.y;
+  v[2] = x.z;
+  v[3] = x.w;
+}
+__device__ __forceinline__ void ld4(const __nv_bfloat16* p, double (&v)[4]) {
+  const uint2 x = __ldcs(reinterpret_cast<const uint2*>(p));
+  const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&x.x);
+  const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&x.y);
+  v[0] = __bfloat162float(a.x);
+  v[1] = __bfloat162float(a.y);
+  v[2] = __bfloat162float(b.x);
+  v[3] = __bfloat162float(b.y);
+}
+
+// J stored as FP32 or BF16 (JT).  A thread owns 4 consecutive columns (one
+// vector load per row; ldj % 4 == 0 keeps it aligned and inside the padded
+// row) and sums its slab's rows in 4 interleaved partial sums per column
+// (rows m = 0, 1, 2, 3 mod 4), added as (s0 + s1) + (s2 + s3).
 template <typename JT>
 __global__ void gemv_t_part_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
                                    const double* __restrict__ y, double* __restrict__ part) {
-  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t k = 4 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
   if (k >= K) return;
   const int64_t rows = (M + gridDim.y - 1) / gridDim.y;
   const int64_t m0 = blockIdx.y * rows, m1 = min(M, m0 + rows);
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double s[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s[j][u] = 0.0;
   int64_t m = m0;
   for (; m + 3 < m1; m += 4) {
-    s0 = fma(jval(J[m * ldj + k]), y[m], s0);
-    s1 = fma(jval(J[(m + 1) * ldj + k]), y[m + 1], s1);
-    s2 = fma(jval(J[(m + 2) * ldj + k]), y[m + 2], s2);
-    s3 = fma(jval(J[(m + 3) * ldj + k]), y[m + 3], s3);
+    double v[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ld4(J + (m + u) * ldj + k, v[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double ym = y[m + u];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s[j][u] = fma(v[u][j], ym, s[j][u]);
+    }
   }
-  for (; m < m1; ++m) s0 = fma(jval(J[m * ldj + k]), y[m], s0);
-  part[blockIdx.y * K + k] = (s0 + s1) + (s2 + s3);
+  for (; m < m1; ++m) {
+    double v[4];
+    ld4(J + m * ldj + k, v);
+    const double ym = y[m];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) s[j][0] = fma(v[j], ym, s[j][0]);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (k + j < K) part[blockIdx.y * K + k + j] = (s[j][0] + s[j][1]) + (s[j][2] + s[j][3]);
 }
 
 __global__ void gemv_t_sum_kernel(const double* __restrict__ part, int slabs, int64_t K, double alpha, double beta,
@@ -345,16 +474,14 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
   cudaStream_t st = as_stream(stream);
   int* err = reinterpret_cast<int*>(work);
   RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
-  const int tthreads = 64;
-  const int trsm_smem = (int)(kNB * tthreads * sizeof(double));  // + 33 KB static: opt in above 48 KB
-  RB_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, trsm_smem));
+  RB_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem));
   for (int64_t j0 = 0; j0 < M; j0 += kNB) {
     const int nb = (int)std::min<int64_t>(kNB, M - j0);
     potrf_diag_kernel<<<1, 256, 0, st>>>(H, ldh, j0, nb, err);
     RB_LAUNCH_CHECK();
     const int64_t rest = M - j0 - nb;
     if (rest <= 0) break;
-    trsm_panel_kernel<<<(unsigned)ceil_div(rest, tthreads), tthreads, trsm_smem, st>>>(
+    trsm_panel_kernel<<<(unsigned)ceil_div(rest, kNB), 256, kTrsmSmem, st>>>(
         H, ldh, M, j0, nb);
     RB_LAUNCH_CHECK();
     const int64_t T = ceil_div(rest, kNB);
@@ -396,10 +523,14 @@ static int gemv_t_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const doub
                       double* out, void* work, size_t work_bytes, void* stream) {
   if (!J || !y || !out || !work || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_t: bad arguments");
   if (work_bytes < rb_gemv_t_work_bytes(K)) return fail(RB_EARG, "rb_gemv_t: workspace too small");
+  if ((reinterpret_cast<uintptr_t>(J) & (4 * sizeof(JT) - 1)) || (ldj % 4))
+    return fail(RB_EARG, "rb_gemv_t: J rows must start on %d-byte boundaries (aligned J, ldj %% 4 == 0)",
+                (int)(4 * sizeof(JT)));
   cudaStream_t st = as_stream(stream);
   const int slabs = (int)std::min<int64_t>(kGemvSlabs, M);
   double* part = reinterpret_cast<double*>(work);
-  gemv_t_part_kernel<JT><<<dim3((unsigned)ceil_div(K, 256), (unsigned)slabs), 256, 0, st>>>(J, M, K, ldj, y, part);
+  gemv_t_part_kernel<JT><<<dim3((unsigned)ceil_div(K, 4 * 256), (unsigned)slabs), 256, 0, st>>>(J, M, K, ldj, y,
+                                                                                                part);
   RB_LAUNCH_CHECK();
   gemv_t_sum_kernel<<<(unsigned)ceil_div(K, 256), 256, 0, st>>>(part, slabs, K, alpha, beta, out);
   RB_LAUNCH_CHECK();
