@@ -4,11 +4,14 @@
 // J is M x K FP32, row-major (K contiguous): the Jacobian rows of redbirdpy's
 // jac / matreform layout.  Both MMA operands are row blocks of the same J and
 // are "K-major", so one TMA tensor map (box 32 x 128, 128-byte swizzle)
-// serves every load.  One CTA computes one 256 x 256 tile of H as two
-// M = 128, N = 256 MMAs that share the B operand (two accumulators filling
-// all 512 TMEM columns), which halves the operand bytes per FLOP against a
-// single 128 x 256 tile.  Only tiles on or above the diagonal are launched;
-// a second kernel mirrors the upper triangle into the lower one.
+// serves every load.  A CTA computes a 256 x 256 tile of H (over one K
+// range at a time) as two M = 128, N = 256 MMAs that share the B operand
+// (two accumulators filling all 512 TMEM columns), which halves the operand
+// bytes per FLOP against a single 128 x 256 tile.  Only tiles on or above the
+// diagonal are computed; a second kernel mirrors the upper triangle into the
+// lower one.  One persistent CTA per SM claims (tile, K range) items in turn
+// (see gram_tf32_kernel), and rows longer than 1 MB are read from compact
+// copies of one 65536-column slab at a time (gram_run).
 //
 // Warp roles (192 threads): warp 0 = TMA producer (one lane), warp 1 = TMEM
 // allocator + MMA issuer (one lane), warps 2..5 = epilogue (each reads the
@@ -489,8 +492,8 @@ static int make_map(CUtensorMap* map, const void* J, int64_t M, int64_t K, int64
 extern "C" {
 
 // workspace: the error word, the item counter (byte 128), then one progress
-// counter per tile from byte 256 (up to
-// kGFlags tiles: M up to about 92,000 rows in one persistent launch)
+// counter per tile from byte 256, for up to kGFlags tiles (M up to about
+// 92,000 rows); larger M takes whole tiles as items, which needs no counters
 constexpr int64_t kGFlags = 65536;
 size_t rb_gram_work_bytes(void) { return 256 + (size_t)kGFlags * sizeof(int); }
 
