@@ -156,3 +156,21 @@ def test_coarse_space_host_rules():
     assert wb(2048, 32, 0, 0) < wb(2048, 128, 0, 0)
     ab = _lib.lib().rb_coarse_aggregate_work_bytes
     assert ab(0, 10) == 0 and ab(1000, 512) > 0
+
+
+def test_gram_staging_rule():
+    """rb_gram_stage_bytes (host arithmetic only): rows up to 1 MB are formed
+    in place (0 bytes); longer rows get one compact 65536-column slab of J
+    (and one of Jlo for the split form), plus 256 bytes of alignment slack."""
+    from redbirdpy_b200 import _lib
+
+    sb = _lib.lib().rb_gram_stage_bytes
+    M = 8192
+    assert sb(M, 135252, 135256, 4, 0) == 0              # 541 KB rows
+    assert sb(M, 262144, 262144, 4, 0) == 0              # exactly 1 MB
+    slab = M * 65536 * 4 + 256
+    assert sb(M, 1040502, 1040504, 4, 0) == slab         # 4 MB rows
+    assert sb(M, 1040502, 1040504, 4, 1) == 2 * (M * 65536 * 4) + 256
+    assert sb(M, 600001, 600008, 2, 0) == M * 65536 * 2 + 256  # BF16 rows of 1.2 MB
+    assert sb(M, 300001, 300008, 2, 0) == 0              # BF16 rows of 600 KB
+    assert sb(0, 1040502, 1040504, 4, 0) == 0 and sb(M, 1040502, 1040504, 3, 0) == 0
