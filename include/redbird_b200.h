@@ -204,6 +204,43 @@ int rb_coarse_aggregate(const double* node, int64_t nn, double x0, double y0, do
                         int32_t* agg_rows, int64_t* nc /* host */, void* work, size_t work_bytes,
                         void* stream);
 
+/* Spatial row groups of the blocked SpMM inside rb_femsolve (no counterpart
+ * in the reference, whose solves run in SuperLU): up to 8 rows per group, the
+ * nodes of one cube of edge about two node spacings, so that one warp gathers
+ * each x row of the group's column union once for all its rows.  Built once
+ * per mesh (rb_rowgroups_bin) and per CSR pattern (rb_rowgroups_union_*).
+ * Device arrays; coef is scratch that every rb_femsolve call using the groups
+ * overwrites (nu x 8 values of the solve's FP32 kind: 32 bytes per entry for
+ * real, 64 for complex), so solves sharing one rb_rowgroups must not overlap
+ * on the GPU. */
+typedef struct rb_rowgroups {
+  int64_t ng;             /* groups */
+  const int32_t* rows;    /* ng x 8 row indices, -1 pads a short group */
+  const int32_t* uptr;    /* ng + 1: each group's union entries */
+  const int32_t* ucol;    /* nu columns, ascending within a group */
+  const uint8_t* umask;   /* nu: bit r set when row r of the group holds the column */
+  int64_t nu;             /* union entries (uptr[ng]) */
+  void* coef;             /* nu x 8 scratch (see above) */
+} rb_rowgroups;
+
+/* Groups from node positions (node: nn x 3 FP64, device): node i falls in the
+ * cube floor((p - (x0, y0, z0)) / h), clamped to the nbx x nby x nbz grid;
+ * each cube's nodes, ascending, are cut into groups of 8 (the last one short).
+ * Groups follow the cubes in blocks of 2 x 2 x 2 cubes (x fastest inside a
+ * block and between blocks).  rows must hold 8 nn int32; *ng (host) receives
+ * the group count.  nbins = nbx nby nbz for the workspace query.
+ * Deterministic. */
+size_t rb_rowgroups_work_bytes(int64_t nn, int64_t nbins);
+int rb_rowgroups_bin(const double* node, int64_t nn, double x0, double y0, double z0, double h,
+                     int32_t nbx, int32_t nby, int32_t nbz, int32_t* rows, int64_t* ng /* host */,
+                     void* work, size_t work_bytes, void* stream);
+/* Column unions of the groups over A's pattern: count writes uptr (ng + 1)
+ * and *nu (host); fill writes ucol and umask (nu each). */
+size_t rb_rowgroups_union_work_bytes(int64_t ng);
+int rb_rowgroups_union_count(const rb_csr* A, const int32_t* rows, int64_t ng, int32_t* uptr,
+                             int64_t* nu /* host */, void* work, size_t work_bytes, void* stream);
+int rb_rowgroups_union_fill(const rb_csr* A, const int32_t* rows, int64_t ng, const int32_t* uptr,
+                            int32_t* ucol, uint8_t* umask, void* stream);
 typedef struct rb_solve_opts {
   int32_t precision;   /* RB_MIXED: FP32 Krylov + FP64 refinement; RB_FP64 */
   int32_t max_outer;   /* refinement sweeps (mixed) */
@@ -215,6 +252,7 @@ typedef struct rb_solve_opts {
   int32_t use_x0;      /* nonzero: X holds an initial guess (e.g. the previous
                           Gauss-Newton iterate's fields); zero: start from 0 */
   const rb_coarse* coarse; /* host pointer; NULL: Jacobi preconditioner only */
+  const rb_rowgroups* groups; /* host pointer; NULL: the SpMM walks rows (or row pairs) */
 } rb_solve_opts;
 
 typedef struct rb_solve_info {

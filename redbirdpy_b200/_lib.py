@@ -46,10 +46,15 @@ class RbCoarse(ctypes.Structure):
     _fields_ = [("nc", _i64), ("agg", _vp), ("agg_ptr", _vp), ("agg_rows", _vp)]
 
 
+class RbRowGroups(ctypes.Structure):
+    _fields_ = [("ng", _i64), ("rows", _vp), ("uptr", _vp), ("ucol", _vp), ("umask", _vp), ("nu", _i64),
+                ("coef", _vp)]
+
+
 class RbSolveOpts(ctypes.Structure):
     _fields_ = [("precision", _i32), ("max_outer", _i32), ("maxiter", _i32), ("check_every", _i32),
                 ("tol", _dbl), ("inner_tol", _dbl), ("profile", _i32), ("use_x0", _i32),
-                ("coarse", ctypes.POINTER(RbCoarse))]
+                ("coarse", ctypes.POINTER(RbCoarse)), ("groups", ctypes.POINTER(RbRowGroups))]
 
 
 class RbSolveInfo(ctypes.Structure):
@@ -82,6 +87,13 @@ _SIGS = {
     "rb_coarse_aggregate_work_bytes": (_sz, [_i64, _i64]),
     "rb_coarse_aggregate": (ctypes.c_int, [_vp, _i64, _dbl, _dbl, _dbl, _dbl, _i32, _i32, _i32, _vp, _vp, _vp,
                                            ctypes.POINTER(_i64), _vp, _sz, _vp]),
+    "rb_rowgroups_work_bytes": (_sz, [_i64, _i64]),
+    "rb_rowgroups_bin": (ctypes.c_int, [_vp, _i64, _dbl, _dbl, _dbl, _dbl, _i32, _i32, _i32, _vp,
+                                        ctypes.POINTER(_i64), _vp, _sz, _vp]),
+    "rb_rowgroups_union_work_bytes": (_sz, [_i64]),
+    "rb_rowgroups_union_count": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _i64, _vp, ctypes.POINTER(_i64), _vp,
+                                                _sz, _vp]),
+    "rb_rowgroups_union_fill": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _i64, _vp, _vp, _vp, _vp]),
     "rb_femsolve": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _vp, _i64, ctypes.POINTER(RbSolveOpts),
                                    ctypes.POINTER(RbSolveInfo), _vp, _sz, _vp]),
     "rb_csr_prepare": (ctypes.c_int, [ctypes.POINTER(RbCsr), _vp, _vp, _vp, _vp]),

@@ -1343,6 +1343,9 @@ static int64_t solve_cols(int64_t k) {
   return ceil_div(k, 4) * 4;
 }
 static bool shape_covers(const Shape& s, int64_t k) { return (int64_t)s.S * s.L * s.V >= k; }
+}  // namespace rb
+#include "rb_spmm_blk.cuh"
+namespace rb {
 
 // D[i][c] = S[i][c] for c < ks, 0 beyond (row-major, ld ks and kd)
 template <typename T>
@@ -1652,8 +1655,8 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
                        double* part_b, T* Xs, T* R, T* P, T* Q, ColState* cs, const int32_t* enable,
                        const OuterState* os, int32_t* counter, double tol, int maxiter, int check_every,
                        int* iters_out,
-                       int* launches, KernelTimer& tm, const GroupPlan* gp, const CoarseOp<T>* co,
-                       cudaStream_t st) {
+                       int* launches, KernelTimer& tm, const GroupPlan* gp, const RowGroupsDev* rg,
+                       const CoarseOp<T>* co, cudaStream_t st) {
   typedef typename Scalar<T>::acc Acc;
   const int64_t n = A.n;
   const unsigned fg = (unsigned)ceil_div(k, 8);
@@ -1692,7 +1695,13 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
       int32_t* next = slot[rd ^ 1];
       RB_TRY(tm.record(st));
       unsigned nb = shs.grid;
-      if (gp) {
+      if (rg) {
+        if constexpr (BlkOn<T>::value) {
+          RB_TRY((spmm_blk<T>(*rg, P, Q, part_a, k, &nb, st, live)));
+        } else {
+          return fail(RB_EARG, "blocked SpMM: unsupported scalar type");
+        }
+      } else if (gp) {
         if constexpr (PairCfg<T>::enabled) {
           RB_TRY((spmm_pair<T, EPI_PQDOT>(A, val, *gp, P, Q, part_a, k, &nb, st, live)));
         } else {
@@ -1789,7 +1798,7 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
 template <typename T64, typename T>
 static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, int64_t k, const rb_solve_opts& o,
                        rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv,
-                       const GroupPlan* gp, const CoarseOp<T>* co, cudaStream_t st) {
+                       const GroupPlan* gp, const RowGroupsDev* rg, const CoarseOp<T>* co, cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
   const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
@@ -1832,8 +1841,8 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     launches += 1;
     int it = 0;
     RB_TRY(inner_solve<T>(A, val, dinv, k, sh, shs, b.part_a, b.part_b, b.Xs, b.R, b.P, b.Q, b.cs, nullptr,
-                          b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, co,
-                          st));
+                          b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, rg,
+                          co, st));
     total_iters += it;
     if (it >= o.maxiter) sweep_flag = 1;
     correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, b.os, X);
@@ -1904,8 +1913,19 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     info.launches += 3 + 5 * (int)ceil_div(cb.op.nc, kGjB);
   }
   GroupPlan gp{nullptr, nullptr, nullptr, 0};
-  const bool plan = (GrpCfg<T>::enabled && grp_cols_ok(kb)) ||
-                    (PairCfg<T>::enabled && pair_cols_ok<T>(kb) && n * kb < (int64_t(1) << 31));
+  // spatial row groups (blocked SpMM) when the caller built them for this
+  // pattern and the column count fits; else the row-pair / row-group plans
+  RowGroupsDev rgd{0, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const rb_rowgroups* og = o.groups;
+  const bool use_rg = og && og->ng > 0 && og->rows && og->uptr && og->ucol && og->umask && og->coef &&
+                      blk_cols_ok<T>(n, kb);
+  if (use_rg) {
+    rgd = RowGroupsDev{og->ng, og->rows, og->uptr, og->ucol, og->umask, og->coef};
+    RB_TRY(rg_fill_coef<T>(A, val, rgd, st));
+    info.launches += 1;
+  }
+  const bool plan = !use_rg && ((GrpCfg<T>::enabled && grp_cols_ok(kb)) ||
+                                (PairCfg<T>::enabled && pair_cols_ok<T>(kb) && n * kb < (int64_t(1) << 31)));
   if (plan && n > 0)
     RB_TRY(build_group_plan<GrpCfg<T>::G>(A, b.gcnt, b.gptr, b.ucol, b.umask, b.scan_work, b.scan_bytes, &gp, st));
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * kb, 256), 148 * 16);
@@ -1918,7 +1938,7 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     }
   }
   RB_TRY((solve_block<T64, T>(A, Bp ? Bp : B, Xp ? Xp : X, kb, kb, o, info, b, val, dinv, gp.ng ? &gp : nullptr,
-                              o.coarse ? &cb.op : nullptr, st)));
+                              use_rg ? &rgd : nullptr, o.coarse ? &cb.op : nullptr, st)));
   if (Xp) {
     copy_cols_kernel<T64><<<eg, 256, 0, st>>>(n, kb, nrhs, Xp, X);
     RB_LAUNCH_CHECK();

@@ -47,6 +47,13 @@ class DeviceMesh:
         with np.errstate(invalid="ignore"):
             self.bbox = (np.nanmin(node[:, :3], axis=0), np.nanmax(node[:, :3], axis=0)) if self.nn else None
         self._coarse = {}
+        self._groups = None
+        self._edge = None
+        if self.ne:
+            sel = np.arange(0, self.ne, max(1, self.ne // 65536))
+            e = np.asarray(elem)[sel, :2].astype(np.int64) - 1
+            if e.min() >= 0 and e.max() < self.nn:
+                self._edge = float(np.median(np.linalg.norm(node[e[:, 1], :3] - node[e[:, 0], :3], axis=1)))
         self.elem = _i32(np.asarray(elem)[:, :4].astype(np.int64) - 1, dev)
         face = np.zeros((0, 3), np.int64) if face is None else np.asarray(face)
         self.nf = int(face.shape[0])
@@ -125,6 +132,15 @@ class DeviceMesh:
         if target not in self._coarse:
             self._coarse[target] = CoarseSpace(self, target)
         return self._coarse[target]
+
+    def row_groups(self):
+        """The RowGroups of the blocked SpMM (built once), or None when the
+        mesh has no usable edge length (e.g. a topology-only mesh)."""
+        if self._groups is None:
+            if not self._edge or not np.isfinite(self._edge) or self._edge <= 0:
+                return None
+            self._groups = RowGroups(self, self._edge)
+        return self._groups
 
     def deldotdel_host(self):
         return self.ddd.cpu().numpy()
@@ -459,6 +475,69 @@ class CoarseSpace:
         self.struct = _lib.RbCoarse(self.nc, self.agg.data_ptr(), self.agg_ptr.data_ptr(), self.agg_rows.data_ptr())
 
 
+class RowGroups:
+    """Spatial row groups of the blocked SpMM (``rb_rowgroups``): the nodes
+    binned into cubes of edge twice the typical edge length (the median length
+    of each tet's first edge), origin half an edge below the bounding box, so
+    that a structured grid falls into 2 x 2 x 2 blocks; each cube's nodes cut
+    into groups of 8; then the column union of every group over the mesh's CSR
+    pattern.  Built once per mesh on the device (rb_rowgroups_bin,
+    rb_rowgroups_union_*); ``coef`` is the per-solve coefficient scratch."""
+
+    def __init__(self, mesh, edge):
+        dev = mesh.device
+        nn = mesh.nn
+        lo, hi = mesh.bbox
+        if not (np.isfinite(edge) and edge > 0 and np.all(np.isfinite(lo)) and np.all(np.isfinite(hi))):
+            raise ValueError("row groups: degenerate mesh geometry")
+        h = 2.0 * edge
+        x0 = lo - 0.5 * edge
+        ext = np.maximum(hi - x0, 0.0)
+        nb = np.maximum(np.ceil(ext / h).astype(np.int64) + 1, 1)
+        while int(np.prod(nb)) > (1 << 26):
+            h *= 1.25
+            nb = np.maximum(np.ceil(ext / h).astype(np.int64) + 1, 1)
+        self.rows = torch.empty(8 * nn, dtype=torch.int32, device=dev)
+        ng = ctypes.c_int64(0)
+        wb = _lib.lib().rb_rowgroups_work_bytes(nn, int(np.prod(nb)))
+        work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        call("rb_rowgroups_bin", ptr(mesh.node), nn, float(x0[0]), float(x0[1]), float(x0[2]), h, int(nb[0]),
+             int(nb[1]), int(nb[2]), ptr(self.rows), ctypes.byref(ng), ptr(work), wb, stream())
+        self.ng = int(ng.value)
+        csr = _lib.RbCsr(nn, mesh.nnz, mesh.indptr.data_ptr(), mesh.indices.data_ptr(), None, None, None, None, 0)
+        self.uptr = torch.empty(self.ng + 1, dtype=torch.int32, device=dev)
+        wb = _lib.lib().rb_rowgroups_union_work_bytes(self.ng)
+        work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        nu = ctypes.c_int64(0)
+        call("rb_rowgroups_union_count", ctypes.byref(csr), ptr(self.rows), self.ng, ptr(self.uptr),
+             ctypes.byref(nu), ptr(work), wb, stream())
+        self.nu = int(nu.value)
+        self.ucol = torch.empty(max(self.nu, 1), dtype=torch.int32, device=dev)
+        self.umask = torch.empty(max(self.nu, 1), dtype=torch.uint8, device=dev)
+        call("rb_rowgroups_union_fill", ctypes.byref(csr), ptr(self.rows), self.ng, ptr(self.uptr), ptr(self.ucol),
+             ptr(self.umask), stream())
+        # coefficient scratch: 8 FP32 values per union entry (real solves)
+        self.coef = torch.empty(max(self.nu, 1) * 8, dtype=torch.float32, device=dev)
+        self.h = h
+        self.struct = _lib.RbRowGroups(self.ng, self.rows.data_ptr(), self.uptr.data_ptr(), self.ucol.data_ptr(),
+                                       self.umask.data_ptr(), self.nu, self.coef.data_ptr())
+
+
+def _resolve_groups(mat, groups):
+    """RowGroups for solve(groups=...): 'auto' (real matrices assembled on a
+    DeviceMesh), a RowGroups, or None/False for the per-row SpMM kernels."""
+    if groups is None or groups is False:
+        return None
+    if isinstance(groups, RowGroups):
+        return groups
+    mesh = getattr(mat, "mesh", None)
+    if groups == "auto":
+        if mat.is_complex or not hasattr(mesh, "row_groups"):
+            return None
+        return mesh.row_groups()
+    raise ValueError(f"groups: unsupported value {groups!r}")
+
+
 def _resolve_coarse(mat, coarse):
     """CoarseSpace for solve(coarse=...): 'auto' (meshes of at least
     COARSE_MIN_NODES nodes), True, an aggregate count, a CoarseSpace, or
@@ -482,7 +561,7 @@ def _resolve_coarse(mat, coarse):
 
 
 def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=2000, max_outer=10,
-          check_every=10, profile=False, x0=None, coarse="auto"):
+          check_every=10, profile=False, x0=None, coarse="auto", groups="auto"):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
     Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
@@ -513,9 +592,11 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
         inner_tol = 1e-5 if cs is not None else 1e-4
     if prec == _lib.RB_FP64 and inner_tol > 1e-6:
         inner_tol = max(tol, 1e-15)
+    rg = _resolve_groups(mat, groups) if prec == _lib.RB_MIXED else None
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
                             int(bool(profile)), int(x0 is not None),
-                            ctypes.pointer(cs.struct) if cs is not None else None)
+                            ctypes.pointer(cs.struct) if cs is not None else None,
+                            ctypes.pointer(rg.struct) if rg is not None else None)
     for c0 in range(0, k, 128):
         kb = min(128, k - c0)
         Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
