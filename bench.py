@@ -389,8 +389,9 @@ def run_gn_step(cfg, mesh, world, args):
         prop[:, 1] = 1.0 / (3.0 * (d_old + dmu[nn:2 * nn])) - prop[:, 0]
 
     state = {"phi": None}
+    refine = 3  # FP64 refinement sweeps of the normal equations (at most)
 
-    def step_mixed(jdtype=torch.float32, apply=True):
+    def step_mixed(jdtype=torch.float32, apply=True, gram_prec="tf32"):
         # one iteration of the GN loop: the forward solve starts from the
         # previous iterate's fields, and the update is applied at the end
         det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg, x0=state["phi"]))
@@ -400,7 +401,7 @@ def run_gn_step(cfg, mesh, world, args):
         mis = data - y
         mis = np.concatenate([mis.real, mis.imag])
         s2 = timed_stage("sumsq", lambda: 1.0 / float(engine.sumsq(J, K).item()))
-        H, _ = timed_stage("gram", lambda: engine.gram(J, K, s2, "tf32"))
+        H, _ = timed_stage("gram", lambda: engine.gram(J, K, s2, gram_prec))
         lam = 0.05 * float(H.diagonal().max().item())
         M = J.shape[0]
         di = torch.empty(M, dtype=torch.float64, device=J.device)
@@ -412,17 +413,12 @@ def run_gn_step(cfg, mesh, world, args):
             engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), wb, engine.stream())
 
         timed_stage("cholesky", chol)
-
-        def solve_apply():
-            r = torch.as_tensor(mis, device=J.device)
-            t = torch.empty(M, dtype=torch.float64, device=J.device)
-            engine.call("rb_vec_mul", engine.ptr(di), engine.ptr(r), engine.ptr(t), M, engine.stream())
-            engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.stream())
-            yv = torch.empty(M, dtype=torch.float64, device=J.device)
-            engine.call("rb_vec_mul", engine.ptr(di), engine.ptr(t), engine.ptr(yv), M, engine.stream())
-            return engine.gemv_t(J, K, yv, s2).cpu().numpy()
-
-        dmu = timed_stage("solve_jty", solve_apply)
+        # solve with FP64 refinement over the stored J, then J^T y
+        rinfo = {}
+        dmu = timed_stage("solve_refine_jty", lambda: engine.normal_solve(
+            J, K, H, di, mis, lam, s2, None, refine=refine, info=rinfo).cpu().numpy())
+        state["refine"] = rinfo
+        state["det"] = det
         del J, H
         if apply:
             apply_update(gcfg["prop"], dmu)
@@ -451,6 +447,7 @@ def run_gn_step(cfg, mesh, world, args):
     def step_fp64():
         gcfg["prop"] = snap[0].copy()
         det, phi, _, _, _ = forward_device(gcfg, precision="fp64", x0=snap[1])
+        state["det64"] = det.cpu().numpy()
         cols, det0, ndet, psrc, pdet, _, _ = engine.pair_map(sd)
         nn = mesh.nn
         K = 2 * nn
@@ -478,8 +475,11 @@ def run_gn_step(cfg, mesh, world, args):
         dmu = torch.mv(J.T, di * t) * s2
         return dmu.cpu().numpy()
 
+    refine_info = dict(state.get("refine", {}))
+    det_mixed = state["det"].cpu().numpy()
     ms64 = None
     err = None
+    det_err = None
     if not args.no_fp64_gn:
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -489,6 +489,7 @@ def run_gn_step(cfg, mesh, world, args):
         torch.cuda.synchronize()
         ms64 = max_over_ranks(f0.elapsed_time(f1), world)
         err = float(np.linalg.norm(dmu_mixed - dmu64) / np.linalg.norm(dmu64))
+        det_err = float(np.max(np.abs(det_mixed - state["det64"]) / np.abs(state["det64"])))
     M, K = 8192, 2 * mesh.nn
     nbt = (M + 255) // 256
     tiles = nbt * (nbt + 1) // 2  # 256 x 256 tiles on or above the diagonal
@@ -496,7 +497,7 @@ def run_gn_step(cfg, mesh, world, args):
     gram_ms = mixed_stages.get("gram")
     # the BF16 form of the same iteration (Jacobian rows rounded to BF16, the
     # kind::f16 MMA): same state as the FP64 comparison
-    bf16 = None
+    bf16 = tf32x3 = None
     if not args.no_fp64_gn:
         gcfg["prop"] = snap[0].copy()
         state["phi"] = snap[1]
@@ -512,7 +513,20 @@ def run_gn_step(cfg, mesh, world, args):
         bf16 = {"ms_per_iter": round(bms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
                 "speedup_vs_fp64": round(ms64 / bms, 3), "iters_per_s": round(1e3 / bms, 4) * world,
                 "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_b - dmu64) / np.linalg.norm(dmu64)),
-                "gram_tflops": round(tiles_flop(mesh) / (stages["gram"] * 1e-3) / 1e12, 1)}
+                "gram_tflops": round(tiles_flop(mesh) / (stages["gram"] * 1e-3) / 1e12, 1),
+                "note": "BF16 Jacobian rows: the refinement converges to the BF16-rounded J's system"}
+        # split-TF32 J J^T (three products, hi/lo), same state
+        step_mixed(apply=False, gram_prec="tf32x3")
+        torch.cuda.synchronize()
+        stages.clear()
+        b0.record()
+        dmu_x3 = step_mixed(apply=False, gram_prec="tf32x3")
+        b1.record()
+        torch.cuda.synchronize()
+        x3ms = max_over_ranks(b0.elapsed_time(b1), world)
+        tf32x3 = {"ms_per_iter": round(x3ms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
+                  "speedup_vs_fp64": round(ms64 / x3ms, 3),
+                  "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_x3 - dmu64) / np.linalg.norm(dmu64))}
     tflops = gram_flop / (gram_ms * 1e-3) / 1e12 if gram_ms else None
     pk, pk_src = 1590.0, "fallback bf16 (burst), no MEASURED_PEAKS.json"
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -522,13 +536,16 @@ def run_gn_step(cfg, mesh, world, args):
             pk, pk_src = float(v), "measured bf16 (burst)"
     return {
         "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
-                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, TF32 J J^T; GN iterations 2..{ks + 1} of the loop (forward warm-started "
+                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, TF32 J J^T + FP64 refinement of the normal "
+                    f"equations; GN iterations 2..{ks + 1} of the loop (forward warm-started "
                     f"from the previous iterate's fields), iteration 1 untimed",
         "iters_per_s": round(1e3 / ms, 4) * world, "ms_per_iter": round(ms, 1), "breakdown_ms": mixed_stages,
         "fp64_iters_per_s": round(1e3 / ms64, 4) * world if ms64 else None,
         "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,
         "speedup_vs_fp64": round(ms64 / ms, 3) if ms64 else None,
         "dmu_rel_err_vs_fp64": err,
+        "forward_det_max_rel_err_vs_fp64": det_err,
+        "refinement": refine_info,
         "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel (tcgen05 kind::tf32, FP32 accumulation "
                                                        "drained to FP64, 256x256 tiles)",
                           "achieved": round(tflops, 1) if tflops else None, "unit": "TFLOP/s",
@@ -536,6 +553,7 @@ def run_gn_step(cfg, mesh, world, args):
                           "frac_of_bf16": round(tflops / pk, 4) if (tflops and pk) else None,
                           "note": "TF32 dense peak is half the BF16 one"},
         "bf16_form": bf16,
+        "tf32x3_form": tf32x3,
     }
 
 

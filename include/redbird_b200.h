@@ -134,6 +134,29 @@ int rb_femlhs_noalloc(const rb_mesh* mesh, const rb_optics* optics, const double
                       const double* ddd, void* val64, void* val32, void* dinv64, void* dinv32,
                       void* stream);
 
+/* meshprep on the device (redbirdpy/utility.py:101-246 with the reference's
+ * fallbacks, utility.py:1005-1109), all index arrays 0-based int32:
+ *   rb_reorient    swap nodes 0 and 1 of tets of negative signed volume, in
+ *                  place (elem ne x 4, 16-byte aligned); evol (optional)
+ *                  receives |V|; flipped (optional, device) counts the swaps
+ *   rb_volface     boundary triangles (each tet's faces (0,2,1), (0,1,3),
+ *                  (0,3,2), (1,2,3); those whose sorted node triple occurs
+ *                  once), in the order of their sorted triples, each with its
+ *                  tet's orientation; face holds 4 ne x 3 int32, *nf (host)
+ *                  the count; nn < 2^21
+ *   rb_face_area   triangle areas
+ *   rb_nodevolume  nvol[n] = 1/4 sum of evol over the tets of node n
+ *                  (incidence lists of rb_incidence)
+ * The arithmetic follows numpy's order without fused multiply-adds: the
+ * results carry the bits of the host fallbacks. */
+int rb_reorient(const double* node, int32_t* elem, int64_t ne, double* evol, int32_t* flipped, void* stream);
+size_t rb_volface_work_bytes(int64_t ne);
+int rb_volface(const int32_t* elem, int64_t ne, int64_t nn, int32_t* face, int64_t* nf /* host */, void* work,
+               size_t work_bytes, void* stream);
+int rb_face_area(const double* node, const int32_t* face, int64_t nf, double* area, void* stream);
+int rb_nodevolume(int64_t nn, const int32_t* node_eptr, const int32_t* node_elist, const double* evol,
+                  double* nvol, void* stream);
+
 /* deldotdel (redbirdpy/utility.py:53-98): ne x 10 values V*grad(phi_i).grad(phi_j)
  * for the pairs (0,0),(0,1),(0,2),(0,3),(1,1),(1,2),(1,3),(2,2),(2,3),(3,3),
  * from the node coordinates; evol (optional, ne) receives |V| like
@@ -154,6 +177,19 @@ int rb_tsearch(const double* node, const int32_t* elem, int64_t ne, const double
  * elem[loc[k]][m], column col0 + k; optodes with loc < 0 leave a zero column. */
 int rb_point_rhs(const int32_t* elem, const int32_t* loc, const double* bary, int64_t npts,
                  int64_t nn, int64_t ld, int64_t col0, double* B, void* stream);
+
+/* Wide-field (pattern) sources and detectors: the dense columns of
+ * cfg['widesrc'] / cfg['widedet'] (W: nn x w, row stride ldw; femrhs,
+ * redbirdpy/forward.py:326-352, where they follow the point columns of their
+ * kind).  rb_wide_rhs copies them into B (nn x ld) at column col0;
+ * rb_wide_getdet forms their detector rows (femgetdet, forward.py:430-442):
+ * detval[d * nsrc + s] = sum_n W[n][d] phi[n * ld + s] for d < wd, phi and
+ * detval of scalar kind `kind` (RB_F64 or RB_C128), deterministic. */
+int rb_wide_rhs(const double* W, int64_t nn, int64_t w, int64_t ldw, int64_t ld, int64_t col0, double* B,
+                void* stream);
+size_t rb_wide_getdet_work_bytes(int64_t wd, int64_t nsrc, int32_t kind);
+int rb_wide_getdet(const double* W, int64_t nn, int64_t wd, int64_t ldw, const void* phi, int64_t ld,
+                   int64_t nsrc, int32_t kind, void* detval, void* work, size_t work_bytes, void* stream);
 
 /* femgetdet (redbirdpy/forward.py:365-442) for point detectors:
  * detval[d * nsrc + s] = sum_m bary_det[d][m] * phi[elem[loc_det[d]][m] * ld + s]
@@ -324,6 +360,27 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
            int32_t rmax, int32_t emax, const double* evol, const double* ddd, void* stream);
 
+/* Dual-mesh Jacobian remap (_remap_jacobian, redbirdpy/recon.py:818-876):
+ * out[r][q] = sum_{p in [map_ptr[q], map_ptr[q+1])} map_w[p] J[r][map_idx[p]]
+ * for rows r < rows and reconstruction nodes q < nq; map_idx lists the
+ * forward nodes whose enclosing reconstruction element has node q (map_w:
+ * that node's barycentric weight), ascending.  J and out of kind `kind`
+ * (RB_F32, RB_C64, RB_F64 or RB_C128), row strides ldj and ldo. */
+int rb_jac_remap(const void* J, int32_t kind, int64_t rows, int64_t ldj, const int32_t* map_ptr,
+                 const int32_t* map_idx, const double* map_w, int64_t nq, void* out, int64_t ldo,
+                 void* stream);
+/* One wavelength's Jacobian rows into the stacked real GN matrix (FP32 rows,
+ * ldd): with v = src[r][c] (scale_re + i scale_im) rowscale[r] (rowscale:
+ * optional complex per-row factors, re/im pairs), dst[row_re + r][col0 + c]
+ * = Re v and, when row_im >= 0, dst[row_im + r][col0 + c] = Im v.  Covers
+ * jacchrome's extinction weights (redbirdpy/forward.py:572-589) and
+ * matreform's forms (recon.py:512-567): 'real' stacking, 'reim' (second
+ * column block with the factor i), 'logphase' (rowscale conj(y)/|y|^2).
+ * src RB_F32 or RB_C64, row stride lds. */
+int rb_jac_block(const void* src, int32_t kind, int64_t rows, int64_t cols, int64_t lds, double scale_re,
+                 double scale_im, const double* rowscale, float* dst, int64_t ldd, int64_t row_re,
+                 int64_t row_im, int64_t col0, void* stream);
+
 /* Element Jacobian Je (nsd x ne, kind of phi: RB_F64 or RB_C128), the second
  * output of jac (forward.py:527-557); src_col/det_col are phi columns. */
 int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,
@@ -395,6 +452,23 @@ int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, voi
 int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
                   size_t work_bytes, void* stream);
 int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream);
+/* FP64 iterative refinement of the normal equations (alpha J J^T + lambda I) y = r
+ * around the tensor-core factor (the refinement residual r - alpha J (J^T y)
+ * - lambda y takes FP64-accumulated products over the stored J, so y reaches
+ * the accuracy of J itself; no counterpart in the reference, which solves the
+ * FP64 normal matrix directly, recon.py:474-483):
+ *   out = alpha J x + beta out     rb_gemv_n (J as for rb_gemv_t, rows padded to
+ *                                  a multiple of 4 entries; x FP64, K entries)
+ *   y = a x + b y                  rb_axpby
+ *   x . y                          rb_dot (the residual norms) */
+int rb_gemv_n(const float* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
+              double* out, void* stream);
+int rb_gemv_n_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
+                   double* out, void* stream);
+int rb_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
+/* *out = x . y (FP64, device scalar; fixed-order reduction) */
+size_t rb_dot_work_bytes(void);
+int rb_dot(int64_t n, const double* x, const double* y, double* out, void* work, size_t work_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -113,11 +113,18 @@ def getbulk(cfg):
     return default
 
 
+def _nwide(cfg, key):
+    w = cfg.get(key)
+    return np.asarray(w).reshape(np.shape(w)[0], -1).shape[1] if w is not None and np.size(w) else 0
+
+
 def sdmap(cfg):
-    """Single-wavelength source/detector pair table (utility.py:675-796)."""
+    """Single-wavelength source/detector pair table (utility.py:675-796):
+    columns [point src | wide src | point det | wide det], detector-major."""
     ns = np.atleast_2d(cfg["srcpos"]).shape[0]
     nd = np.atleast_2d(cfg["detpos"]).shape[0]
-    ss, dd = np.meshgrid(np.arange(ns), ns + np.arange(nd))
+    ws, wd = _nwide(cfg, "widesrc"), _nwide(cfg, "widedet")
+    ss, dd = np.meshgrid(np.arange(ns + ws), ns + ws + np.arange(nd + wd))
     sd = np.column_stack([ss.ravel(), dd.ravel()])
     return np.column_stack([sd, np.ones(len(sd))])
 
@@ -279,24 +286,40 @@ def getoptodes(cfg):
 
 
 def femrhs(cfg):
-    """Point-optode right-hand sides [src | det] (forward.py:259-362)."""
+    """Right-hand sides (forward.py:259-362), columns [point src | wide src |
+    point det | wide det]: 4 barycentric weights per located point optode,
+    the cfg['widesrc'] / cfg['widedet'] pattern columns as given; loc / bary
+    NaN for wide-field columns."""
     src, det = getoptodes(cfg)
     nn = cfg["node"].shape[0]
     e0 = cfg["elem"][:, :4].astype(np.int64) - 1
+    ns, nd = src.shape[0], det.shape[0]
+    ws, wd = _nwide(cfg, "widesrc"), _nwide(cfg, "widedet")
+    ncol = ns + ws + nd + wd
     pts = np.vstack([src, det])
-    loc, bary = tsearchn(cfg["node"], cfg["elem"][:, :4], pts[:, :3])
+    ploc, pbary = tsearchn(cfg["node"], cfg["elem"][:, :4], pts[:, :3])
+    pcol = np.r_[np.arange(ns), ns + ws + np.arange(nd)]
+    loc = np.full(ncol, np.nan)
+    bary = np.full((ncol, 4), np.nan)
+    loc[pcol], bary[pcol] = ploc, pbary
     rows, cols, vals = [], [], []
-    for k in range(pts.shape[0]):
-        if not np.isnan(loc[k]):
-            rows += list(e0[int(loc[k]) - 1]); cols += [k] * 4; vals += list(bary[k])
-    rhs = sparse.csr_matrix((vals, (rows, cols)), shape=(nn, pts.shape[0]))
+    for k, c in enumerate(pcol):
+        if not np.isnan(ploc[k]):
+            rows += list(e0[int(ploc[k]) - 1]); cols += [c] * 4; vals += list(pbary[k])
+    for key, c0, w in (("widesrc", ns, ws), ("widedet", ns + ws + nd, wd)):
+        if w:
+            W = np.asarray(cfg[key], dtype=np.float64).reshape(nn, -1)
+            r, c = np.nonzero(W)
+            rows += list(r); cols += list(c + c0); vals += list(W[r, c])
+    rhs = sparse.csr_matrix((vals, (rows, cols)), shape=(nn, ncol))
     return rhs, loc, bary, pts
 
 
 def femgetdet(phi, cfg, rhs):
-    """detval = rhs[:, det]^T phi[:, src] (forward.py:365-442)."""
-    ns = np.atleast_2d(cfg["srcpos"]).shape[0]
-    nd = np.atleast_2d(cfg["detpos"]).shape[0]
+    """detval = rhs[:, det]^T phi[:, src] over point and wide-field columns
+    (forward.py:365-442)."""
+    ns = np.atleast_2d(cfg["srcpos"]).shape[0] + _nwide(cfg, "widesrc")
+    nd = np.atleast_2d(cfg["detpos"]).shape[0] + _nwide(cfg, "widedet")
     rdet = rhs[:, ns:ns + nd]
     rdet = rdet.toarray() if sparse.issparse(rdet) else rdet
     return rdet.T @ phi[:, :ns]

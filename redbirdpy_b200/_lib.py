@@ -77,11 +77,19 @@ _SIGS = {
     "rb_femlhs_noalloc": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp,
                                          _vp, _vp]),
     "rb_deldotdel": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "rb_reorient": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "rb_volface_work_bytes": (_sz, [_i64]),
+    "rb_volface": (ctypes.c_int, [_vp, _i64, _i64, _vp, ctypes.POINTER(_i64), _vp, _sz, _vp]),
+    "rb_face_area": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "rb_nodevolume": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _vp]),
     "rb_tsearch": (ctypes.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "rb_point_rhs": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),
     "rb_prop_from_labels": (ctypes.c_int, [_vp, _i64, _vp, _i64, _i32, _vp, _vp, _vp]),
     "rb_adjoint_fields": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _vp, _vp]),
     "rb_femgetdet": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _i64, _i64, _i32, _vp, _vp]),
+    "rb_wide_rhs": (ctypes.c_int, [_vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp]),
+    "rb_wide_getdet_work_bytes": (_sz, [_i64, _i64, _i32]),
+    "rb_wide_getdet": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _vp, _sz, _vp]),
     "rb_femsolve_work_bytes": (_sz, [_i64, _i64, _i64, _i32, _i32]),
     "rb_coarse_work_bytes": (_sz, [_i64, _i64, _i32, _i32]),
     "rb_coarse_aggregate_work_bytes": (_sz, [_i64, _i64]),
@@ -100,6 +108,8 @@ _SIGS = {
     "rb_spmm": (ctypes.c_int, [ctypes.POINTER(RbCsr), _i32, _vp, _vp, _i64, _vp]),
     "rb_jac": (ctypes.c_int, [ctypes.POINTER(RbMesh), _i32, _vp, _i32, _i64, _vp, _i32, _i32, _i32, _vp, _vp,
                               _i64, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
+    "rb_jac_remap": (ctypes.c_int, [_vp, _i32, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp]),
+    "rb_jac_block": (ctypes.c_int, [_vp, _i32, _i64, _i64, _i64, _dbl, _dbl, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "rb_jac_elem": (ctypes.c_int, [ctypes.POINTER(RbMesh), _vp, _vp, _i32, _i64, _vp, _vp, _i64, _vp, _vp]),
     "rb_gram_work_bytes": (_sz, []),
     "rb_gram": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _dbl, _vp, _i64, _vp, _sz, _vp]),
@@ -119,6 +129,11 @@ _SIGS = {
     "rb_sumsq": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "rb_sumsq_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "rb_vec_mul": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp]),
+    "rb_gemv_n": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
+    "rb_gemv_n_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
+    "rb_axpby": (ctypes.c_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
+    "rb_dot_work_bytes": (_sz, []),
+    "rb_dot": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _sz, _vp]),
 }
 
 _lib = None

@@ -238,6 +238,8 @@ extern "C" int rb_femlhs(const rb_mesh* mesh, const rb_optics* optics, const dou
   if (!o.mua || !o.musp) return fail(RB_EARG, "rb_femlhs: mua and musp are required");
   if (o.kind != RB_PROP_NODE && o.kind != RB_PROP_ELEM) return fail(RB_EARG, "rb_femlhs: bad property kind");
   if (!(o.omega >= 0.0)) return fail(RB_EARG, "rb_femlhs: omega must be >= 0");
+  if (m.nn < 1 || (o.kind == RB_PROP_NODE ? m.nn : m.ne) < 1)
+    return fail(RB_EARG, "rb_femlhs: empty mesh (%lld nodes, %lld tets)", (long long)m.nn, (long long)m.ne);
   if (work_bytes < rb_femlhs_work_bytes(m.nn, m.ne)) return fail(RB_EARG, "rb_femlhs: workspace too small");
   cudaStream_t st = as_stream(stream);
   double* dco = reinterpret_cast<double*>(work);
@@ -306,7 +308,9 @@ extern "C" int rb_femlhs_noalloc(const rb_mesh* mesh, const rb_optics* optics, c
   const rb_optics& o = *optics;
   if (o.kind != RB_PROP_NODE && o.kind != RB_PROP_ELEM) return fail(RB_EARG, "rb_femlhs_noalloc: bad property kind");
   const int64_t np = (o.kind == RB_PROP_NODE) ? m.nn : m.ne;
-  if (np < 0 || np > kNoallocScratchMax)
+  if (m.nn < 1 || np < 1)
+    return fail(RB_EARG, "rb_femlhs_noalloc: empty mesh (%lld nodes, %lld tets)", (long long)m.nn, (long long)m.ne);
+  if (np > kNoallocScratchMax)
     return fail(RB_ESIZE,
                 "rb_femlhs_noalloc: %lld %s exceed the fixed scratch of %lld entries; use rb_femlhs with a workspace",
                 (long long)np, o.kind == RB_PROP_NODE ? "nodes" : "tets", (long long)kNoallocScratchMax);

@@ -394,6 +394,72 @@ __global__ void gemv_t_sum_kernel(const double* __restrict__ part, int slabs, in
   out[k] = alpha * s + (beta != 0.0 ? beta * out[k] : 0.0);
 }
 
+// out[m] = alpha sum_k J[m][k] x[k] + beta out[m] for 4 rows per block: the
+// FP32 (or BF16) rows stream from DRAM once, x (FP64) from L2 once per 4 rows;
+// each thread keeps 4 partial sums per row (k chunks of 4), then a fixed-order
+// block reduction: the result is the same bits on every run.
+constexpr int kGemvNRows = 4;
+template <typename JT>
+__global__ void __launch_bounds__(256) gemv_n_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+                                                     const double* __restrict__ x, double alpha, double beta,
+                                                     double* __restrict__ out) {
+  __shared__ double red[kGemvNRows][8];
+  const int64_t m0 = (int64_t)blockIdx.x * kGemvNRows;
+  double s[kGemvNRows];
+#pragma unroll
+  for (int r = 0; r < kGemvNRows; ++r) s[r] = 0.0;
+  for (int64_t k = 4 * (int64_t)threadIdx.x; k < K; k += 4 * (int64_t)blockDim.x) {
+    double xv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) xv[j] = (k + j < K) ? x[k + j] : 0.0;
+#pragma unroll
+    for (int r = 0; r < kGemvNRows; ++r) {
+      if (m0 + r < M) {
+        double v[4];
+        ld4(J + (m0 + r) * ldj + k, v);  // padded row: entries past K are read, then skipped
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (k + j < K) s[r] = fma(v[j], xv[j], s[r]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < kGemvNRows; ++r) {
+    const double t = warp_sum(s[r]);
+    if (lane == 0) red[r][w] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < kGemvNRows && m0 + threadIdx.x < M) {
+    double t = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[threadIdx.x][q];
+    const int64_t m = m0 + threadIdx.x;
+    out[m] = alpha * t + (beta != 0.0 ? beta * out[m] : 0.0);
+  }
+}
+
+// per-block partial sums of x . y (FP64), fixed order
+__global__ void dot_part_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                double* __restrict__ part) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s = fma(x[i], y[i], s);
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+  }
+}
+
+__global__ void axpby_kernel(int64_t n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i] + (b != 0.0 ? b * y[i] : 0.0);
+}
+
 // per-block partial sums of J^2
 template <typename JT>
 __global__ void sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
@@ -537,8 +603,53 @@ static int gemv_t_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const doub
   return RB_OK;
 }
 
+template <typename JT>
+static int gemv_n_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
+                      double* out, void* stream) {
+  if (!J || !x || !out || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_n: bad arguments");
+  if ((reinterpret_cast<uintptr_t>(J) & (4 * sizeof(JT) - 1)) || (ldj % 4) || ldj < ceil_div(K, 4) * 4)
+    return fail(RB_EARG, "rb_gemv_n: J rows must start on %d-byte boundaries and hold K rounded up to 4 entries",
+                (int)(4 * sizeof(JT)));
+  gemv_n_kernel<JT><<<(unsigned)ceil_div(M, kGemvNRows), 256, 0, as_stream(stream)>>>(J, M, K, ldj, x, alpha, beta,
+                                                                                       out);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
 extern "C" {
 
+int rb_gemv_n(const float* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
+              double* out, void* stream) {
+  return gemv_n_run(J, M, K, ldj, x, alpha, beta, out, stream);
+}
+
+int rb_gemv_n_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
+                   double* out, void* stream) {
+  return gemv_n_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, x, alpha, beta, out, stream);
+}
+
+size_t rb_dot_work_bytes(void) { return 64 * sizeof(double) + 256; }
+
+int rb_dot(int64_t n, const double* x, const double* y, double* out, void* work, size_t work_bytes, void* stream) {
+  if (!x || !y || !out || !work || n < 1) return fail(RB_EARG, "rb_dot: bad arguments");
+  if (work_bytes < rb_dot_work_bytes()) return fail(RB_EARG, "rb_dot: workspace too small");
+  cudaStream_t st = as_stream(stream);
+  const int blocks = (int)std::min<int64_t>(64, ceil_div(n, 256));
+  double* part = reinterpret_cast<double*>(work);
+  dot_part_kernel<<<blocks, 256, 0, st>>>(n, x, y, part);
+  RB_LAUNCH_CHECK();
+  sum_parts_kernel<<<1, 64, 0, st>>>(part, blocks, out);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
+
+int rb_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream) {
+  if (!x || !y || n < 0) return fail(RB_EARG, "rb_axpby: bad arguments");
+  if (n == 0) return RB_OK;
+  axpby_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, as_stream(stream)>>>(n, a, x, b, y);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
+}
 
 int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha, double beta,
               double* out, void* work, size_t work_bytes, void* stream) {

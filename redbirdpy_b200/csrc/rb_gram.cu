@@ -351,9 +351,10 @@ gram_tf32_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         if (lane == 0) {
           const int want = 4 * (int)s;
           long long i = 0;
-          while (ld_acquire(done + t) < want && ++i < kGWaitLimit) __nanosleep(64);
-          seen = i < kGWaitLimit;
-          if (!seen) atomicExch(err, 7);
+          // stop at once when another role has already failed (its error code stays)
+          while (ld_acquire(done + t) < want && !aborted(err) && ++i < kGWaitLimit) __nanosleep(64);
+          seen = ld_acquire(done + t) >= want;
+          if (!seen && i >= kGWaitLimit) atomicExch(err, 7);
         }
         if (!__shfl_sync(0xffffffffu, (int)seen, 0)) break;
         (void)ld_acquire(done + t);  // every lane orders its reads of H after the flag

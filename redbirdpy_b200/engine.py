@@ -12,6 +12,7 @@ here computes on the CPU; every numerical step is a call into
 
 import ctypes
 import weakref
+import zlib
 
 import numpy as np
 import torch
@@ -120,10 +121,13 @@ class DeviceMesh:
         return self._evol
 
     def labels(self, seg):
-        """Device int32 copy of a per-tet label array, cached per array."""
-        key = (id(seg), np.shape(seg))
+        """Device int32 copy of a per-tet label array, cached by content (a
+        CRC of its bytes: an array edited in place, or a new array that takes
+        a freed one's id, is uploaded again)."""
+        a = np.ascontiguousarray(seg)
+        key = (a.shape, a.dtype.str, zlib.crc32(memoryview(a).cast("B")))
         if self._labels[0] != key:
-            self._labels = (key, _i32(np.asarray(seg).ravel(), self.device))
+            self._labels = (key, _i32(a.ravel(), self.device))
         return self._labels[1]
 
     def coarse_space(self, target):
@@ -166,28 +170,50 @@ class DeviceMesh:
 def topology_of(elem, nn):
     """A DeviceMesh built from connectivity alone (coordinates zero), enough
     for the Jacobian kernels, which take volumes and deldotdel explicitly.
-    Cached per elem array."""
-    key = (id(elem), np.shape(elem), int(nn))
-    hit = _TOPO.get("key")
-    if hit == key:
+    Cached by content (shape and a CRC of elem's bytes)."""
+    a = np.ascontiguousarray(elem)
+    key = (a.shape, a.dtype.str, zlib.crc32(memoryview(a).cast("B")), int(nn))
+    if _TOPO.get("key") == key:
         return _TOPO["mesh"]
-    m = DeviceMesh(np.zeros((nn, 3)), elem, None, None, evol=np.zeros(elem.shape[0]))
-    _TOPO.update(key=key, mesh=m, ref=elem)
+    m = DeviceMesh(np.zeros((nn, 3)), a, None, None, evol=np.zeros(a.shape[0]))
+    _TOPO.update(key=key, mesh=m)
     return m
 
 
 _TOPO = {}
 
 
+def _same_arrays(refs, arrays):
+    """True when every weak reference still points at the very same object."""
+    return len(refs) == len(arrays) and all(
+        (r is None and a is None) or (r is not None and r() is a) for r, a in zip(refs, arrays))
+
+
+def _weak(a):
+    if a is None:
+        return None
+    try:
+        return weakref.ref(a)
+    except TypeError:  # a list or other non-referenceable container: never reused
+        return lambda: object()
+
+
 def mesh_of(cfg):
-    """The DeviceMesh cached in ``cfg['_b200']`` (rebuilt when node/elem/face change)."""
-    key = (id(cfg["node"]), id(cfg["elem"]), id(cfg.get("face")), np.shape(cfg["node"]), np.shape(cfg["elem"]),
-           np.shape(cfg.get("face")))
+    """The DeviceMesh cached in ``cfg['_b200']``, rebuilt when cfg's node,
+    elem or face array is replaced by another object.  The cache holds weak
+    references to the arrays it was built from, so an array freed and
+    replaced by a new one at the same address (same id) is not mistaken for
+    it.  Like redbirdpy, which derives face/area/evol/deldotdel from node and
+    elem once in meshprep and stores them in cfg, the mesh arrays are taken
+    as fixed once prepared: replace them (e.g. run meshprep again) rather
+    than edit them in place."""
+    arrays = (cfg["node"], cfg["elem"], cfg.get("face"))
+    shapes = tuple(np.shape(a) for a in arrays)
     cache = cfg.get("_b200")
-    if cache is not None and cache.get("key") == key:
+    if cache is not None and cache.get("shapes") == shapes and _same_arrays(cache.get("refs", ()), arrays):
         return cache["mesh"]
     m = DeviceMesh(cfg["node"], cfg["elem"], cfg.get("face"), cfg.get("area"), cfg.get("evol"))
-    cfg["_b200"] = {"key": key, "mesh": m}
+    cfg["_b200"] = {"refs": tuple(_weak(a) for a in arrays), "shapes": shapes, "mesh": m}
     return m
 
 
@@ -362,11 +388,16 @@ def assemble(mesh, optics, ddd=None, evol=None):
 
 # ------------------------------------------------------------------ optodes
 class Optodes:
-    """Located point optodes: loc (int32, -1 outside), bary (npts x 4)."""
+    """The optodes of one forward model.  Point optodes are located
+    (loc int32, -1 outside; bary npts x 4); wide-field patterns (dense nn x
+    w columns, cfg['widesrc'] / cfg['widedet']) are kept on the device.
+    Right-hand-side columns follow redbirdpy's femrhs order
+    (forward.py:278-352): [point src | wide src | point det | wide det];
+    ``nsrc`` / ``ndet`` count point and wide ones together."""
 
-    def __init__(self, mesh, pts, nsrc, ndet):
+    def __init__(self, mesh, pts, nsrc, ndet, wsrc=None, wdet=None):
         dev = mesh.device
-        self.nsrc, self.ndet = int(nsrc), int(ndet)
+        self.npsrc, self.npdet = int(nsrc), int(ndet)
         self.pts_host = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
         self.npts = self.pts_host.shape[0]
         self.pts = _f64(self.pts_host, dev) if self.npts else torch.zeros(3, dtype=torch.float64, device=dev)
@@ -375,42 +406,84 @@ class Optodes:
         if self.npts:
             call("rb_tsearch", ptr(mesh.node), ptr(mesh.elem), mesh.ne, ptr(self.pts), self.npts, ptr(self.loc),
                  ptr(self.bary), stream())
+        self.wsrc = self._patterns(mesh, wsrc)
+        self.wdet = self._patterns(mesh, wdet)
+        self.nwsrc = 0 if self.wsrc is None else self.wsrc.shape[1]
+        self.nwdet = 0 if self.wdet is None else self.wdet.shape[1]
+        self.nsrc = self.npsrc + self.nwsrc
+        self.ndet = self.npdet + self.nwdet
+        self.ncol = self.nsrc + self.ndet
+
+    @staticmethod
+    def _patterns(mesh, w):
+        if w is None or np.size(w) == 0:
+            return None
+        w = np.asarray(w, dtype=np.float64)
+        if w.ndim == 1:
+            w = w[:, None]
+        if w.shape[0] != mesh.nn:
+            raise ValueError("wide-field patterns must have one row per node (Nn x Npattern)")
+        return _f64(w, mesh.device)
 
     def rhs(self, mesh):
-        """Dense nn x (nsrc+ndet) real RHS, columns [src | det]."""
-        B = torch.zeros((mesh.nn, self.npts), dtype=torch.float64, device=mesh.device)
-        if self.npts:
-            call("rb_point_rhs", ptr(mesh.elem), ptr(self.loc), ptr(self.bary), self.npts, mesh.nn, self.npts, 0,
-                 ptr(B), stream())
+        """Dense nn x ncol real RHS in femrhs's column order."""
+        ld = self.ncol
+        B = torch.zeros((mesh.nn, ld), dtype=torch.float64, device=mesh.device)
+        if self.npsrc:
+            call("rb_point_rhs", ptr(mesh.elem), ptr(self.loc), ptr(self.bary), self.npsrc, mesh.nn, ld, 0, ptr(B),
+                 stream())
+        if self.nwsrc:
+            call("rb_wide_rhs", ptr(self.wsrc), mesh.nn, self.nwsrc, self.nwsrc, ld, self.npsrc, ptr(B), stream())
+        if self.npdet:
+            call("rb_point_rhs", ptr(mesh.elem), ptr(self.loc[self.npsrc:]), ptr(self.bary[self.npsrc:]), self.npdet,
+                 mesh.nn, ld, self.nsrc, ptr(B), stream())
+        if self.nwdet:
+            call("rb_wide_rhs", ptr(self.wdet), mesh.nn, self.nwdet, self.nwdet, ld, self.nsrc + self.npdet, ptr(B),
+                 stream())
         return B
 
     def loc_bary_host(self):
+        """loc (1-based float, NaN outside the mesh and for wide-field
+        columns) and bary (NaN rows for wide-field), one entry per RHS column
+        in femrhs's order (forward.py:298-301)."""
         loc = self.loc[: self.npts].cpu().numpy().astype(np.float64)
         bary = self.bary[: self.npts].cpu().numpy()
         outside = loc < 0
         loc = loc + 1.0
         loc[outside] = np.nan
-        return loc, bary
+        if not (self.nwsrc or self.nwdet):
+            return loc, bary
+        L = np.full(self.ncol, np.nan)
+        Bb = np.full((self.ncol, 4), np.nan)
+        L[:self.npsrc], Bb[:self.npsrc] = loc[:self.npsrc], bary[:self.npsrc]
+        d0 = self.nsrc
+        L[d0:d0 + self.npdet], Bb[d0:d0 + self.npdet] = loc[self.npsrc:], bary[self.npsrc:]
+        return L, Bb
 
 
 def locate_optodes(mesh, cfg, wv=""):
     from .utility import getoptodes
 
     src, det, wsrc, wdet = getoptodes(cfg, wv)
-    if (wsrc is not None and np.size(wsrc)) or (wdet is not None and np.size(wdet)):
-        raise NotImplementedError("wide-field sources/detectors are outside this engine's scope")
     parts = [p for p in (src, det) if p is not None]
     pts = np.vstack(parts) if parts else np.zeros((0, 3))
-    return Optodes(mesh, pts, 0 if src is None else src.shape[0], 0 if det is None else det.shape[0])
+    return Optodes(mesh, pts, 0 if src is None else src.shape[0], 0 if det is None else det.shape[0], wsrc, wdet)
 
 
 def getdet(mesh, opt, phi):
-    """detval (ndet x nsrc) = rhs_det^T phi_src (redbirdpy/forward.py:365-442)."""
+    """detval (ndet x nsrc) = rhs_det^T phi_src (redbirdpy/forward.py:365-442):
+    point detector rows by the 4-node barycentric gather, wide-field rows by
+    the pattern product over all nodes; columns = point then wide sources."""
     kind = _lib.RB_C128 if phi.is_complex() else _lib.RB_F64
     out = torch.empty((opt.ndet, opt.nsrc), dtype=phi.dtype, device=phi.device)
-    if opt.ndet and opt.nsrc:
-        call("rb_femgetdet", ptr(mesh.elem), ptr(opt.loc[opt.nsrc:]), ptr(opt.bary[opt.nsrc:]), opt.ndet,
+    if opt.npdet and opt.nsrc:
+        call("rb_femgetdet", ptr(mesh.elem), ptr(opt.loc[opt.npsrc:]), ptr(opt.bary[opt.npsrc:]), opt.npdet,
              ptr(phi), phi.shape[1], opt.nsrc, kind, ptr(out), stream())
+    if opt.nwdet and opt.nsrc:
+        wb = _lib.lib().rb_wide_getdet_work_bytes(opt.nwdet, opt.nsrc, kind)
+        work = torch.empty(wb, dtype=torch.uint8, device=phi.device)
+        call("rb_wide_getdet", ptr(opt.wdet), mesh.nn, opt.nwdet, opt.nwdet, ptr(phi), phi.shape[1], opt.nsrc, kind,
+             ptr(out[opt.npdet:]), ptr(work), wb, stream())
     return out
 
 
@@ -778,27 +851,98 @@ def gram(J, K, alpha=1.0, precision="tf32"):
     return H, lo
 
 
-def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None):
-    """reginvunder (recon.py:429-509) for the rows of J (scaled by sqrt(alpha)):
-    H = alpha J J^T + lam I, unit-diagonal normalisation, FP64 Cholesky,
-    returns alpha J^T y on the device (K-vector, FP64)."""
+def gemv_n(J, K, x, alpha=1.0, beta=0.0, out=None, lo=None):
+    """out = alpha J x + beta out on the device (J FP32 / BF16 rows, x FP64
+    K-vector); with ``lo`` the split remainder of J is added as well."""
+    M, ldj = J.shape
+    if out is None:
+        out = torch.empty(M, dtype=torch.float64, device=J.device)
+    fn = "rb_gemv_n_bf16" if J.dtype == torch.bfloat16 else "rb_gemv_n"
+    call(fn, ptr(J), M, K, ldj, ptr(x), float(alpha), float(beta), ptr(out), stream())
+    if lo is not None:
+        call("rb_gemv_n", ptr(lo), M, K, ldj, ptr(x), float(alpha), 1.0, ptr(out), stream())
+    return out
+
+
+def norm2(x):
+    """||x||_2 of an FP64 device vector (rb_dot), as a Python float."""
+    out = torch.empty(1, dtype=torch.float64, device=x.device)
+    wb = _lib.lib().rb_dot_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=x.device)
+    call("rb_dot", x.numel(), ptr(x), ptr(x), ptr(out), ptr(work), wb, stream())
+    return float(out.item()) ** 0.5
+
+
+def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None):
+    """The tensor-core half of reginvunder (recon.py:474-483): H = alpha J J^T
+    (+ lam I, lam relative to the largest diagonal entry with ``lam_rel``),
+    unit-diagonal normalisation (_normalize_diag, recon.py:784-789), FP64
+    Cholesky in place.  Returns (H, di, lo, lam)."""
     M, ldj = J.shape
     dev = J.device
     H, lo = gram(J, K, alpha, precision)
-    if lam_rel is not None:  # lambda relative to the largest diagonal entry
+    if lam_rel is not None:
         lam = float(lam_rel) * float(H.diagonal().max().item())
     di = torch.empty(M, dtype=torch.float64, device=dev)
     call("rb_reginv_prepare", ptr(H), M, M, float(lam), ptr(di), stream())
     wb = _lib.lib().rb_cholesky_work_bytes()
     work = torch.empty(wb, dtype=torch.uint8, device=dev)
     call("rb_cholesky", ptr(H), M, M, ptr(work), wb, stream())
+    return H, di, lo, float(lam)
+
+
+def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1e-14, info=None, return_y=False):
+    """y = (alpha J J^T + lam I)^-1 r with the factor of normal_factor, then
+    returns alpha J^T y (K-vector, FP64), or y itself with ``return_y``.
+
+    The factor comes from tensor-core products, whose inputs are rounded
+    (~1e-3 relative for TF32).  ``refine`` sweeps of FP64 iterative
+    refinement make y the solution for the stored J itself: the residual
+    r - alpha J (J^T y) - lam y takes FP64-accumulated GEMVs over J (two
+    passes over J per sweep), and y += C^-1 residual with the factor C as the
+    preconditioner, until ||residual|| <= refine_tol ||r||.  ``info`` (a dict)
+    receives the sweeps done and the last relative residual."""
+    M = J.shape[0]
+    dev = J.device
     rr = torch.as_tensor(np.ascontiguousarray(r, dtype=np.float64), device=dev) if not torch.is_tensor(r) else r
-    t = torch.empty(M, dtype=torch.float64, device=dev)
-    call("rb_vec_mul", ptr(di), ptr(rr), ptr(t), M, stream())
-    call("rb_chol_solve", ptr(H), M, M, ptr(t), stream())
-    y = torch.empty(M, dtype=torch.float64, device=dev)
-    call("rb_vec_mul", ptr(di), ptr(t), ptr(y), M, stream())
-    return gemv_t(J, K, y, alpha, lo=lo)
+
+    def precond(v):
+        t = torch.empty(M, dtype=torch.float64, device=dev)
+        call("rb_vec_mul", ptr(di), ptr(v), ptr(t), M, stream())
+        call("rb_chol_solve", ptr(H), M, M, ptr(t), stream())
+        out = torch.empty(M, dtype=torch.float64, device=dev)
+        call("rb_vec_mul", ptr(di), ptr(t), ptr(out), M, stream())
+        return out
+
+    y = precond(rr)
+    sweeps, rel = 0, None
+    if refine:
+        rnorm = norm2(rr) or 1.0
+        u = torch.empty(K, dtype=torch.float64, device=dev)
+        res = torch.empty(M, dtype=torch.float64, device=dev)
+        for it in range(int(refine)):
+            gemv_t(J, K, y, 1.0, out=u, lo=lo)  # u = J^T y
+            res.copy_(rr)
+            gemv_n(J, K, u, -float(alpha), 1.0, out=res, lo=lo)  # res = r - alpha J u
+            call("rb_axpby", M, -float(lam), ptr(y), 1.0, ptr(res), stream())  # res -= lam y
+            rel = norm2(res) / rnorm
+            if rel <= refine_tol:
+                break
+            call("rb_axpby", M, 1.0, ptr(precond(res)), 1.0, ptr(y), stream())
+            sweeps = it + 1
+    if info is not None:
+        info.update(refine_sweeps=sweeps, refine_relres=rel, lam=float(lam))
+    return y if return_y else gemv_t(J, K, y, alpha, lo=lo)
+
+
+def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None, refine=3, refine_tol=1e-14,
+                        info=None):
+    """reginvunder (recon.py:429-509) for the rows of J (scaled by sqrt(alpha)):
+    H = alpha J J^T + lam I on the tensor cores, unit-diagonal normalisation,
+    FP64 Cholesky, FP64 refinement (normal_solve); returns alpha J^T y on the
+    device (K-vector, FP64)."""
+    H, di, lo, lam = normal_factor(J, K, lam, alpha, precision, lam_rel)
+    return normal_solve(J, K, H, di, r, lam, alpha, lo, refine, refine_tol, info)
 
 
 def gemv_t(J, K, y, alpha=1.0, beta=0.0, out=None, lo=None):

@@ -3,9 +3,10 @@
 and ``jac`` with the reference signatures and return types, computed on the
 GPU by ``librbb200.so``.
 
-Scope: single-wavelength ``cfg['prop']`` arrays (label/seg, per-node or
-per-tet rows), point sources and detectors, CW or frequency domain.
-Multi-wavelength dicts and wide-field optodes raise NotImplementedError.
+Scope: ``cfg['prop']`` arrays (label/seg, per-node or per-tet rows) or
+per-wavelength dicts of them, point and wide-field (``cfg['widesrc']`` /
+``cfg['widedet']`` pattern columns) sources and detectors, CW or frequency
+domain.
 """
 
 import numpy as np
@@ -15,7 +16,7 @@ from scipy import sparse
 from . import engine
 from .solver import femsolve, solver_options
 
-__all__ = ["runforward", "femlhs", "femrhs", "femgetdet", "jac", "C0", "forward_device"]
+__all__ = ["runforward", "femlhs", "femrhs", "femgetdet", "jac", "jacchrome", "C0", "forward_device"]
 
 C0 = engine.C0
 
@@ -85,42 +86,69 @@ def femlhs(cfg, deldotdel_mat=None, wavelength="", mode=1):
 
 
 def femrhs(cfg, sd=None, wv="", md=1):
-    """Point-optode RHS ``(rhs, loc, bary, optode)`` (redbirdpy/forward.py:259-362):
-    rhs is Nn x (Nsrc+Ndet) CSR with 4 barycentric weights per column, loc
-    1-based (NaN outside the mesh)."""
+    """RHS ``(rhs, loc, bary, optode)`` (redbirdpy/forward.py:259-362): rhs is
+    Nn x Ncol CSR in the column order [point src | wide src | point det |
+    wide det] -- 4 barycentric weights per point column, the pattern's
+    nonzeros per wide-field column; loc 1-based (NaN outside the mesh and for
+    wide-field columns), bary NaN rows for wide-field columns."""
     mesh = engine.mesh_of(cfg)
     opt = engine.locate_optodes(mesh, cfg, wv)
     nn = mesh.nn
-    if opt.npts == 0:
+    if opt.ncol == 0:
         return sparse.csr_matrix((nn, 0)), np.array([]), np.array([]).reshape(0, 4), np.array([])
     loc, bary = opt.loc_bary_host()
-    B = opt.rhs(mesh)
-    rhs = sparse.csr_matrix(B.cpu().numpy())
+    # point columns straight from (loc, bary): the 4 weights of each located
+    # optode at its tet's nodes, zero weights dropped (as the reference's
+    # sparse column writes leave them out); wide columns from the patterns
+    inside = ~np.isnan(loc)
+    cols = np.repeat(np.nonzero(inside)[0], 4)
+    tets = loc[inside].astype(np.int64) - 1
+    rows = np.asarray(cfg["elem"])[tets, :4].astype(np.int64).ravel() - 1
+    vals = bary[inside].ravel()
+    keep = vals != 0
+    R, C, V = [rows[keep]], [cols[keep]], [vals[keep]]
+    for w, c0 in ((cfg.get("widesrc"), opt.npsrc), (cfg.get("widedet"), opt.nsrc + opt.npdet)):
+        if w is not None and np.size(w):
+            w = np.asarray(w, dtype=np.float64).reshape(nn, -1)
+            r, c = np.nonzero(w)
+            R.append(r), C.append(c + c0), V.append(w[r, c])
+    rhs = sparse.csr_matrix((np.concatenate(V), (np.concatenate(R), np.concatenate(C))), shape=(nn, opt.ncol))
     return rhs, loc, bary, opt.pts_host
 
 
 def femgetdet(phi, cfg, rhs, loc=None, bary=None):
-    """Detector readout ``rhs_det^T phi_src`` (redbirdpy/forward.py:365-442).
+    """Detector readout ``rhs_det^T phi_src`` (redbirdpy/forward.py:365-442),
+    (point + wide detectors) x (point + wide sources).
 
-    With ``loc``/``bary`` given (point detectors) the GPU gathers the four
-    barycentric weights per detector; otherwise the sparse product of the
-    given rhs columns is formed on the GPU by the same kernel after locating
-    the detectors again."""
+    With ``loc``/``bary`` given (femrhs's outputs) the GPU gathers the four
+    barycentric weights per point detector; otherwise the detectors are
+    located again.  Wide-field detector rows come from cfg['widedet']."""
     ns = np.atleast_2d(cfg["srcpos"]).shape[0] if cfg.get("srcpos") is not None and np.size(cfg["srcpos"]) else 0
     nd = np.atleast_2d(cfg["detpos"]).shape[0] if cfg.get("detpos") is not None and np.size(cfg["detpos"]) else 0
-    if ns == 0 or nd == 0:
+    wsrc, wdet = cfg.get("widesrc"), cfg.get("widedet")
+    ws = np.asarray(wsrc).reshape(np.shape(wsrc)[0], -1).shape[1] if wsrc is not None and np.size(wsrc) else 0
+    wd = np.asarray(wdet).reshape(np.shape(wdet)[0], -1).shape[1] if wdet is not None and np.size(wdet) else 0
+    if ns + ws == 0 or nd + wd == 0:
         return np.array([])
     mesh = engine.mesh_of(cfg)
     dev = mesh.device
     if loc is None or bary is None:
         opt = engine.locate_optodes(mesh, cfg)
     else:
+        loc = np.asarray(loc, dtype=np.float64).ravel()
+        bary = np.asarray(bary, dtype=np.float64).reshape(-1, 4)
+        if ws or wd:  # entries in femrhs's column order: keep the point ones
+            idx = np.r_[np.arange(ns), ns + ws + np.arange(nd)]
+            loc, bary = loc[idx], bary[idx]
         opt = engine.Optodes.__new__(engine.Optodes)
-        loc = np.asarray(loc, dtype=np.float64)
         l0 = np.where(np.isnan(loc), -1, loc - 1).astype(np.int32)
-        opt.nsrc, opt.ndet, opt.npts = ns, nd, ns + nd
+        opt.npsrc, opt.npdet, opt.npts = ns, nd, ns + nd
         opt.loc = torch.as_tensor(l0, device=dev)
-        opt.bary = torch.as_tensor(np.nan_to_num(np.asarray(bary, dtype=np.float64)), device=dev)
+        opt.bary = torch.as_tensor(np.nan_to_num(bary), device=dev)
+        opt.wsrc = engine.Optodes._patterns(mesh, wsrc)
+        opt.wdet = engine.Optodes._patterns(mesh, wdet)
+        opt.nwsrc, opt.nwdet = ws, wd
+        opt.nsrc, opt.ndet, opt.ncol = ns + ws, nd + wd, ns + ws + nd + wd
     phi_t = torch.as_tensor(np.ascontiguousarray(phi), device=dev)
     return engine.getdet(mesh, opt, phi_t).cpu().numpy()
 
@@ -139,3 +167,22 @@ def jac(sd, phi, deldotdel_mat, elem, evol, iselem=False):
     jn = engine.jacobian(mesh, phi_t, sd, "mua", out_dtype=torch.float64, evol=ev)
     je = engine.jacobian_elem(mesh, phi_t, sd, evol=ev)
     return jn.cpu().numpy(), je.cpu().numpy()
+
+
+def jacchrome(Jmua, chromophores, extin=None):
+    """Chromophore Jacobians from per-wavelength mua Jacobians
+    (redbirdpy/forward.py:572-589): for each chromophore, the wavelengths'
+    blocks Jmua[wv] * extin(wv, ch) stacked in wavelength order.  ``extin``
+    (Nwv x Nchrome, or see property.extinction) is taken from redbirdpy's
+    spectra when not given.  Works on numpy arrays or device tensors."""
+    from .property import extinction
+
+    if not isinstance(Jmua, dict):
+        raise ValueError("Jmua must be a dict with wavelength keys")
+    wavelengths = list(Jmua.keys())
+    ext, _ = extinction(wavelengths, chromophores, extin)
+    out = {}
+    for i, ch in enumerate(chromophores):
+        blocks = [Jmua[wv] * ext[j, i] for j, wv in enumerate(wavelengths)]
+        out[ch] = torch.cat(blocks, 0) if torch.is_tensor(blocks[0]) else np.vstack(blocks)
+    return out

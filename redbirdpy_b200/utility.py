@@ -7,7 +7,10 @@ in ``cfg`` are 1-based; the device layer converts once.  Heavy mesh work
 ``redbirdpy_b200.engine``.
 """
 
+import weakref
+
 import numpy as np
+import torch
 
 __all__ = [
     "meshprep", "deldotdel", "sdmap", "getoptodes", "getdistance", "getltr", "getreff",
@@ -89,16 +92,21 @@ def getreff(n_in, n_out=1.0):
 
 def _first_elem_with_node(cfg, v):
     """Index of the first tet that has (1-based) node v, or None; cached in
-    cfg['_b200'] per elem array (a full scan of elem otherwise)."""
+    cfg['_b200'] beside the mesh (a full scan of elem otherwise), and dropped
+    with it when cfg's elem array is replaced."""
     elem = cfg["elem"]
-    key = (id(elem), np.shape(elem), int(v))
     cache = cfg.get("_b200")
-    if isinstance(cache, dict) and cache.get("first_elem_key") == key:
+    hit_cache = isinstance(cache, dict) and cache.get("first_elem_key") == (int(v), np.shape(elem))
+    if hit_cache and cache.get("first_elem_ref") is not None and cache["first_elem_ref"]() is elem:
         return cache["first_elem"]
     hit = np.nonzero(np.any(elem[:, :4] == v, axis=1))[0]
     r = int(hit[0]) if len(hit) else None
     if isinstance(cache, dict):
-        cache["first_elem_key"], cache["first_elem"] = key, r
+        try:
+            ref = weakref.ref(elem)
+        except TypeError:
+            ref = None
+        cache["first_elem_key"], cache["first_elem"], cache["first_elem_ref"] = (int(v), np.shape(elem)), r, ref
     return r
 
 
@@ -201,22 +209,32 @@ def getdistance(srcpos, detpos, badsrc=None, baddet=None, widesrc=None, widedet=
     return dist
 
 
+def _npattern(w):
+    return np.asarray(w).reshape(np.shape(w)[0], -1).shape[1] if w is not None and np.size(w) else 0
+
+
 def sdmap(cfg, maxdist=np.inf, **kwargs):
-    """Source/detector pair table [src_col, det_col, active] (utility.py:675-796,
-    single-wavelength point-optode case).  Rows are detector-major (meshgrid)."""
+    """Source/detector pair table [src_col, det_col, active] (utility.py:675-796).
+    Rows are detector-major (meshgrid); columns index the RHS / phi columns in
+    femrhs's order [point src | wide src | point det | wide det].  Excluded
+    point optodes are left out; ``maxdist`` deactivates point pairs only
+    (wide-field pairs stay active)."""
     ns = np.atleast_2d(cfg["srcpos"]).shape[0] if cfg.get("srcpos") is not None and np.size(cfg["srcpos"]) else 0
     nd = np.atleast_2d(cfg["detpos"]).shape[0] if cfg.get("detpos") is not None and np.size(cfg["detpos"]) else 0
-    if ns == 0 or nd == 0:
+    ws, wd = _npattern(cfg.get("widesrc")), _npattern(cfg.get("widedet"))
+    if ns + ws == 0 or nd + wd == 0:
         raise ValueError("Must define at least one source and detector")
     badsrc = kwargs.get("excludesrc", cfg.get("excludesrc", []))
     baddet = kwargs.get("excludedet", cfg.get("excludedet", []))
-    gs = sorted(set(range(ns)) - set(badsrc))
-    gd = sorted(set(range(nd)) - set(baddet))
-    ss, dd = np.meshgrid(gs, [ns + d for d in gd])
+    gs = sorted(set(range(ns)) - set(badsrc)) + list(range(ns, ns + ws))
+    d0 = ns + ws  # first detector column
+    gd = [d0 + d for d in sorted(set(range(nd)) - set(baddet))] + [d0 + nd + j for j in range(wd)]
+    ss, dd = np.meshgrid(gs, gd)
     sd = np.column_stack([ss.ravel(), dd.ravel()])
-    if maxdist < np.inf:
+    if maxdist < np.inf and ns > 0 and nd > 0:
         dist = getdistance(cfg["srcpos"], cfg["detpos"], badsrc, baddet)
-        active = np.array([1.0 if dist[int(d) - ns, int(s)] < maxdist else 0.0 for s, d in sd])
+        active = np.array([1.0 if not (s < ns and d - d0 < nd) or dist[int(d) - d0, int(s)] < maxdist else 0.0
+                           for s, d in sd])
         out = np.column_stack([sd, active])
     else:
         out = np.column_stack([sd, np.ones(len(sd))])
@@ -249,6 +267,54 @@ def deldotdel(cfg):
     return engine.mesh_of(cfg).deldotdel_host(), None
 
 
+def _device_geometry(cfg, node, nn):
+    """Reorientation, boundary faces, face areas and tet volumes on the GPU
+    (rb_reorient / rb_volface / rb_face_area): the reference's fallbacks
+    (utility.py:1047-1109), bit for bit, returned into cfg as numpy with the
+    reference's 1-based indices."""
+    from . import engine
+
+    elem = cfg["elem"]
+    need = (not cfg.get("isreoriented", False)) or cfg.get("face") is None or cfg.get("area") is None \
+        or cfg.get("evol") is None
+    if not need:
+        return
+    dev = engine._dev()
+    node_d = torch.as_tensor(np.ascontiguousarray(node[:, :3]), device=dev)
+    e0 = torch.as_tensor(np.ascontiguousarray(np.asarray(elem)[:, :4].astype(np.int64) - 1, dtype=np.int32),
+                         device=dev)
+    ne = e0.shape[0]
+    st = engine.stream()
+    evol = torch.empty(max(ne, 1), dtype=torch.float64, device=dev)
+    if not cfg.get("isreoriented", False):
+        engine.call("rb_reorient", engine.ptr(node_d), engine.ptr(e0), ne, engine.ptr(evol), None, st)
+        r = e0.cpu().numpy().astype(np.asarray(elem).dtype) + 1
+        cfg["elem"] = np.column_stack([r, elem[:, 4:]]) if elem.shape[1] > 4 else r
+        cfg["isreoriented"] = True
+    elif cfg.get("evol") is None:  # volumes only: a scratch copy takes the swaps
+        tmp = e0.clone()
+        engine.call("rb_reorient", engine.ptr(node_d), engine.ptr(tmp), ne, engine.ptr(evol), None, st)
+    if cfg.get("face") is None or cfg.get("area") is None:
+        if cfg.get("face") is None:
+            face = torch.empty((4 * ne, 3), dtype=torch.int32, device=dev)
+            wb = engine._lib.lib().rb_volface_work_bytes(ne)
+            work = torch.empty(wb, dtype=torch.uint8, device=dev)
+            nf = engine.ctypes.c_int64(0)
+            engine.call("rb_volface", engine.ptr(e0), ne, nn, engine.ptr(face), engine.ctypes.byref(nf),
+                        engine.ptr(work), wb, st)
+            face = face[: nf.value]
+            cfg["face"] = face.cpu().numpy().astype(np.int64) + 1
+        else:
+            face = torch.as_tensor(np.ascontiguousarray(np.asarray(cfg["face"])[:, :3].astype(np.int64) - 1,
+                                                        dtype=np.int32), device=dev)
+        if cfg.get("area") is None:
+            area = torch.empty(max(face.shape[0], 1), dtype=torch.float64, device=dev)
+            engine.call("rb_face_area", engine.ptr(node_d), engine.ptr(face), face.shape[0], engine.ptr(area), st)
+            cfg["area"] = area[: face.shape[0]].cpu().numpy()
+    if cfg.get("evol") is None:
+        cfg["evol"] = evol[:ne].cpu().numpy()
+
+
 def meshprep(cfg):
     """Prepare the mesh dict in place (utility.py:101-246): reorientation,
     boundary faces, areas/volumes, nodal volumes, reff/musp0, the sparse
@@ -264,27 +330,26 @@ def meshprep(cfg):
     nn = node.shape[0]
     if elem.shape[1] > 4 and cfg.get("seg") is None:
         cfg["seg"] = elem[:, 4].astype(int)
-    if not cfg.get("isreoriented", False):
-        r = _reorient(node, elem[:, :4])
-        cfg["elem"] = np.column_stack([r, elem[:, 4:]]) if elem.shape[1] > 4 else r
-        cfg["isreoriented"] = True
-    if cfg.get("face") is None:
-        cfg["face"] = _volface(cfg["elem"], nn)
-    if cfg.get("area") is None:
-        cfg["area"] = _elemvolume(node, cfg["face"])
-    if cfg.get("evol") is None:
-        cfg["evol"] = _elemvolume(node, cfg["elem"][:, :4])
+    # a tet that repeats a node has zero volume: caught on the host before any
+    # device work (other zero volumes once the device has computed them)
+    se = np.sort(np.asarray(cfg["elem"])[:, :4], axis=1)
+    rep = np.nonzero(np.any(se[:, 1:] == se[:, :-1], axis=1))[0]
+    if rep.size:
+        raise ValueError(f"Degenerate elements detected at indices: {rep}")
+    _device_geometry(cfg, node, nn)
     if np.any(cfg["evol"] == 0):
         bad = np.where(cfg["evol"] == 0)[0]
         raise ValueError(f"Degenerate elements detected at indices: {bad}")
-    if cfg.get("nvol") is None:
-        cfg["nvol"] = _nodevolume(nn, cfg["elem"], cfg["evol"])
     if "srcpos" not in cfg:
         raise ValueError("cfg.srcpos is required")
     if "srcdir" not in cfg:
         raise ValueError("cfg.srcdir is required")
     if isinstance(cfg.get("prop"), dict) and "param" in cfg:
-        raise NotImplementedError("chromophore (multi-spectral 'param') properties are outside this engine's scope")
+        # multi-spectral: per-wavelength properties from the chromophores
+        # (utility.py:193-194); coefficients from cfg['extin'] when given
+        from .property import updateprop
+
+        cfg["prop"] = updateprop(cfg, extin=cfg.get("extin"))
     if cfg.get("reff") is None:
         bk = getbulk(cfg)
         if isinstance(bk, dict):  # per wavelength (utility.py:198-205)
@@ -293,14 +358,24 @@ def meshprep(cfg):
         else:
             cfg["reff"] = getreff(bk[3], 1.0)
             cfg["musp0"] = bk[1] * (1 - bk[2])
-    srctype = cfg.get("srctype", "pencil")
-    dettype = cfg.get("dettype", "pencil")
-    if srctype not in ("pencil", "isotropic") or dettype not in ("pencil", "isotropic") \
-            or "widesrcid" in cfg or "widedetid" in cfg:
-        raise NotImplementedError("wide-field sources/detectors are outside this engine's scope")
+    # wide-field patterns: taken as given in cfg['widesrc'] / cfg['widedet']
+    # (Nn x Npattern); making them from a source type (src2bc's projection of
+    # an illumination pattern onto the boundary, utility.py:252-636) is
+    # outside this engine (utility.py:210-224 calls it only when they are
+    # missing)
+    for kind in ("src", "det"):
+        typ = cfg.get(kind + "type", "pencil")
+        if (typ not in ("pencil", "isotropic") or ("wide%sid" % kind) in cfg) and ("wide" + kind) not in cfg:
+            raise NotImplementedError(f"wide-field {kind} patterns must be given as cfg['wide{kind}'] "
+                                      "(src2bc's pattern projection is outside this engine's scope)")
     from . import engine
 
     dm = engine.mesh_of(cfg)
+    if cfg.get("nvol") is None:
+        nvol = torch.empty(nn, dtype=torch.float64, device=dm.device)
+        engine.call("rb_nodevolume", nn, engine.ptr(dm.eptr), engine.ptr(dm.elist), engine.ptr(dm.evol),
+                    engine.ptr(nvol), engine.stream())
+        cfg["nvol"] = nvol.cpu().numpy()
     if cfg.get("cols") is None:
         cfg["rows"], cfg["cols"], cfg["idxcount"] = dm.adjacency_host()
     if cfg.get("idxsum") is None:

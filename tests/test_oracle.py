@@ -119,3 +119,23 @@ def test_tsearch_outside_and_ties():
     e0 = elem - 1
     contains = [k for k in range(len(elem)) if 13 in e0[k]]
     assert loc[2] == contains[0] + 1
+
+
+@pytest.mark.parametrize("case", ["wide_cw", "wide_fd"])
+def test_wide_field_matches_reference(golden, case):
+    """Wide-field pattern columns (cfg['widesrc'] / cfg['widedet']) in the
+    RHS, the pair table and the readout, against the reference's run."""
+    g = golden(case)
+    cfg = cfg_from(g)
+    cfg["widesrc"], cfg["widedet"] = g["widesrc"], g["widedet"]
+    cfg, sd = fo.meshprep(cfg)
+    assert np.array_equal(sd, g["sd"])
+    rhs, loc, bary, _ = fo.femrhs(cfg)
+    np.testing.assert_allclose(rhs.toarray(), g["rhs"], rtol=1e-13, atol=1e-15)
+    np.testing.assert_array_equal(np.isnan(loc), np.isnan(g["loc"]))
+    np.testing.assert_allclose(loc[~np.isnan(loc)], g["loc"][~np.isnan(g["loc"])])
+    det, phi = fo.runforward(cfg)
+    assert det.shape == g["detval"].shape
+    np.testing.assert_allclose(det, g["detval"], rtol=1e-9)
+    jn, _ = fo.jac(sd, phi, cfg["elem"], cfg["evol"])
+    np.testing.assert_allclose(jn, g["jn"], rtol=1e-8, atol=1e-12 * np.abs(g["jn"]).max())
