@@ -243,8 +243,14 @@ def run_b200(args):
     ne, nf = mesh.ne, mesh.nf
     pk = 8 if optics.kind == 0 else 8  # mua/musp per entity
     nprop = mesh.nn if optics.kind == 0 else ne
-    asm_bytes = (ne * (16 + 80 + 8 + 16) + nprop * (2 * pk + 8) + nnz * (4 + 8 + 4) + n * (4 * 3 + 12)
-                 + nf * (12 + 8 + 12))
+    # per tet: elem, deldotdel row, volume, its 4 incidence entries (+ their
+    # 4 packed slot words with the contributor tables); per property entity
+    # mua, musp and D; per nonzero: column index read, FP64 + FP32 value
+    # written (+ the contributor mask); per node: the three row pointers and
+    # the FP64 + FP32 reciprocal diagonal; per boundary face: nodes and area
+    tab = mesh.inc_slot is not None
+    asm_bytes = (ne * (16 + 80 + 8 + 16 + (16 if tab else 0)) + nprop * (2 * pk + 8)
+                 + nnz * (4 + 8 + 4 + (4 if tab else 0)) + n * (4 * 3 + 12) + nf * (12 + 8 + 12))
     asm_gbs = asm_bytes / (asm_ms * 1e-3) / 1e9
 
     # end to end through the public API (host arrays in, numpy out)
@@ -261,14 +267,28 @@ def run_b200(args):
         det_h, phi_h = rbb.runforward(host_cfg)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / ke, world)
-    h2d = (2 * mesh.ne * 8) + 128 * 3 * 8
+    # what one runforward call uploads: the optode positions (located on the
+    # device every call) and the label property table (mua, musp, g rows)
+    # expanded per tet on the device; the mesh and the per-tet labels are
+    # uploaded once and kept on the device across calls (as redbirdpy keeps
+    # the prepared mesh in cfg)
+    props = np.atleast_2d(cfg["prop"])
+    h2d = int(cfg["srcpos"].size * 8 + cfg["detpos"].size * 8 + props.shape[0] * min(3, props.shape[1]) * 8)
     d2h = det_h.nbytes + phi_h.nbytes
 
+    # DRAM bytes per launch from an earlier ncu capture of this workload,
+    # stored beside the summaries (not measured in this run)
     traffic = {}
     tp = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp))
     it = infos[-1]
+    spk = it.get("spmm_kernel", "spmm_pair_kernel")
+    spmm_desc = {"spmm_blk_kernel": "spmm_blk_kernel (FP32 CSR SpMM over 2x2x2 spatial row groups, one gather per "
+                                    "group column, 128 RHS, fused p.Ap)",
+                 "spmm_pair_kernel": "spmm_pair_kernel (FP32 CSR SpMM, two rows per warp over their column union, "
+                                     "128 RHS, fused p.Ap)"}[spk]
+    asm_kernel = "femlhs_tab_kernel" if mesh.inc_slot is not None else "femlhs_rows_kernel"
     out = {
         "metric": METRIC, "value": round(world * nrhs / (ms_mixed * 1e-3), 3), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
@@ -287,20 +307,22 @@ def run_b200(args):
                                                / max(1, sum(i["coarse_launches"] for i in pinfos)), 4),
                    "jacobi_only_ms_per_step": round(ms_jac, 3), "jacobi_only_iters": infos_jac[-1]["iters"]},
         "gpu_launches": int(sum(i["launches"] for i in infos) / len(infos)) + 6,
-        "roofline": {"bound": "hbm", "kernel": "spmm_pair_kernel (FP32 CSR SpMM, two rows per warp over their column union, 128 RHS, fused p.Ap)",
+        "roofline": {"bound": "hbm", "kernel": spmm_desc,
                      "achieved": round(sp_gbs, 1) if sp_gbs else None, "peak": peak, "unit": "GB/s",
                      "frac": round(sp_gbs / peak, 4) if sp_gbs else None, "peak_source": peak_kind,
                      "algorithmic_bytes": spmm_bytes, "launch_ms": round(sp_ms, 4),
-                     "traffic": traffic.get("spmm_pair_kernel<EPI_PQDOT>"),
-                     "traffic_source": "ncu capture, profiles/forward_3Mtet_128rhs_launches_and_kernels.md"},
+                     "traffic": traffic.get(spk + "<EPI_PQDOT>"),
+                     "traffic_source": "stored: an earlier ncu capture of this workload, not measured in this run"},
         "roofline_update": {"kernel": "cg_update_agg_kernel<float> (r update + r.z, r.r, coarse restriction)",
                             "achieved": round(up_gbs, 1) if up_gbs else None,
                             "unit": "GB/s", "frac": round(up_gbs / peak, 4) if up_gbs else None,
                             "algorithmic_bytes": upd_bytes, "launch_ms": round(up_ms, 4),
-                            "traffic": traffic.get("cg_update_agg_kernel<float,32,4>")},
-        "roofline_assembly": {"kernel": "femlhs_rows_kernel (+ dcoeff prologue)", "achieved": round(asm_gbs, 1),
+                            "traffic": traffic.get("cg_update_agg_kernel<float,32,4>"),
+                            "traffic_source": "stored (earlier ncu capture)"},
+        "roofline_assembly": {"kernel": asm_kernel + " (+ dcoeff prologue)", "achieved": round(asm_gbs, 1),
                               "unit": "GB/s", "frac": round(asm_gbs / peak, 4), "algorithmic_bytes": asm_bytes,
-                              "launch_ms": round(asm_ms, 4), "traffic": traffic.get("femlhs_rows_kernel<real,per-tet>")},
+                              "launch_ms": round(asm_ms, 4), "traffic": traffic.get(asm_kernel + "<real,per-tet>"),
+                              "traffic_source": "stored (earlier ncu capture)"},
         "e2e": {"value": round(world * nrhs / e2e_s, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,
@@ -587,6 +609,18 @@ def run_profile(args):
     print(json.dumps(out))
 
 
+def _masked_log_amp_loss(own, tgt):
+    """0.5 sum (log|det| - log|target|)^2 over every instance's own (detector,
+    source) pairs of the stacked batch matrix, as one set of tensor ops."""
+    import torch
+
+    def loss(det):
+        d = torch.where(own, det, torch.ones_like(det))
+        t = torch.where(own, tgt, torch.ones_like(tgt))
+        return 0.5 * torch.sum((torch.log(torch.abs(d)) - torch.log(torch.abs(t))) ** 2)
+    return loss
+
+
 def _log_amp_loss(parts, targets):
     import torch
 
@@ -682,6 +716,12 @@ def run_adjoint(world, args):
     return out
 
 
+def engine_status(code):
+    from redbirdpy_b200.engine import INSTANCE_STATUS
+
+    return INSTANCE_STATUS[int(code)]
+
+
 def run_batch(world, args):
     """256 uneven box instances (seed 2; extents ~ U[30, 80] mm per axis,
     spacing in {2, 3, 4} mm, per-node mua ~ U[0.005, 0.03], mus ~ U[0.5, 2],
@@ -704,12 +744,14 @@ def run_batch(world, args):
     d0 = torch.as_tensor(np.concatenate([1.0 / (3.0 * (c["prop"][:, 0] + c["prop"][:, 1])) for c in cfgs]),
                          device="cuda")
     with torch.no_grad():
-        targets = bm.split(detector_values(bm, mua0 * 1.1, d0))
+        tgt_all = detector_values(bm, mua0 * 1.1, d0)
+        targets = bm.split(tgt_all)
+    loss_fn = _masked_log_amp_loss(bm.own, tgt_all)
 
     def step():
         mua = mua0.clone().requires_grad_(True)
         dco = d0.clone().requires_grad_(True)
-        _log_amp_loss(bm.split(detector_values(bm, mua, dco)), targets).backward()
+        loss_fn(detector_values(bm, mua, dco)).backward()
         return mua.grad
 
     for _ in range(2):
@@ -723,6 +765,24 @@ def run_batch(world, args):
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
+    # the same step replayed from one CUDA graph (fixed solve budget from a
+    # checked calibration solve; no host round trips inside the step)
+    from redbirdpy_b200.adjoint import CapturedStep
+
+    cap = CapturedStep(bm, loss_fn, mua0, d0)
+    for _ in range(3):
+        cap(mua0, d0)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(ks):
+        cap(mua0, d0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_graph = max_over_ranks(e0.elapsed_time(e1) / ks, world)
+    graph_status = cap.status.cpu().numpy()
+    g_graph = cap.gmua.clone()
+    cap.release()
+    g_err = float((torch.abs(g_graph - g).max() / torch.abs(g).max()).item())
     # accuracy: detector values against the FP64 form of the same batch
     with torch.no_grad():
         dm = detector_values(bm, mua0, d0)
@@ -751,8 +811,16 @@ def run_batch(world, args):
     l1.record()
     torch.cuda.synchronize()
     loop_ms = l0.elapsed_time(l1) / nloop
+    st = np.asarray(bm.status)
     return {"workload": f"256 instances, {nn} nodes / {ne} tets in total, {bm.S} source + {bm.D} detector columns",
+            "convergence": "per (instance, column): ||b_i - A_i x_i|| / ||b_i|| <= tol for each instance",
+            "inst_relres_max": float(np.max(bm.relres)),
+            "inst_status": {engine_status(k): int(np.sum(st == k)) for k in np.unique(st)},
             "instances_per_s": round(world * 256 / (ms * 1e-3), 2), "ms_per_batch": round(ms, 2),
+            "graph": {"instances_per_s": round(world * 256 / (ms_graph * 1e-3), 2),
+                      "ms_per_batch": round(ms_graph, 2), "budget": list(cap.budget),
+                      "instances_converged": int(np.sum(graph_status == 0)),
+                      "grad_rel_err_vs_checked": g_err},
             "loop_instances_per_s": round(world * 1e3 / loop_ms, 2),
             "loop_sample": f"first {nloop} instances, one model each (same kernels, launch-bound)",
             "speedup_vs_loop": round(loop_ms * 256 / ms, 2), "det_max_rel_err_vs_fp64": err}

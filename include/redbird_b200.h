@@ -63,6 +63,12 @@ typedef struct rb_mesh {
   const int32_t* node_flist; /* 3*nf, ascending */
   const int32_t* indptr;     /* nn+1 CSR row pointer */
   const int32_t* indices;    /* nnz CSR column indices, ascending per row */
+  /* Optional assembly tables from rb_assembly_tables (NULL: not used):
+   * inc_slot[node_eptr[n] + u] packs, one byte each, the CSR slots within
+   * row n of the 4 nodes of n's u-th incident tet; slot_mask[p] has bit u
+   * set when that tet holds column indices[p]. */
+  const uint32_t* inc_slot;  /* 4*ne */
+  const uint32_t* slot_mask; /* nnz */
 } rb_mesh;
 
 /* Node -> cell incidence (cells are tets, nv=4, or triangles, nv=3):
@@ -87,6 +93,15 @@ int rb_csr_pattern_fill(const int32_t* elem, int64_t nn, const int32_t* node_ept
                         void* stream);
 
 /* ------------------------------------------------------------- assembly */
+/* Incidence tables that let femlhs sum each matrix entry over only the tets
+ * that hold it.  Fills inc_slot (4*ne) and slot_mask (nnz) and sets *usable
+ * to 1 when every node has at most 32 incident tets and every row at most
+ * 255 columns (the tables' limits); with *usable 0 the mesh is assembled
+ * without them (leave rb_mesh.inc_slot / slot_mask NULL).  Synchronises
+ * the stream. */
+int rb_assembly_tables(const rb_mesh* mesh, uint32_t* inc_slot, uint32_t* slot_mask, int32_t* usable,
+                       void* stream);
+
 typedef struct rb_optics {
   int32_t kind;        /* RB_PROP_NODE: arrays have nn entries; RB_PROP_ELEM: ne */
   const double* mua;   /* 1/mm */
@@ -277,11 +292,37 @@ int rb_rowgroups_union_count(const rb_csr* A, const int32_t* rows, int64_t ng, i
                              int64_t* nu /* host */, void* work, size_t work_bytes, void* stream);
 int rb_rowgroups_union_fill(const rb_csr* A, const int32_t* rows, int64_t ng, const int32_t* uptr,
                             int32_t* ucol, uint8_t* umask, void* stream);
+/* Independent systems stacked block-diagonally in one matrix (a batch of
+ * instances): rows row_ptr[i] .. row_ptr[i+1]-1 belong to instance i.  With
+ * it the refinement tests ||b_i - A_i x_i|| / ||b_i|| of every (instance,
+ * column) on its own, scales each instance's correction right-hand side to
+ * unit norm on its rows, and stops correcting an instance's column once it
+ * is done, so that an instance's accuracy does not depend on the others.
+ * The caller adds rb_instances_work_bytes to the femsolve workspace. */
+typedef struct rb_instances {
+  int64_t ninst;
+  const int64_t* row_ptr;  /* device, ninst+1, ascending, row_ptr[ninst] = n */
+  const int32_t* row_inst; /* device, n: the instance of each row */
+  int32_t* status;         /* device out, ninst: 0 converged, 1 not converged within
+                              the sweep / iteration caps, 2 Krylov breakdown,
+                              3 non-finite residual, 4 a bounded in-kernel wait
+                              gave up (results invalid) */
+  double* relres;          /* device out, ninst x nrhs (row-major), or NULL: the final
+                              ||b_i - A_i x_i|| / ||b_i|| per (instance, column) */
+} rb_instances;
+size_t rb_instances_work_bytes(int64_t ninst, int64_t nrhs);
+
 typedef struct rb_solve_opts {
   int32_t precision;   /* RB_MIXED: FP32 Krylov + FP64 refinement; RB_FP64 */
   int32_t max_outer;   /* refinement sweeps (mixed) */
   int32_t maxiter;     /* cap on Krylov iterations per sweep */
-  int32_t check_every; /* iterations between host convergence checks */
+  int32_t check_every; /* iterations between host convergence checks; 0: a fixed
+                          budget of max_outer sweeps x maxiter iterations with no
+                          host check or read-back at all (the call only queues
+                          work: it can be captured into a CUDA graph); converged
+                          columns turn the remaining launches into no-ops.  Needs
+                          instances (the outcome is in their status words) and
+                          no coarse space; info->flag and relres are -1. */
   double tol;          /* target max relative residual ||b-Ax||/||b|| */
   double inner_tol;    /* relative residual of each FP32 correction solve */
   int32_t profile;     /* nonzero: time the Krylov kernels with CUDA events */
@@ -289,6 +330,7 @@ typedef struct rb_solve_opts {
                           Gauss-Newton iterate's fields); zero: start from 0 */
   const rb_coarse* coarse; /* host pointer; NULL: Jacobi preconditioner only */
   const rb_rowgroups* groups; /* host pointer; NULL: the SpMM walks rows (or row pairs) */
+  const rb_instances* instances; /* host pointer; NULL: one system */
 } rb_solve_opts;
 
 typedef struct rb_solve_info {
@@ -303,6 +345,7 @@ typedef struct rb_solve_info {
   int32_t update_launches;
   double coarse_ms;    /* profile only: total time of the coarse corrections */
   int32_t coarse_launches; /* profile only: coarse corrections timed */
+  int32_t sweep_iters_max; /* the most Krylov iterations one refinement sweep took */
 } rb_solve_info;
 
 /* femsolve (redbirdpy/solver.py:385-948) for all columns at once: Jacobi-
@@ -359,6 +402,14 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
            int32_t rmax, int32_t emax, const double* evol, const double* ddd, void* stream);
+/* rb_jac for the nodes node0 .. node0+count-1 only: J column c holds node
+ * node0 + c (ldj >= count).  A GN step whose full J would not fit in HBM
+ * forms its products from node slabs recomputed on demand. */
+int rb_jac_range(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
+                 const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
+                 const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
+                 int32_t rmax, int32_t emax, const double* evol, const double* ddd, int64_t node0,
+                 int64_t count, void* stream);
 
 /* Dual-mesh Jacobian remap (_remap_jacobian, redbirdpy/recon.py:818-876):
  * out[r][q] = sum_{p in [map_ptr[q], map_ptr[q+1])} map_w[p] J[r][map_idx[p]]

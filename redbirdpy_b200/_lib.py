@@ -29,7 +29,7 @@ class RbMesh(ctypes.Structure):
     _fields_ = [("nn", _i64), ("ne", _i64), ("nf", _i64), ("nnz", _i64),
                 ("node", _vp), ("elem", _vp), ("face", _vp), ("area", _vp),
                 ("node_eptr", _vp), ("node_elist", _vp), ("node_fptr", _vp), ("node_flist", _vp),
-                ("indptr", _vp), ("indices", _vp)]
+                ("indptr", _vp), ("indices", _vp), ("inc_slot", _vp), ("slot_mask", _vp)]
 
 
 class RbOptics(ctypes.Structure):
@@ -51,16 +51,21 @@ class RbRowGroups(ctypes.Structure):
                 ("coef", _vp)]
 
 
+class RbInstances(ctypes.Structure):
+    _fields_ = [("ninst", _i64), ("row_ptr", _vp), ("row_inst", _vp), ("status", _vp), ("relres", _vp)]
+
+
 class RbSolveOpts(ctypes.Structure):
     _fields_ = [("precision", _i32), ("max_outer", _i32), ("maxiter", _i32), ("check_every", _i32),
                 ("tol", _dbl), ("inner_tol", _dbl), ("profile", _i32), ("use_x0", _i32),
-                ("coarse", ctypes.POINTER(RbCoarse)), ("groups", ctypes.POINTER(RbRowGroups))]
+                ("coarse", ctypes.POINTER(RbCoarse)), ("groups", ctypes.POINTER(RbRowGroups)),
+                ("instances", ctypes.POINTER(RbInstances))]
 
 
 class RbSolveInfo(ctypes.Structure):
     _fields_ = [("iters", _i32), ("outer", _i32), ("flag", _i32), ("launches", _i32), ("relres", _dbl),
                 ("spmm_ms", _dbl), ("update_ms", _dbl), ("spmm_launches", _i32), ("update_launches", _i32),
-                ("coarse_ms", _dbl), ("coarse_launches", _i32)]
+                ("coarse_ms", _dbl), ("coarse_launches", _i32), ("sweep_iters_max", _i32)]
 
 
 _SIGS = {
@@ -71,7 +76,9 @@ _SIGS = {
     "rb_csr_pattern_work_bytes": (_sz, [_i64]),
     "rb_csr_pattern_count": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
     "rb_csr_pattern_fill": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "rb_assembly_tables": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "rb_femlhs_work_bytes": (_sz, [_i64, _i64]),
+    "rb_instances_work_bytes": (_sz, [_i64, _i64]),
     "rb_femlhs": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp, _vp,
                                  _vp, _sz, _vp]),
     "rb_femlhs_noalloc": (ctypes.c_int, [ctypes.POINTER(RbMesh), ctypes.POINTER(RbOptics), _vp, _vp, _vp, _vp, _vp,
@@ -108,6 +115,8 @@ _SIGS = {
     "rb_spmm": (ctypes.c_int, [ctypes.POINTER(RbCsr), _i32, _vp, _vp, _i64, _vp]),
     "rb_jac": (ctypes.c_int, [ctypes.POINTER(RbMesh), _i32, _vp, _i32, _i64, _vp, _i32, _i32, _i32, _vp, _vp,
                               _i64, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
+    "rb_jac_range": (ctypes.c_int, [ctypes.POINTER(RbMesh), _i32, _vp, _i32, _i64, _vp, _i32, _i32, _i32, _vp,
+                                    _vp, _i64, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _i64, _i64, _vp]),
     "rb_jac_remap": (ctypes.c_int, [_vp, _i32, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp]),
     "rb_jac_block": (ctypes.c_int, [_vp, _i32, _i64, _i64, _i64, _dbl, _dbl, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "rb_jac_elem": (ctypes.c_int, [ctypes.POINTER(RbMesh), _vp, _vp, _i32, _i64, _vp, _vp, _i64, _vp, _vp]),

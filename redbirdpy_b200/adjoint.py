@@ -27,7 +27,7 @@ import torch
 from . import engine
 from .solver import solver_options
 
-__all__ = ["DeviceModel", "BatchModel", "detector_values"]
+__all__ = ["DeviceModel", "BatchModel", "CapturedStep", "detector_values"]
 
 
 class DeviceModel:
@@ -42,7 +42,7 @@ class DeviceModel:
         self.mesh = engine.mesh_of(cfg)
         if props.shape[0] != self.mesh.nn:
             raise ValueError("detector_values needs node-based properties (one prop row per node)")
-        self.nref = props[:, 3] if props.shape[1] >= 4 else 1.37
+        self.nref = _nref_of(props[:, 3] if props.shape[1] >= 4 else np.full(props.shape[0], 1.37), self.mesh.device)
         self.omega = float(cfg.get("omega", 0) or 0)
         self.reff = cfg.get("reff", 0.493)
         self.opt = engine.locate_optodes(self.mesh, cfg)
@@ -67,12 +67,44 @@ class DeviceModel:
     def fields(self, mua, dcoef):
         mat = engine.assemble(self.mesh, self.optics(mua, dcoef))
         phi, info = engine.solve(mat, self.B, **self.solve_kw)
-        if info["flag"] != 0:
+        if info["flag"] is None:  # fixed budget: the outcome stays on the device
+            self.status = info["inst_status"]
+        elif info["flag"] != 0:
             raise RuntimeError(f"forward solve did not converge (flag {info['flag']})")
         return phi, mat
 
     def getdet(self, phi):
         return engine.getdet(self.mesh, self.opt, phi)
+
+    def calibrate_budget(self, mua, dcoef, margin=1.25):
+        """A fixed solve budget (sweeps, iterations per sweep) for this model
+        at these properties: one solve with host checks, its sweep count and
+        the most iterations a sweep took, times ``margin``.  Cached per
+        (nn, nnz, columns) bucket so that models of one size share it."""
+        key = (self.mesh.nn, self.mesh.nnz, int(self.B.shape[1]), self.solve_kw.get("precision"))
+        hit = _BUDGETS.get(key)
+        if hit is not None:
+            return hit
+        kw = {k: v for k, v in self.solve_kw.items() if k != "budget"}
+        mat = engine.assemble(self.mesh, self.optics(mua.detach(), dcoef.detach()))
+        _, info = engine.solve(mat, self.B, **kw)
+        if info["flag"] != 0:
+            raise RuntimeError(f"budget calibration: the checked solve did not converge (flag {info['flag']})")
+        budget = (max(1, int(info["outer"])), max(8, int(np.ceil(margin * info["sweep_iters_max"]))))
+        _BUDGETS[key] = budget
+        return budget
+
+
+_BUDGETS = {}
+
+
+def _nref_of(nref, dev):
+    """A per-node refractive index on the device, or the scalar when uniform
+    (uploaded once per model, not per assembly)."""
+    nref = np.asarray(nref, dtype=np.float64)
+    if nref.size and np.ptp(nref) == 0:
+        return float(nref.ravel()[0])
+    return torch.as_tensor(nref, device=dev)
 
 
 class BatchModel(DeviceModel):
@@ -110,9 +142,9 @@ class BatchModel(DeviceModel):
         if any(p.shape[0] != n for p, n in zip(props, nns)):
             raise ValueError("detector_values needs node-based properties (one prop row per node)")
         nref = np.concatenate([p[:, 3] if p.shape[1] >= 4 else np.full(p.shape[0], 1.37) for p in props])
-        self.nref = nref if np.ptp(nref) > 0 else float(nref[0])
         self.mesh = engine.DeviceMesh(node, elem, face, area, evol)
         dev = self.mesh.device
+        self.nref = _nref_of(nref, dev)
         # optodes: located among each instance's own tets
         self.ns, self.nd = [], []
         locs, barys = [], []
@@ -142,19 +174,51 @@ class BatchModel(DeviceModel):
         self.loc_det = torch.cat([l[n:] for l, n in zip(locs, self.ns)]).contiguous()
         self.bary_det = torch.cat([b[n:] for b, n in zip(barys, self.ns)]).contiguous()
         self.row0 = torch.as_tensor(self.node_off, dtype=torch.int64, device=dev)
-        self.det0 = torch.as_tensor(np.concatenate([[0], np.cumsum(self.nd)]), dtype=torch.int64, device=dev)
+        self.det0_host = np.concatenate([[0], np.cumsum(self.nd)]).astype(np.int64)
+        self.det0 = torch.as_tensor(self.det0_host, device=dev)
         self.ninst = len(cfgs)
+        # the (detector row, source column) entries that are an instance's own
+        # pairs; the rest of the block-diagonal detector matrix pairs one
+        # instance's detector with another's source column
+        own = np.zeros((int(self.det0_host[-1]), self.S), dtype=bool)
+        for i in range(self.ninst):
+            own[self.det0_host[i]:self.det0_host[i + 1], :self.ns[i]] = True
+        self.own = torch.as_tensor(own, device=dev)
         self.solve_kw = dict(solver_options(solver_kw), precision=precision)
         # Jacobi alone unless asked: the position-binned coarse space would put
         # nodes of overlapping instances into one aggregate, coupling blocks
         # that are independent (and were slower: 337 ms against 259 ms for the
         # 256-instance batch of 2.7M nodes)
         self.solve_kw.setdefault("coarse", False)
+        # convergence judged per instance: each instance's residual against
+        # its own right-hand side, whatever the others' sizes and scales
+        self.instances = engine.Instances(self.node_off, dev)
+        self.solve_kw["instances"] = self.instances
+        if precision == "fp64":
+            # the FP64 form is the accuracy reference of the batch: each
+            # instance is refined to its own FP64 floor (a sweep that no
+            # longer gains 4x ends it), as far-field detector values 1e-11
+            # of an instance's largest need; at 1e-15 relative residual they
+            # carried errors up to 5e-6
+            self.solve_kw.setdefault("tol", 1e-17)
+        self.status = None
+
+    def fields(self, mua, dcoef):
+        mat = engine.assemble(self.mesh, self.optics(mua, dcoef))
+        phi, info = engine.solve(mat, self.B, **self.solve_kw)
+        self.status, self.relres = info["inst_status"], info["inst_relres"]
+        if info["flag"] is None:  # fixed budget: read the status words later
+            return phi, mat
+        bad = np.flatnonzero(self.status)
+        if bad.size:
+            desc = ", ".join(f"{i}: {engine.INSTANCE_STATUS[int(self.status[i])]}" for i in bad[:8])
+            raise RuntimeError(f"forward solve failed for {bad.size} instance(s) ({desc})")
+        return phi, mat
 
     def getdet(self, phi):
         """All instances' detector values: row det0[i] + d, column s."""
         kind = engine._lib.RB_C128 if phi.is_complex() else engine._lib.RB_F64
-        nd = int(self.det0[-1].item())
+        nd = int(self.det0_host[-1])
         out = torch.empty((nd, self.S), dtype=phi.dtype, device=phi.device)
         engine.call("rb_femgetdet", engine.ptr(self.mesh.elem), engine.ptr(self.loc_det), engine.ptr(self.bary_det),
                     nd, engine.ptr(phi), phi.shape[1], self.S, kind, engine.ptr(out), engine.stream())
@@ -162,7 +226,7 @@ class BatchModel(DeviceModel):
 
     def split(self, det):
         """Per-instance (ndet_i x nsrc_i) views of getdet's output."""
-        d0 = self.det0.cpu().numpy()
+        d0 = self.det0_host
         return [det[d0[i]:d0[i + 1], :self.ns[i]] for i in range(self.ninst)]
 
     def node_slices(self, v):
@@ -221,3 +285,58 @@ def detector_values(model, mua, dcoef, resolve=False):
     max(nsrc) for a BatchModel (``split`` gives the per-instance blocks).
     Real for CW, complex in the frequency domain."""
     return _DetectorValues.apply(mua, dcoef, model, resolve)
+
+
+class CapturedStep:
+    """Forward plus adjoint gradient of a loss, captured once as a CUDA graph
+    and replayed per call.
+
+    The solves run on a fixed budget (sweeps x iterations per sweep, see
+    engine.solve), so nothing in the step waits for the host; the budget
+    comes from ``model.calibrate_budget`` (one checked solve, with margin)
+    unless given.  ``loss_fn(det)`` maps the model's detector values to a
+    scalar with torch operations.  A call copies ``mua`` / ``dcoef`` into the
+    captured inputs, replays the graph and returns (loss, det, dL/dmua,
+    dL/dD), device tensors that the next call overwrites.  ``status`` holds
+    the per-instance outcome of the last replay's forward solve (0
+    converged; see engine.INSTANCE_STATUS); check it before trusting a
+    result, since a fixed budget can end before convergence."""
+
+    def __init__(self, model, loss_fn, mua, dcoef, budget=None, warmup=2):
+        if budget is None:
+            budget = model.calibrate_budget(mua, dcoef)
+        self.budget = tuple(budget)
+        self.model = model
+        self.solve_kw_checked = model.solve_kw
+        model.solve_kw = dict(model.solve_kw, budget=self.budget)
+        if "instances" not in model.solve_kw:
+            model.solve_kw["instances"] = engine.Instances([0, model.mesh.nn], model.mesh.device)
+        self.mua = mua.detach().clone().requires_grad_(True)
+        self.dco = dcoef.detach().clone().requires_grad_(True)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                self.mua.grad = self.dco.grad = None
+                loss_fn(detector_values(model, self.mua, self.dco)).backward()
+        torch.cuda.current_stream().wait_stream(side)
+        self.mua.grad = self.dco.grad = None
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.det = detector_values(model, self.mua, self.dco)
+            self.loss = loss_fn(self.det)
+            self.loss.backward()
+        self.gmua, self.gdco = self.mua.grad, self.dco.grad
+        self.status = model.status
+
+    def __call__(self, mua, dcoef):
+        with torch.no_grad():
+            self.mua.copy_(mua)
+            self.dco.copy_(dcoef)
+        self.graph.replay()
+        return self.loss, self.det, self.gmua, self.gdco
+
+    def release(self):
+        """Drop the graph and give the model back its checked solves."""
+        self.graph = None
+        self.model.solve_kw = self.solve_kw_checked

@@ -200,6 +200,142 @@ femlhs_rows_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, cons
   }
 }
 
+// Precomputed incidence tables (rb_assembly_tables): for each row n and each
+// of its incident tets u (u < 32, ascending), the CSR slots of the tet's 4
+// nodes within row n (one byte each), and for each CSR slot the mask of the
+// incident tets that hold its column.  With them a slot's sum visits only
+// its own contributors (in ascending tet order) instead of comparing every
+// staged tet's 4 nodes against its column, and the diagonal (every tet of the
+// row contributes) is a fixed-order butterfly sum across the lanes.
+__global__ void asm_tables_kernel(rb_mesh m, uint32_t* __restrict__ inc_slot, uint32_t* __restrict__ slot_mask,
+                                  int32_t* __restrict__ bad) {
+  __shared__ uint32_t s_mask[kAsmWarps][256];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * kAsmWarps;
+  for (int64_t row = blockIdx.x * (int64_t)kAsmWarps + w; row < m.nn; row += warps) {
+    const int32_t rb = m.indptr[row], rn = m.indptr[row + 1] - rb;
+    const int32_t eb = m.node_eptr[row], ek = m.node_eptr[row + 1] - eb;
+    if (ek > 32 || rn > 255) {
+      if (lane == 0) atomicExch(bad, 1);
+      continue;
+    }
+    for (int s = lane; s < rn; s += 32) s_mask[w][s] = 0u;
+    __syncwarp();
+    if (lane < ek) {
+      const int4 en = reinterpret_cast<const int4*>(m.elem)[m.node_elist[eb + lane]];
+      const int32_t nd[4] = {en.x, en.y, en.z, en.w};
+      uint32_t packed = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int lo = 0, hi = rn - 1, pos = 0;
+        while (lo <= hi) {  // the column is in the row (the pattern holds every tet's nodes)
+          const int mid = (lo + hi) >> 1;
+          const int32_t c = m.indices[rb + mid];
+          if (c == nd[j]) {
+            pos = mid;
+            break;
+          }
+          if (c < nd[j]) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        packed |= (uint32_t)pos << (8 * j);
+        atomicOr(&s_mask[w][pos], 1u << lane);
+      }
+      inc_slot[eb + lane] = packed;
+    }
+    __syncwarp();
+    for (int s = lane; s < rn; s += 32) slot_mask[rb + s] = s_mask[w][s];
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ double shfl_xor_s(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ cdouble shfl_xor_s(cdouble v, int o) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
+
+// Table-driven assembly: one warp per row.  Lane u < ek evaluates the row's
+// u-th incident tet and stages its 4 values; the diagonal (every tet
+// contributes its (li, li) value) is a butterfly sum across the lanes; lane
+// s then owns CSR slot s and sums the staged values of the tets in its
+// contributor mask in ascending tet order.  The slot's column index and
+// mask of the first 32 slots are loaded before the tets, so that their
+// latency overlaps the tet loads.
+template <bool CPLX, int KIND>
+__global__ void __launch_bounds__(kAsmWarps * 32)
+femlhs_tab_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, const double* __restrict__ ddd,
+                  const double* __restrict__ dco, const uint32_t* __restrict__ inc_slot,
+                  const uint32_t* __restrict__ slot_mask, double bc, double wc,
+                  typename AsmVal<CPLX>::T* __restrict__ val64, typename AsmVal<CPLX>::T32* __restrict__ val32,
+                  typename AsmVal<CPLX>::T* __restrict__ dinv64, typename AsmVal<CPLX>::T32* __restrict__ dinv32) {
+  typedef typename AsmVal<CPLX>::T T;
+  __shared__ T s_vals[kAsmWarps][32][4];
+  __shared__ uint32_t s_ps[kAsmWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * kAsmWarps;
+  for (int64_t row = blockIdx.x * (int64_t)kAsmWarps + w; row < m.nn; row += warps) {
+    const int32_t rb = m.indptr[row], rn = m.indptr[row + 1] - rb;
+    const int32_t eb = m.node_eptr[row], ek = m.node_eptr[row + 1] - eb;
+    const int32_t fb = m.node_fptr[row], fk = m.node_fptr[row + 1] - fb;
+    const int32_t col0 = (lane < rn) ? m.indices[rb + lane] : -1;
+    const uint32_t msk0 = (lane < rn) ? slot_mask[rb + lane] : 0u;
+    T d = s_zero(T());
+    if (lane < ek) {
+      const int64_t e = m.node_elist[eb + lane];
+      const uint32_t ps = inc_slot[eb + lane];
+      const int4 en = reinterpret_cast<const int4*>(m.elem)[e];
+      T v[4];
+      tet_row<CPLX, KIND>(m, o, evol, ddd, dco, wc, e, en, row, v);
+      const int li = (en.y == row) ? 1 : (en.z == row) ? 2 : (en.w == row) ? 3 : 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        s_vals[w][lane][j] = v[j];
+        if (j == li) d = v[j];
+      }
+      s_ps[w][lane] = ps;
+    }
+    // diagonal: every incident tet contributes its (li, li) entry
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) d = s_add(d, shfl_xor_s(d, off));
+    __syncwarp();
+    for (int32_t sl = lane; sl < rn; sl += 32) {
+      const int32_t col = (sl == lane) ? col0 : m.indices[rb + sl];
+      T acc = s_zero(T());
+      if (col == row) {
+        acc = d;
+      } else {
+        uint32_t msk = (sl == lane) ? msk0 : slot_mask[rb + sl];
+        while (msk) {
+          const int u = __ffs(msk) - 1;
+          msk &= msk - 1;
+          const uint32_t ps = s_ps[w][u];
+          const int j = ((ps & 255u) == (uint32_t)sl) ? 0 : (((ps >> 8) & 255u) == (uint32_t)sl) ? 1
+                        : (((ps >> 16) & 255u) == (uint32_t)sl) ? 2 : 3;
+          acc = s_add(acc, s_vals[w][u][j]);
+        }
+      }
+      // Robin boundary: area*bc on the diagonal, half of it off the diagonal
+      for (int32_t t = 0; t < fk; ++t) {
+        const int32_t f = m.node_flist[fb + t];
+        const double a = m.area[f] * bc;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int32_t nq = m.face[3 * (int64_t)f + q];
+          if (nq == col) add_real(acc, (nq == row) ? a : 0.5 * a);
+        }
+      }
+      val64[rb + sl] = acc;
+      if (val32) val32[rb + sl] = narrow(acc);
+      if (col == row) {
+        const T r = recip(acc);
+        if (dinv64) dinv64[row] = r;
+        if (dinv32) dinv32[row] = narrow(r);
+      }
+    }
+    __syncwarp();  // the staged values are rewritten for the next row
+  }
+}
+
 template <bool CPLX, int KIND>
 int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, const double* ddd, double* dco,
                   void* v64, void* v32, void* d64, void* d32, cudaStream_t st) {
@@ -211,8 +347,12 @@ int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, cons
   dcoeff_kernel<<<(unsigned)std::min<int64_t>(ceil_div(np, 256), 148 * 16), 256, 0, st>>>(np, o.mua, o.musp, dco);
   RB_LAUNCH_CHECK();
   unsigned g = (unsigned)std::min<int64_t>(ceil_div(m.nn, kAsmWarps), 148 * 64);
-  femlhs_rows_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, bc, wc, (T*)v64, (T32*)v32,
-                                                                 (T*)d64, (T32*)d32);
+  if (m.inc_slot && m.slot_mask)
+    femlhs_tab_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, m.inc_slot, m.slot_mask, bc,
+                                                                  wc, (T*)v64, (T32*)v32, (T*)d64, (T32*)d32);
+  else
+    femlhs_rows_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, bc, wc, (T*)v64, (T32*)v32,
+                                                                   (T*)d64, (T32*)d32);
   RB_LAUNCH_CHECK();
   return RB_OK;
 }
@@ -220,6 +360,30 @@ int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, cons
 }  // namespace rb
 
 using namespace rb;
+
+extern "C" int rb_assembly_tables(const rb_mesh* mesh, uint32_t* inc_slot, uint32_t* slot_mask, int32_t* usable,
+                                  void* stream) {
+  if (!mesh || !inc_slot || !slot_mask || !usable || mesh->nn < 1)
+    return fail(RB_EARG, "rb_assembly_tables: bad arguments");
+  const rb_mesh& m = *mesh;
+  if (!m.elem || !m.indptr || !m.indices || !m.node_eptr || !m.node_elist)
+    return fail(RB_EARG, "rb_assembly_tables: mesh arrays missing");
+  cudaStream_t st = as_stream(stream);
+  int32_t* bad = nullptr;
+  RB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&bad), sizeof(int32_t), st));
+  RB_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
+  unsigned g = (unsigned)std::min<int64_t>(ceil_div(m.nn, kAsmWarps), 148 * 64);
+  asm_tables_kernel<<<g, kAsmWarps * 32, 0, st>>>(m, inc_slot, slot_mask, bad);
+  const cudaError_t le = cudaGetLastError();
+  int32_t hb = 1;
+  const cudaError_t ce = cudaMemcpyAsync(&hb, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(bad, st);
+  RB_CUDA_TRY(le);
+  RB_CUDA_TRY(ce);
+  RB_CUDA_TRY(cudaStreamSynchronize(st));
+  *usable = hb == 0;
+  return RB_OK;
+}
 
 extern "C" size_t rb_femlhs_work_bytes(int64_t nn, int64_t ne) {
   return (size_t)std::max(nn, ne) * sizeof(double) + 256;

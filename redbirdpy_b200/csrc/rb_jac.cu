@@ -64,6 +64,7 @@ struct JacArgs {
   int64_t nsd, ld, ldj;
   int32_t rmax, emax, what;
   int32_t grid;  // pairs are all (source slot, detector) combinations, detector-major
+  int64_t node0;  // first node of the range (J column 0); nn is the range's end
 };
 
 // Per-node strides of the staged phi and C blocks, padded so that the TN
@@ -148,7 +149,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   const int warp = tid_warp(), lane = threadIdx.x & 31;
   constexpr int kWarps = kJacThreads / 32;
 
-  const int64_t n0 = (int64_t)blockIdx.x * TN;
+  const int64_t n0 = a.node0 + (int64_t)blockIdx.x * TN;
   const int tid = threadIdx.x;
   // 1. rows and incident tets of the TN nodes
   if (tid < TN) {
@@ -288,7 +289,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int64_t k = (int64_t)(db * 4 + v) * nsu + sb * 4 + u;
-          jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n, acc[u][v]);
+          jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n - a.node0, acc[u][v]);
         }
     }
     return;
@@ -307,7 +308,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
     // complex rows are split into a block of real parts and a block of
     // imaginary parts (matreform 'real', recon.py:532-546)
-    jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n, s);
+    jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n - a.node0, s);
   }
 }
 
@@ -344,7 +345,7 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
   while (TN > 1 && jac_smem<C>(TN, a.rmax, a.nc, a.ndet, a.emax) > budget) TN >>= 1;
   const size_t sm = jac_smem<C>(TN, a.rmax, a.nc, a.ndet, a.emax);
   if (sm > 200 * 1024) return fail(RB_ESIZE, "rb_jac: staging needs %zu bytes of shared memory", sm);
-  const unsigned g = (unsigned)ceil_div(a.nn, TN);
+  const unsigned g = (unsigned)ceil_div(a.nn - a.node0, TN);
 #define RB_JL(TN_)                                                                                     \
   do {                                                                                                 \
     RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID, BF>,                          \
@@ -419,19 +420,21 @@ int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, co
 }
 
 
-int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
-            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
-            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind, int32_t rmax,
-            int32_t emax, const double* evol, const double* ddd, void* stream) {
+int rb_jac_range(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
+                 const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
+                 const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind, int32_t rmax,
+                 int32_t emax, const double* evol, const double* ddd, int64_t node0, int64_t count,
+                 void* stream) {
   if (!mesh || !phi || !cols || !pair_src || !pair_det || !J || !evol) return fail(RB_EARG, "rb_jac: null argument");
   if (what == JAC_D && !ddd) return fail(RB_EARG, "rb_jac: RB_JAC_D needs deldotdel");
   if (what < JAC_MUA_REF || what > JAC_D) return fail(RB_EARG, "rb_jac: bad quantity");
-  if (nc < 1 || ndet < 1 || det0 < 0 || det0 + ndet > nc || ldj < mesh->nn)
+  if (node0 < 0 || count < 0 || node0 + count > mesh->nn) return fail(RB_EARG, "rb_jac: node range outside the mesh");
+  if (nc < 1 || ndet < 1 || det0 < 0 || det0 + ndet > nc || ldj < count)
     return fail(RB_EARG, "rb_jac: bad column map");
   if (rmax < 1 || rmax > 64 || emax < 1 || emax > 256) return fail(RB_ESIZE, "rb_jac: rmax/emax out of range");
-  if (nsd == 0) return RB_OK;
-  JacArgs a{mesh->indptr, mesh->indices, mesh->node_eptr, mesh->node_elist, mesh->elem, evol, ddd, mesh->nn,
-            cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what, 0};
+  if (nsd == 0 || count == 0) return RB_OK;
+  JacArgs a{mesh->indptr, mesh->indices, mesh->node_eptr, mesh->node_elist, mesh->elem, evol, ddd, node0 + count,
+            cols, nc, det0, ndet, pair_src, pair_det, nsd, ld, ldj, rmax, emax, what, 0, node0};
   // the blocked path needs the full detector-major grid of sources x detectors
   // with both counts multiple of 4; the caller flags it through nsd < 0
   if (nsd < 0) {
@@ -473,6 +476,15 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
     case RB_C128 * 4 + RB_C128: return launch_jac<cdouble, cdouble>(a, phi, J, st);
     default: return fail(RB_EARG, "rb_jac: bad kinds");
   }
+}
+
+int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
+           const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
+           const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind, int32_t rmax,
+           int32_t emax, const double* evol, const double* ddd, void* stream) {
+  if (!mesh) return fail(RB_EARG, "rb_jac: null argument");
+  return rb_jac_range(mesh, what, phi, phi_kind, ld, cols, nc, det0, ndet, pair_src, pair_det, nsd, J, ldj,
+                      out_kind, rmax, emax, evol, ddd, 0, mesh->nn, stream);
 }
 
 int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,

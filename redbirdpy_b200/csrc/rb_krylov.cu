@@ -1247,14 +1247,22 @@ __global__ void fin_outer_kernel(int64_t k, int nb, const double* part, OuterSta
   if (o.active) atomicAdd(nactive, 1);
 }
 
+// The state that scales row `i`'s entry of column c: the column's own, or
+// with stacked instances (rinst given) that of the row's (instance, column)
+__device__ __forceinline__ const OuterState& row_state(const OuterState* os, const int32_t* __restrict__ rinst,
+                                                       int64_t i, int64_t k, int64_t c) {
+  return rinst ? os[(int64_t)rinst[i / k] * k + c] : os[c];
+}
+
 // r_inner = T(R64 * scale) for active columns, 0 elsewhere
 template <typename T64, typename T>
 __global__ void cast_scale_kernel(int64_t n, int64_t k, const T64* __restrict__ R64, const OuterState* os,
-                                  T* __restrict__ R) {
+                                  const int32_t* __restrict__ rinst, T* __restrict__ R) {
   const int64_t total = n * k;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = i % k;
-    const double s = os[c].active ? os[c].scale : 0.0;
+    const OuterState& o = row_state(os, rinst, i, k, c);
+    const double s = o.active ? o.scale : 0.0;
     T64 v = R64[i];
     if constexpr (Scalar<T>::is_complex) {
       R[i] = T{(typename Scalar<T>::real)(v.x * s), (typename Scalar<T>::real)(v.y * s)};
@@ -1267,12 +1275,13 @@ __global__ void cast_scale_kernel(int64_t n, int64_t k, const T64* __restrict__ 
 // X64 += D / scale for active columns
 template <typename T64, typename T>
 __global__ void correct_kernel(int64_t n, int64_t k, const T* __restrict__ D, const OuterState* os,
-                               T64* __restrict__ X) {
+                               const int32_t* __restrict__ rinst, T64* __restrict__ X) {
   const int64_t total = n * k;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = i % k;
-    if (!os[c].active) continue;
-    const double inv = 1.0 / os[c].scale;
+    const OuterState& o = row_state(os, rinst, i, k, c);
+    if (!o.active) continue;
+    const double inv = 1.0 / o.scale;
     T d = D[i];
     if constexpr (Scalar<T>::is_complex) {
       X[i].x += (double)d.x * inv;
@@ -1281,6 +1290,150 @@ __global__ void correct_kernel(int64_t n, int64_t k, const T* __restrict__ D, co
       X[i] += (double)d * inv;
     }
   }
+}
+
+constexpr int64_t kMaxCols = 128;  // columns per Krylov block
+
+// ------------------------------------------- stacked independent instances
+// With a batch of independent systems stacked block-diagonally, the
+// refinement keeps one OuterState per (instance, column): each instance is
+// tested against its own ||b_i||, its correction right-hand side is scaled
+// to unit norm on its own rows, and it stops being corrected once its
+// columns are done, whatever the other instances do.  The inner Krylov
+// sweep still runs on whole columns; its per-column state is the summary
+// of the column's instances (active if any is, the tightest inner tolerance).
+
+__device__ __forceinline__ double sq_abs(double v) { return v * v; }
+__device__ __forceinline__ double sq_abs(cdouble v) { return v.x * v.x + v.y * v.y; }
+
+// out[i * k + c] = sum over instance i's rows of |X[r][c]|^2: one block per
+// instance, warps over rows, lanes over columns, summed in a fixed order
+constexpr int kSegWarps = 8;
+template <typename T64>
+__global__ void __launch_bounds__(kSegWarps * 32)
+seg_norm_kernel(int64_t ninst, int64_t k, const int64_t* __restrict__ row_ptr, const T64* __restrict__ X,
+                double* __restrict__ out) {
+  __shared__ double sm[kSegWarps][kMaxCols];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t i = blockIdx.x; i < ninst; i += gridDim.x) {
+    double a[kMaxCols / 32];
+#pragma unroll
+    for (int q = 0; q < kMaxCols / 32; ++q) a[q] = 0.0;
+    const int64_t r1 = row_ptr[i + 1];
+    for (int64_t r = row_ptr[i] + w; r < r1; r += kSegWarps) {
+      const T64* xr = X + r * k;
+#pragma unroll
+      for (int q = 0; q < kMaxCols / 32; ++q)
+        if (lane + 32 * q < k) a[q] += sq_abs(xr[lane + 32 * q]);
+    }
+#pragma unroll
+    for (int q = 0; q < kMaxCols / 32; ++q)
+      if (lane + 32 * q < k) sm[w][lane + 32 * q] = a[q];
+    __syncthreads();
+    for (int64_t c = threadIdx.x; c < k; c += blockDim.x) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < kSegWarps; ++q) t += sm[q][c];
+      out[i * k + c] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void seg_bnorm_kernel(int64_t m, const double* __restrict__ s2, OuterState* __restrict__ seg) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const double s = s2[j];
+  OuterState o;
+  o.bnorm = sqrt(s);
+  o.relres = (s > 0.0) ? 1e300 : 0.0;
+  o.prev = 1e300;
+  o.scale = 0.0;
+  o.itol2 = -1.0;
+  o.active = s > 0.0;
+  o.done = (s > 0.0) ? 0 : 1;
+  seg[j] = o;
+}
+
+// the rules of fin_outer_kernel, per (instance, column)
+__global__ void seg_outer_kernel(int64_t m, const double* __restrict__ s2, OuterState* __restrict__ seg, double tol,
+                                 double stall, double inner_tol, double itol_min) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= m || !seg[j].active) return;
+  const double s = s2[j];
+  OuterState o = seg[j];
+  const double rel = sqrt(s) / o.bnorm;
+  o.prev = o.relres;
+  o.relres = rel;
+  if (!isfinite(rel)) {
+    o.active = 0;
+    o.done = 3;
+  } else if (!(rel > tol)) {
+    o.active = 0;
+    o.done = 1;
+  } else if (rel > stall * o.prev) {
+    o.active = 0;
+    o.done = 2;
+  } else {
+    o.scale = 1.0 / sqrt(s);
+    double it = inner_tol;
+    if (rel * inner_tol < 10.0 * tol) it = fmax(fmin(inner_tol, 1e-2 * tol / rel), itol_min);
+    o.itol2 = it * it;
+  }
+  seg[j] = o;
+}
+
+// column summary of the instances' states; counts the active columns
+__global__ void seg_summary_kernel(int64_t ninst, int64_t k, const OuterState* __restrict__ seg,
+                                   OuterState* __restrict__ os, int32_t* __restrict__ nactive) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= k) return;
+  OuterState o;
+  o.bnorm = 0.0;
+  o.relres = 0.0;
+  o.prev = 0.0;
+  o.scale = 1.0;
+  o.itol2 = -1.0;
+  o.active = 0;
+  bool nonfinite = false, open = false, stalled = false;
+  for (int64_t i = 0; i < ninst; ++i) {
+    const OuterState& q = seg[i * k + c];
+    if (isfinite(q.relres)) o.relres = fmax(o.relres, q.relres);
+    else nonfinite = true;
+    nonfinite |= q.done == 3;
+    open |= q.done == 0;
+    stalled |= q.done == 2;
+    if (q.active) {
+      o.itol2 = o.active ? fmin(o.itol2, q.itol2) : q.itol2;
+      o.active = 1;
+    }
+  }
+  // the column's worst instance: non-finite, still open, stalled, converged
+  o.done = nonfinite ? 3 : open ? 0 : stalled ? 2 : 1;
+  if (nonfinite) o.relres = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  os[c] = o;
+  if (o.active) atomicAdd(nactive, 1);
+}
+
+// per-instance outcome: 0 converged, 1 not converged within the caps,
+// 2 Krylov breakdown, 3 non-finite residual; relres per (instance, column)
+__global__ void seg_status_kernel(int64_t ninst, int64_t k, int64_t ncol, const OuterState* __restrict__ seg,
+                                  const ColState* __restrict__ cs, const int32_t* __restrict__ counter,
+                                  int32_t* __restrict__ status, double* __restrict__ relres) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ninst) return;
+  // 4: a bounded in-kernel wait of the SpMM gave up (results not valid)
+  int32_t st = counter[2] ? 4 : 0;
+  for (int64_t c = 0; c < ncol; ++c) {
+    const OuterState& q = seg[i * k + c];
+    if (relres) relres[i * ncol + c] = q.relres;
+    int32_t v = 0;
+    if (q.done == 3) v = 3;
+    else if (cs[c].status == 2 && q.relres > 1e-10 && q.done != 1) v = 2;
+    else if (q.done == 0 || (q.done == 2 && q.relres > 1e-10)) v = 1;
+    st = max(st, v);
+  }
+  status[i] = st;
 }
 
 // squared column norms of a real FP64 n x k array
@@ -1521,8 +1674,6 @@ struct Carver {
   }
 };
 
-constexpr int64_t kMaxCols = 128;  // columns per Krylov block
-
 template <typename T64, typename T>
 struct SolveBufs {
   T64* R64;
@@ -1540,6 +1691,19 @@ struct SolveBufs {
   void* scan_work;
   size_t scan_bytes;
 };
+
+// per-(instance, column) refinement state of a stacked batch
+struct SegBufs {
+  const rb_instances* in = nullptr;
+  int64_t ncol = 0;        // the caller's columns (relres layout)
+  double* s2 = nullptr;    // ninst x k squared norms
+  OuterState* seg = nullptr;  // ninst x k
+};
+static size_t seg_carve(Carver& cv, SegBufs& sb, int64_t ninst, int64_t k) {
+  sb.s2 = cv.take<double>(ninst * k);
+  sb.seg = cv.take<OuterState>(ninst * k);
+  return cv.used;
+}
 
 template <typename T64, typename T>
 static size_t carve(Carver& cv, SolveBufs<T64, T>& b, int64_t n, int64_t nnz, int64_t k) {
@@ -1757,6 +1921,13 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
   // no GPU time.  The burst queued after the converged one runs as no-ops.
   // With per-kernel timing on, bursts are read one at a time (the timer's
   // events are harvested at each read).
+  if (check_every == 0) {
+    // fixed budget: every iteration is queued and none is read back; the
+    // kernels of iterations after convergence return at once (live == 0)
+    RB_TRY(enqueue_burst(maxiter));
+    *iters_out = maxiter;
+    return RB_OK;
+  }
   BurstSync bs;
   RB_TRY(bs.init());
   int it = 0, pend = -1, pend_it = 0, next_snap = 0;
@@ -1798,7 +1969,8 @@ static int inner_solve(const rb_csr& A, const T* val, const T* dinv, int64_t k, 
 template <typename T64, typename T>
 static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, int64_t k, const rb_solve_opts& o,
                        rb_solve_info& info, SolveBufs<T64, T>& b, const T* val, const T* dinv,
-                       const GroupPlan* gp, const RowGroupsDev* rg, const CoarseOp<T>* co, cudaStream_t st) {
+                       const GroupPlan* gp, const RowGroupsDev* rg, const CoarseOp<T>* co, const SegBufs& sb,
+                       cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
   const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
@@ -1817,9 +1989,22 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
   fin_bnorm_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os);
   if (!o.use_x0) RB_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(T64) * n * k, st));
   launches += 2;
+  const bool segm = sb.in != nullptr;
+  const int64_t ninst = segm ? sb.in->ninst : 0, nseg = ninst * k;
+  const unsigned sgg = (unsigned)std::min<int64_t>(std::max<int64_t>(ninst, 1), 148 * 8);
+  const unsigned sgm = (unsigned)ceil_div(std::max<int64_t>(nseg, 1), 256);
+  const int32_t* rinst = segm ? sb.in->row_inst : nullptr;
+  const OuterState* scale_state = segm ? sb.seg : b.os;
+  if (segm) {
+    seg_norm_kernel<double><<<sgg, kSegWarps * 32, 0, st>>>(ninst, k, sb.in->row_ptr, B, sb.s2);
+    seg_bnorm_kernel<<<sgm, 256, 0, st>>>(nseg, sb.s2, sb.seg);
+    RB_LAUNCH_CHECK();
+    launches += 2;
+  }
   const double stall = 0.25;
+  const bool budget = o.check_every == 0;
   KernelTimer tm;
-  tm.on = o.profile != 0;
+  tm.on = o.profile != 0 && !budget;
   tm.with_coarse = o.coarse != nullptr;
   int total_iters = 0, outer = 0;
   int sweep_flag = 0;
@@ -1827,16 +2012,29 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     // R64 = B - A X (FP64)
     RB_TRY((spmm_t<T64, EPI_RESID>(A, (const T64*)A.val64, X, b.R64, B, b.part_b, k, sh64, st)));
     RB_CUDA_TRY(cudaMemsetAsync(b.counter + 1, 0, sizeof(int32_t), st));
-    fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os, o.tol, stall, o.inner_tol,
-                                         sizeof(T) == sizeof(T64) ? o.inner_tol : std::min(o.inner_tol, 1e-6),
-                                         b.counter + 1);
+    const double itol_min = sizeof(T) == sizeof(T64) ? o.inner_tol : std::min(o.inner_tol, 1e-6);
+    if (segm) {
+      seg_norm_kernel<T64><<<sgg, kSegWarps * 32, 0, st>>>(ninst, k, sb.in->row_ptr, b.R64, sb.s2);
+      seg_outer_kernel<<<sgm, 256, 0, st>>>(nseg, sb.s2, sb.seg, o.tol, stall, o.inner_tol, itol_min);
+      seg_summary_kernel<<<(unsigned)ceil_div(k, 128), 128, 0, st>>>(ninst, k, sb.seg, b.os, b.counter + 1);
+      launches += 2;
+    } else {
+      fin_outer_kernel<<<fg, 256, 0, st>>>(k, (int)sh64.grid, b.part_b, b.os, o.tol, stall, o.inner_tol, itol_min,
+                                           b.counter + 1);
+    }
     RB_LAUNCH_CHECK();
     launches += 2;
-    int32_t nact = 0;
-    RB_CUDA_TRY(cudaMemcpyAsync(&nact, b.counter + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    RB_CUDA_TRY(cudaStreamSynchronize(st));
-    if (nact == 0 || outer == o.max_outer) break;
-    cast_scale_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.R64, b.os, b.R);
+    if (budget) {
+      // fixed budget: max_outer sweeps, none read back; a done column's
+      // cast, solve and correction are no-ops
+      if (outer == o.max_outer) break;
+    } else {
+      int32_t nact = 0;
+      RB_CUDA_TRY(cudaMemcpyAsync(&nact, b.counter + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      RB_CUDA_TRY(cudaStreamSynchronize(st));
+      if (nact == 0 || outer == o.max_outer) break;
+    }
+    cast_scale_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.R64, scale_state, rinst, b.R);
     RB_LAUNCH_CHECK();
     launches += 1;
     int it = 0;
@@ -1844,10 +2042,25 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
                           b.os, b.counter, o.inner_tol, o.maxiter, o.check_every, &it, &launches, tm, gp, rg,
                           co, st));
     total_iters += it;
+    info.sweep_iters_max = std::max(info.sweep_iters_max, it);
     if (it >= o.maxiter) sweep_flag = 1;
-    correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, b.os, X);
+    correct_kernel<T64, T><<<eg, 256, 0, st>>>(n, k, b.Xs, scale_state, rinst, X);
     RB_LAUNCH_CHECK();
     launches += 1;
+  }
+  if (segm) {
+    seg_status_kernel<<<(unsigned)ceil_div(ninst, 128), 128, 0, st>>>(ninst, k, sb.ncol, sb.seg, b.cs, b.counter,
+                                                                       sb.in->status, sb.in->relres);
+    RB_LAUNCH_CHECK();
+    launches += 1;
+  }
+  if (budget) {  // nothing is read back: the outcome is in the status words
+    info.iters += outer * o.maxiter;
+    info.outer = std::max(info.outer, outer);
+    info.flag = -1;
+    info.launches += launches;
+    info.relres = -1.0;
+    return RB_OK;
   }
   // summary
   int32_t hcnt[4] = {0, 0, 0, 0};
@@ -1866,6 +2079,13 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
     if ((hcs[c].status == 2 && hos[c].relres > 1e-10) || hos[c].done == 3) flag = 2;
   }
   if (flag == 1 && sweep_flag == 0 && worst <= o.tol) flag = 0;
+  if (segm) {  // the flag of the worst instance
+    std::vector<int32_t> hst(ninst);
+    RB_CUDA_TRY(cudaMemcpyAsync(hst.data(), sb.in->status, sizeof(int32_t) * ninst, cudaMemcpyDeviceToHost, st));
+    RB_CUDA_TRY(cudaStreamSynchronize(st));
+    flag = 0;
+    for (int32_t v : hst) flag = std::max(flag, v >= 2 ? 2 : v);
+  }
   info.iters += total_iters;
   info.outer = std::max(info.outer, outer);
   info.flag = std::max(info.flag, flag);
@@ -1907,6 +2127,13 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     if (!cb.A64 || !cb.Rb || !cb.Cb || !cb.Dinv || !cb.op.X || !cb.op.rc || !cb.op.ec || !cb.op.part || !cb.err)
       return fail(RB_EARG, "rb_femsolve: workspace too small for the coarse space");
   }
+  SegBufs sb;
+  if (o.instances) {
+    sb.in = o.instances;
+    sb.ncol = nrhs;
+    seg_carve(cv, sb, o.instances->ninst, kb);
+    if (!sb.s2 || !sb.seg) return fail(RB_EARG, "rb_femsolve: workspace too small for the instances");
+  }
   RB_CUDA_TRY(cudaMemsetAsync(b.counter, 0, 8 * sizeof(int32_t), st));
   if (o.coarse) {
     RB_TRY((coarse_setup<T64, T>(A, cb, st)));
@@ -1938,7 +2165,7 @@ static int femsolve_t(const rb_csr& A, const double* B, T64* X, int64_t nrhs, co
     }
   }
   RB_TRY((solve_block<T64, T>(A, Bp ? Bp : B, Xp ? Xp : X, kb, kb, o, info, b, val, dinv, gp.ng ? &gp : nullptr,
-                              use_rg ? &rgd : nullptr, o.coarse ? &cb.op : nullptr, st)));
+                              use_rg ? &rgd : nullptr, o.coarse ? &cb.op : nullptr, sb, st)));
   if (Xp) {
     copy_cols_kernel<T64><<<eg, 256, 0, st>>>(n, kb, nrhs, Xp, X);
     RB_LAUNCH_CHECK();
@@ -2003,6 +2230,14 @@ size_t rb_femsolve_work_bytes(int64_t n, int64_t nnz, int64_t nrhs, int32_t is_c
   return bytes + 4096;
 }
 
+size_t rb_instances_work_bytes(int64_t ninst, int64_t nrhs) {
+  if (ninst < 1) return 0;
+  const int64_t k = solve_cols(std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols));
+  Carver cv{nullptr, 0};
+  SegBufs sb;
+  return seg_carve(cv, sb, ninst, k) + 512;
+}
+
 size_t rb_coarse_work_bytes(int64_t nc, int64_t nrhs, int32_t is_complex, int32_t precision) {
   const int64_t k = solve_cols(std::min<int64_t>(std::max<int64_t>(nrhs, 1), kMaxCols));
   Carver cv{nullptr, 0};
@@ -2026,14 +2261,23 @@ int rb_femsolve(const rb_csr* A, const double* B, void* X, int64_t nrhs, const r
   if (o.precision != RB_MIXED && o.precision != RB_FP64) return fail(RB_EARG, "rb_femsolve: bad precision");
   if (!A->val64 || !A->dinv64 || !A->indptr || !A->indices) return fail(RB_EARG, "rb_femsolve: matrix arrays missing");
   if (o.precision == RB_MIXED && (!A->val32 || !A->dinv32)) return fail(RB_EARG, "rb_femsolve: mixed precision needs val32/dinv32");
-  if (o.maxiter < 1 || o.check_every < 1 || o.max_outer < 1 || !(o.tol > 0) || !(o.inner_tol > 0))
+  if (o.maxiter < 1 || o.check_every < 0 || o.max_outer < 1 || !(o.tol > 0) || !(o.inner_tol > 0))
     return fail(RB_EARG, "rb_femsolve: bad options");
+  if (o.check_every == 0 && (!o.instances || o.coarse))
+    return fail(RB_EARG, "rb_femsolve: a fixed budget (check_every 0) needs instances (the status words) "
+                         "and no coarse space");
   size_t need = rb_femsolve_work_bytes(A->n, A->nnz, nrhs, A->is_complex, o.precision);
   if (o.coarse) {
     const rb_coarse& c = *o.coarse;
     if (c.nc < 1 || c.nc > kCoarseMax || c.nc > A->n || !c.agg || !c.agg_ptr || !c.agg_rows)
       return fail(RB_EARG, "rb_femsolve: coarse space needs 1 <= nc <= min(n, %d) and its three arrays", kCoarseMax);
     need += rb_coarse_work_bytes(c.nc, nrhs, A->is_complex, o.precision);
+  }
+  if (o.instances) {
+    const rb_instances& in = *o.instances;
+    if (in.ninst < 1 || !in.row_ptr || !in.row_inst || !in.status)
+      return fail(RB_EARG, "rb_femsolve: instances need ninst >= 1, row_ptr, row_inst and status");
+    need += rb_instances_work_bytes(in.ninst, nrhs);
   }
   if (work_bytes < need) return fail(RB_EARG, "rb_femsolve: workspace too small");
   *info = rb_solve_info{};

@@ -88,6 +88,17 @@ class DeviceMesh:
             self.nn, self.ne, self.nf, self.nnz, self.node.data_ptr(), self.elem.data_ptr(),
             self.face.data_ptr(), self.area.data_ptr(), self.eptr.data_ptr(), self.elist.data_ptr(),
             self.fptr.data_ptr(), self.flist.data_ptr(), self.indptr.data_ptr(), self.indices.data_ptr())
+        # per-entry contributor tables of the assembly (4*ne + nnz words)
+        self.inc_slot = torch.empty(max(4 * self.ne, 1), dtype=torch.int32, device=dev)
+        self.slot_mask = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        usable = ctypes.c_int32(0)
+        call("rb_assembly_tables", ctypes.byref(self.struct), ptr(self.inc_slot), ptr(self.slot_mask),
+             ctypes.byref(usable), st)
+        if usable.value:
+            self.struct.inc_slot = self.inc_slot.data_ptr()
+            self.struct.slot_mask = self.slot_mask.data_ptr()
+        else:
+            self.inc_slot = self.slot_mask = None
 
     def _incidence(self, cells, nv, ncell, st):
         p = torch.empty(self.nn + 1, dtype=torch.int32, device=self.device)
@@ -268,7 +279,10 @@ class Optics:
             raise ValueError("Property format not recognized")
         self.mua = mua if isinstance(mua, torch.Tensor) else _f64(mua, dev)
         self.musp = musp if isinstance(musp, torch.Tensor) else _f64(musp, dev)
-        if np.ndim(nref) > 0 and len(nref) == len(mua):
+        if isinstance(nref, torch.Tensor) and nref.numel() == len(mua):
+            self.nref = nref  # already on the device (kept by the caller across calls)
+            self.nref_scalar = 0.0
+        elif np.ndim(nref) > 0 and len(nref) == len(mua):
             self.nref = _f64(nref, dev)
             self.nref_scalar = 0.0
         else:
@@ -366,9 +380,11 @@ class DeviceMatrix:
         return m
 
 
-def assemble(mesh, optics, ddd=None, evol=None):
+def assemble(mesh, optics, ddd=None, evol=None, tables=True):
     """femlhs on the device -> DeviceMatrix (redbirdpy/forward.py:90-256).
-    ``ddd``/``evol`` default to the mesh's own deldotdel rows and volumes."""
+    ``ddd``/``evol`` default to the mesh's own deldotdel rows and volumes;
+    ``tables=False`` assembles without the mesh's contributor tables (the
+    scan of every incident tet per entry)."""
     dev = mesh.device
     ddd = mesh.ddd if ddd is None else ddd
     evol = mesh.evol if evol is None else evol
@@ -381,7 +397,11 @@ def assemble(mesh, optics, ddd=None, evol=None):
     d32 = torch.empty(mesh.nn, dtype=t32, device=dev)
     wb = _lib.lib().rb_femlhs_work_bytes(mesh.nn, mesh.ne)
     work = torch.empty(wb, dtype=torch.uint8, device=dev)
-    call("rb_femlhs", ctypes.byref(mesh.struct), ctypes.byref(optics.struct), ptr(evol), ptr(ddd), ptr(v64), ptr(v32),
+    ms = mesh.struct
+    if not tables:
+        ms = _lib.RbMesh.from_buffer_copy(mesh.struct)
+        ms.inc_slot = ms.slot_mask = None
+    call("rb_femlhs", ctypes.byref(ms), ctypes.byref(optics.struct), ptr(evol), ptr(ddd), ptr(v64), ptr(v32),
          ptr(d64), ptr(d32), ptr(work), wb, stream())
     return DeviceMatrix(mesh, cplx, v64, v32, d64, d32)
 
@@ -633,8 +653,33 @@ def _resolve_coarse(mat, coarse):
     raise ValueError(f"coarse: unsupported value {coarse!r}")
 
 
+class Instances:
+    """Independent systems stacked block-diagonally (a batch): instance i
+    owns rows row_off[i] .. row_off[i+1]-1.  solve(instances=...) then tests
+    convergence per (instance, column) and reports each instance's outcome."""
+
+    def __init__(self, row_off, device):
+        row_off = np.asarray(row_off, dtype=np.int64)
+        if row_off.ndim != 1 or row_off.size < 2 or row_off[0] != 0 or np.any(np.diff(row_off) < 0):
+            raise ValueError("instances: row offsets must start at 0 and not decrease")
+        self.ninst = row_off.size - 1
+        self.n = int(row_off[-1])
+        self.row_ptr = torch.as_tensor(row_off, device=device)
+        self.row_inst = torch.as_tensor(np.repeat(np.arange(self.ninst, dtype=np.int32), np.diff(row_off)),
+                                        device=device)
+        self.status = torch.empty(self.ninst, dtype=torch.int32, device=device)
+
+    def struct(self, relres):
+        return _lib.RbInstances(self.ninst, self.row_ptr.data_ptr(), self.row_inst.data_ptr(),
+                                self.status.data_ptr(), relres.data_ptr())
+
+
+# per-instance outcome codes of solve(instances=...)
+INSTANCE_STATUS = {0: "converged", 1: "iteration cap", 2: "breakdown", 3: "non-finite"}
+
+
 def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=2000, max_outer=10,
-          check_every=10, profile=False, x0=None, coarse="auto", groups="auto"):
+          check_every=10, profile=False, x0=None, coarse="auto", groups="auto", instances=None, budget=None):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
     Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
@@ -648,7 +693,15 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
     1e-5 with a coarse space and 1e-4 without: on the 520k-node box at 128
     columns, 1e-5 took 3 sweeps / 130 iterations / 113.5 ms against 4 / 150 /
     129.3 ms at 1e-4 and 3 / 150 / 128.6 ms at 1e-6, while Jacobi alone is
-    fastest at 1e-4."""
+    fastest at 1e-4.  ``instances`` (an Instances over the matrix's rows):
+    convergence per (instance, column); info then holds ``inst_status``
+    (ninst, codes of INSTANCE_STATUS) and ``inst_relres`` (ninst x k).
+    ``budget=(sweeps, iterations)``: a fixed budget with no host check or
+    read-back (nothing synchronises, so the call can be captured into a CUDA
+    graph); columns that converge early turn the rest into no-ops.  It
+    needs ``instances`` (one covering all rows is made when None) and no
+    coarse space; ``inst_status`` / ``inst_relres`` are then device tensors
+    and ``flag`` is None until read."""
     prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
     n, k = B.shape
     xdt = torch.complex128 if mat.is_complex else torch.float64
@@ -660,18 +713,31 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
         X = torch.empty((n, k), dtype=xdt, device=B.device)
     info = {"iters": 0, "outer": 0, "flag": 0, "launches": 0, "relres": 0.0, "spmm_ms": 0.0, "update_ms": 0.0,
             "spmm_launches": 0, "update_launches": 0, "coarse_ms": 0.0, "coarse_launches": 0}
+    if budget is not None:
+        max_outer, maxiter = int(budget[0]), int(budget[1])
+        check_every = 0
+        coarse = False
+        if instances is None:
+            instances = Instances([0, n], B.device)
     cs = _resolve_coarse(mat, coarse)
     if inner_tol is None:
         inner_tol = 1e-5 if cs is not None else 1e-4
     if prec == _lib.RB_FP64 and inner_tol > 1e-6:
         inner_tol = max(tol, 1e-15)
     rg = _resolve_groups(mat, groups) if prec == _lib.RB_MIXED else None
+    if instances is not None and instances.n != n:
+        raise ValueError("instances do not cover the matrix's rows")
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
                             int(bool(profile)), int(x0 is not None),
                             ctypes.pointer(cs.struct) if cs is not None else None,
-                            ctypes.pointer(rg.struct) if rg is not None else None)
+                            ctypes.pointer(rg.struct) if rg is not None else None, None)
+    inst_status, inst_relres = [], []
     for c0 in range(0, k, 128):
         kb = min(128, k - c0)
+        if instances is not None:
+            rel = torch.empty((instances.ninst, kb), dtype=torch.float64, device=B.device)
+            ist = instances.struct(rel)
+            opts.instances = ctypes.pointer(ist)
         Bb = B[:, c0:c0 + kb].contiguous() if (c0 or kb != k) else B
         if c0 or kb != k:
             Xb = X[:, c0:c0 + kb].contiguous() if x0 is not None else torch.empty((n, kb), dtype=xdt, device=B.device)
@@ -680,6 +746,8 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
         wb = _lib.lib().rb_femsolve_work_bytes(n, mat.struct.nnz, kb, int(mat.is_complex), prec)
         if cs is not None:
             wb += _lib.lib().rb_coarse_work_bytes(cs.nc, kb, int(mat.is_complex), prec)
+        if instances is not None:
+            wb += _lib.lib().rb_instances_work_bytes(instances.ninst, kb)
         work = torch.empty(wb, dtype=torch.uint8, device=B.device)
         inf = _lib.RbSolveInfo()
         call("rb_femsolve", ctypes.byref(mat.struct), ptr(Bb), ptr(Xb), kb, ctypes.byref(opts), ctypes.byref(inf),
@@ -688,12 +756,29 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
             X[:, c0:c0 + kb] = Xb
         info["iters"] += inf.iters
         info["outer"] = max(info["outer"], inf.outer)
-        info["flag"] = max(info["flag"], inf.flag)
+        info["flag"] = max(info["flag"], inf.flag) if info["flag"] is not None else None
         info["launches"] += inf.launches
+        info["sweep_iters_max"] = max(info.get("sweep_iters_max", 0), inf.sweep_iters_max)
         info["relres"] = max(info["relres"], inf.relres)
         for key in ("spmm_ms", "update_ms", "spmm_launches", "update_launches", "coarse_ms", "coarse_launches"):
             info[key] += getattr(inf, key)
+        if instances is not None:
+            inst_status.append(instances.status.clone() if budget is not None else instances.status.cpu().numpy())
+            inst_relres.append(rel)
+    if instances is not None and budget is not None:
+        info["flag"] = None
+        info["relres"] = None
+        info["inst_status"] = torch.amax(torch.stack(inst_status), dim=0) if len(inst_status) > 1 else inst_status[0]
+        info["inst_relres"] = torch.cat(inst_relres, dim=1) if len(inst_relres) > 1 else inst_relres[0]
+    elif instances is not None:
+        info["inst_status"] = np.max(np.stack(inst_status), axis=0)
+        info["inst_relres"] = torch.cat(inst_relres, dim=1).cpu().numpy()
     info["coarse_nc"] = cs.nc if cs is not None else 0
+    # the FP32 product of the last column block: the row-group kernel when
+    # groups were given and the block width suits its lane layout
+    kb = k - 128 * ((k - 1) // 128) if k else 0
+    info["spmm_kernel"] = ("spmm_blk_kernel" if rg is not None and 65 <= kb <= 128 and kb % 4 == 0
+                           else "spmm_pair_kernel")
     return X, info
 
 
@@ -724,12 +809,31 @@ def _grid_nsd(psrc, pdet, nsu, ndet):
     return nsd
 
 
+_PAIRS = {}
+
+
+def _pair_dev(sd, dev):
+    """pair_map of ``sd`` with its three index arrays on the device, cached
+    by content (a loop over one sd table uploads them once)."""
+    a = np.ascontiguousarray(sd)
+    key = (a.shape, a.dtype.str, zlib.crc32(memoryview(a).cast("B")), str(dev))
+    hit = _PAIRS.get(key)
+    if hit is None:
+        cols, det0, ndet, psrc, pdet, _, _ = pair_map(a)
+        hit = (cols, det0, ndet, psrc, pdet, _i32(cols, dev), _i32(psrc, dev), _i32(pdet, dev),
+               _grid_nsd(psrc, pdet, det0, ndet))
+        if len(_PAIRS) > 64:
+            _PAIRS.clear()
+        _PAIRS[key] = hit
+    return hit
+
+
 def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=None, evol=None, ddd=None):
     """Adjoint Jacobian rows on the device (nsd x nn), see rb_jac.
     what: 'mua' (reference semantics, forward.py:509-569), 'mua_nodal'
     (exact for node-based properties at fixed D) or 'D'."""
     dev = phi.device
-    cols, det0, ndet, psrc, pdet, _, _ = pair_map(sd)
+    cols, det0, ndet, psrc, pdet, colsd, ps, pd, gnsd = _pair_dev(sd, dev)
     nsd = len(psrc)
     cplx = phi.is_complex()
     if cplx and not out_dtype.is_complex:
@@ -744,15 +848,11 @@ def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=Non
     w = {"mua": _lib.RB_JAC_MUA_REF, "mua_nodal": _lib.RB_JAC_MUA_NODAL, "D": _lib.RB_JAC_D}[what]
     ev = evol if evol is not None else mesh.evol
     dd = ddd if ddd is not None else (mesh.ddd if w == _lib.RB_JAC_D else None)
-    colsd = _i32(cols, dev)
-    ps = _i32(psrc, dev)
-    pd = _i32(pdet, dev)
     # pair groups: at most 128 staged columns / 64 detectors per launch
     if len(cols) > 128 or ndet > 64:
         raise ValueError("rb_jac stages at most 128 phi columns and 64 detectors per call")
     call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0, ndet,
-         ptr(ps), ptr(pd), _grid_nsd(psrc, pdet, det0, ndet), ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev),
-         ptr(dd), stream())
+         ptr(ps), ptr(pd), gnsd, ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev), ptr(dd), stream())
     return J
 
 
@@ -791,7 +891,11 @@ def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torc
     nn = mesh.nn
     bf = dtype == torch.bfloat16
     ldj = _pad8(len(params) * nn) if bf else _pad4(len(params) * nn)
-    J = torch.zeros((rows, ldj), dtype=dtype, device=phi.device)
+    # every column below len(params) * nn is written by rb_jac; only the
+    # row padding (read by the gram's aligned tiles) is cleared here
+    J = torch.empty((rows, ldj), dtype=dtype, device=phi.device)
+    if ldj > len(params) * nn:
+        J[:, len(params) * nn:].zero_()
     if bf:
         out_kind = _lib.RB_JAC_SPLIT_BF16 if cplx else _lib.RB_JAC_BF16
     else:

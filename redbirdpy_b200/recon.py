@@ -81,8 +81,10 @@ def _device_rows(A):
         raise ValueError("reginv expects a real matrix (use matreform first)")
     M, K = A.shape
     ld = engine._pad4(K)
-    J = torch.zeros((M, ld), dtype=torch.float32, device=engine._dev())
+    J = torch.empty((M, ld), dtype=torch.float32, device=engine._dev())
     J[:, :K] = torch.as_tensor(np.ascontiguousarray(A, dtype=np.float32), device=J.device)
+    if ld > K:
+        J[:, K:].zero_()
     return J, K
 
 
@@ -245,7 +247,11 @@ def _stacked_matrix(mesh, phis, sds, dets, y0s, wavelengths, weights, nq, remap,
     nb = len(weights[wavelengths[0]])
     K = nb * nq * (2 if (reform == "reim" and cplx) else 1)
     rows_total = 2 * R if cplx else R
-    J = torch.zeros((rows_total, engine._pad4(K)), dtype=torch.float32, device=mesh.device)
+    # every (row, column < K) is written by the blocks below; the padding
+    # columns are cleared
+    J = torch.empty((rows_total, engine._pad4(K)), dtype=torch.float32, device=mesh.device)
+    if J.shape[1] > K:
+        J[:, K:].zero_()
     rhs = []
     r0 = 0
     for j, wv in enumerate(wavelengths):

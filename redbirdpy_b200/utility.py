@@ -61,7 +61,7 @@ def _elemvolume(node, cells):
     if c0.shape[1] >= 4:
         return np.abs(_signed_volume6(node, c0)) / 6.0
     v = np.cross(node[c0[:, 1]] - node[c0[:, 0]], node[c0[:, 2]] - node[c0[:, 0]])
-    return 0.5 * np.sqrt(np.einsum("ij,ij->i", v, v))
+    return 0.5 * np.sqrt(np.sum(v ** 2, axis=1))
 
 
 def _nodevolume(nn, elem, evol):

@@ -2,8 +2,8 @@
 reference redbirdpy here (tests/golden/make_golden.py --contract):
 
 * the 3M-tet forward (box 100 x 100 x 50 mm at 1 mm, 64 + 64 optodes, CW):
-  4 x 4 detector values against the reference's femsolve(method='cg',
-  tol=1e-10) on that subset;
+  4 x 4 detector values against the reference's femsolve(method='cg') on
+  that subset, at tol=1e-14 and at its default tol=1e-10;
 * the 375k-tet adjoint case (2 mm box, per-node properties, 32 x 32 pairs):
   the reference's run (all 32 x 32 detector values) and jac (64 node columns
   of all 1024 rows), and central differences (h = 1e-4 relative) of
@@ -115,7 +115,14 @@ def test_c3_adjoint_gradient_vs_central_fd(c3, precision):
 
 def test_c2_detector_subset_matches_reference_cg(golden):
     """The full 128-column solve of the 3M-tet box against the reference's
-    femsolve(method='cg', tol=1e-10) on 4 sources and 4 detectors."""
+    femsolve(method='cg') on 4 sources and 4 detectors.  The subset's values
+    span 1 to 1.2e-10 of the largest; a residual-norm criterion determines
+    each value only to about (FP64 floor) x (largest / value), so the bar is
+    set per magnitude: 1e-6 relative for values >= 1e-4 of the largest
+    (against the reference at tol=1e-14, relative residuals ~1e-14), and
+    1e-10 of the largest value for every entry.  The reference's default
+    tol=1e-10 run stops with the far pairs tens of percent off; against it
+    the bar is 1e-6 of the largest value."""
     _need("c2_contract")
     g = golden("c2_contract")
     node, elem = kuhn_box([100, 100, 50], 1)
@@ -126,9 +133,16 @@ def test_c2_detector_subset_matches_reference_cg(golden):
     cfg, sd = rbb.meshprep(cfg)
     det, _ = rbb.run(cfg)
     sub = det[np.ix_(g["idet"], g["isrc"])]
-    assert int(g["flag"]) == 0
-    err = np.abs(sub - g["detval"]) / np.abs(g["detval"])
-    assert err.max() <= 1e-6, err.max()
+    assert int(g["flag"]) == 0 and int(g["flag14"]) == 0
+    assert g["relres14"].max() <= 1e-13
+    ref = g["detval14"]
+    big = np.abs(ref).max()
+    err = np.abs(sub - ref) / np.abs(ref)
+    near = np.abs(ref) >= 1e-4 * big
+    assert err[near].max() <= 1e-6, np.array2string(err, precision=2)
+    assert np.abs(sub - ref).max() <= 1e-10 * big, np.array2string(err, precision=2)
+    err10 = np.abs(sub - g["detval"]).max() / np.abs(g["detval"]).max()
+    assert err10 <= 1e-6, err10
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])

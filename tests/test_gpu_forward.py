@@ -206,6 +206,37 @@ def test_large_pattern_vs_scipy():
     assert np.abs(A.data - R.data).max() / np.abs(R.data).max() <= 1e-12
 
 
+@pytest.mark.parametrize("case", CASES)
+def test_assembly_tables(golden, case):
+    """The contributor tables against a numpy restatement, and the assembly
+    through them against the scan of every incident tet."""
+    g = golden(case)
+    cfg = cfg_from(g)
+    m = engine.mesh_of(cfg)
+    eptr, elist = m.eptr.cpu().numpy(), m.elist.cpu().numpy()
+    indptr, indices = m.indptr.cpu().numpy(), m.indices[: m.nnz].cpu().numpy()
+    elem = m.elem.cpu().numpy().reshape(-1, 4)
+    if np.diff(eptr).max() > 32 or np.diff(indptr).max() > 255:
+        assert m.inc_slot is None and m.struct.inc_slot is None
+        return
+    inc = m.inc_slot[: 4 * m.ne].cpu().numpy().view(np.uint32)
+    msk = m.slot_mask[: m.nnz].cpu().numpy().view(np.uint32)
+    want_msk = np.zeros(m.nnz, dtype=np.uint32)
+    for n in range(m.nn):
+        cols = indices[indptr[n]:indptr[n + 1]]
+        for u, e in enumerate(elist[eptr[n]:eptr[n + 1]]):
+            pos = np.searchsorted(cols, elem[e])
+            assert np.array_equal(cols[pos], elem[e])
+            assert inc[eptr[n] + u] == sum(int(p) << (8 * j) for j, p in enumerate(pos))
+            want_msk[indptr[n] + pos] |= np.uint32(1 << u)
+    assert np.array_equal(msk, want_msk)
+    optics = engine.Optics.from_cfg(m, cfg)
+    a = engine.assemble(m, optics)
+    b = engine.assemble(m, optics, tables=False)
+    va, vb = a.val64[: m.nnz].cpu().numpy(), b.val64[: m.nnz].cpu().numpy()
+    assert np.abs(va - vb).max() <= 1e-14 * np.abs(vb).max()
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 def test_femsolve_breakdown_is_a_flag_not_a_hang(cplx):
     """(p, A p) = 0 on the first step (indefinite / complex-symmetric

@@ -183,3 +183,94 @@ def test_batched_instances_match_per_instance_models():
             for got, ref in ((gms[i], mu.grad), (gds[i], dc.grad)):
                 e = (torch.abs(got - ref).max() / torch.abs(ref).max()).item()
                 assert e <= max(tol, 1e-9) * 10, (prec, i, e)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_convergence_is_per_instance(precision):
+    """Two instances whose right-hand sides differ by 1e8 in scale: each one
+    reaches the tolerance against its own ||b_i|| (a whole-column criterion
+    would let the small one stop at 1e8 times the tolerance), and each
+    matches its own solve; statuses and per-(instance, column) residuals
+    come back."""
+    from redbirdpy_b200.meshgen import kuhn_box
+    from scipy.sparse.linalg import splu
+
+    from oracle import femoracle as fo
+
+    parts = []
+    for dims, h, mua in (([20, 16, 12], 2.0, 0.01), ([16, 16, 10], 2.0, 0.03)):
+        node, elem = kuhn_box(dims, h)
+        cfg = dict(node=node, elem=elem, prop=np.array([[0, 0, 1, 1], [mua, 1.0, 0, 1.37]]),
+                   seg=np.ones(elem.shape[0], dtype=np.int32), srcpos=np.array([[8, 8, 0.0]]),
+                   srcdir=np.array([[0, 0, 1.0]]), detpos=np.array([[10, 8, 0.0]]), omega=0.0)
+        parts.append(rbb.meshprep(cfg)[0])
+    A = [fo.femlhs(dict(c), fo.deldotdel(c["node"], c["elem"], c["evol"])) for c in parts]
+    n = [a.shape[0] for a in A]
+    from scipy import sparse
+
+    Ab = sparse.block_diag(A, format="csr")
+    rng = np.random.default_rng(3)
+    B = rng.standard_normal((sum(n), 4))
+    B[n[0]:] *= 1e-8
+    mat = engine.DeviceMatrix.from_scipy(Ab)
+    inst = engine.Instances([0, n[0], n[0] + n[1]], "cuda")
+    Bd = torch.as_tensor(B, device="cuda")
+    X, info = engine.solve(mat, Bd, precision=precision, tol=1e-10, instances=inst, coarse=False, groups=None)
+    assert info["flag"] == 0
+    assert list(info["inst_status"]) == [0, 0]
+    assert info["inst_relres"].shape == (2, 4) and info["inst_relres"].max() <= 1e-10
+    X = X.cpu().numpy()
+    for i, (a, lo) in enumerate(zip(A, (0, n[0]))):
+        xi = X[lo:lo + n[i]]
+        bi = B[lo:lo + n[i]]
+        rel = np.linalg.norm(bi - a @ xi, axis=0) / np.linalg.norm(bi, axis=0)
+        assert rel.max() <= 1e-10, (i, rel)
+        ref = splu(a.tocsc()).solve(bi)
+        assert np.abs(xi - ref).max() <= 1e-8 * np.abs(ref).max(), i
+
+
+def _masked_log_loss(own, tgt):
+    def loss(det):
+        d = torch.where(own, det, torch.ones_like(det))
+        t = torch.where(own, tgt, torch.ones_like(tgt))
+        return 0.5 * torch.sum((torch.log(torch.abs(d)) - torch.log(torch.abs(t))) ** 2)
+    return loss
+
+
+def test_captured_batch_step_matches_checked_solves():
+    """Forward + adjoint of a batch replayed from one CUDA graph (fixed solve
+    budget, no host checks) against the same step with checked solves, at
+    the captured properties and at new ones copied in before a replay."""
+    from redbirdpy_b200.adjoint import BatchModel, CapturedStep, detector_values
+    from redbirdpy_b200.meshgen import batch_boxes
+
+    cfgs = [rbb.meshprep(c)[0] for c in batch_boxes(6, seed=5, dims=(12.0, 24.0), spacings=(3.0, 4.0), nopt=(2, 5))]
+    bm = BatchModel(cfgs, precision="mixed")
+    mua0 = torch.as_tensor(np.concatenate([c["prop"][:, 0] for c in cfgs]), device="cuda")
+    d0 = torch.as_tensor(np.concatenate([1.0 / (3.0 * (c["prop"][:, 0] + c["prop"][:, 1])) for c in cfgs]),
+                         device="cuda")
+    with torch.no_grad():
+        tgt = detector_values(bm, mua0 * 1.1, d0)
+    loss_fn = _masked_log_loss(bm.own, tgt)
+
+    def checked(mua, dco):
+        m = mua.clone().requires_grad_(True)
+        d = dco.clone().requires_grad_(True)
+        det = detector_values(bm, m, d)
+        loss = loss_fn(det)
+        loss.backward()
+        return loss.detach(), det.detach(), m.grad, d.grad
+
+    step = CapturedStep(bm, loss_fn, mua0, d0)
+    assert step.budget[0] >= 1 and step.budget[1] >= 8
+    for scale in (1.0, 1.05):
+        got = [t.clone() for t in step(mua0 * scale, d0)]
+        assert int(step.status.max().item()) == 0
+        step_kw = bm.solve_kw
+        bm.solve_kw = step.solve_kw_checked
+        ref = checked(mua0 * scale, d0)
+        bm.solve_kw = step_kw
+        for a, b in zip(got, ref):
+            e = (torch.abs(a - b).max() / torch.abs(b).max()).item()
+            assert e <= 1e-8, (scale, e)
+    step.release()
