@@ -422,8 +422,15 @@ def run_gn_step(cfg, mesh, world, args):
         y = det.cpu().numpy().ravel()
         mis = data - y
         mis = np.concatenate([mis.real, mis.imag])
-        s2 = timed_stage("sumsq", lambda: 1.0 / float(engine.sumsq(J, K).item()))
-        H, _ = timed_stage("gram", lambda: engine.gram(J, K, s2, gram_prec))
+        # row sums of squares: the Frobenius scale and the exact diagonal of
+        # J J^T (the product's own diagonal carries the TF32 input rounding,
+        # which lam = 0.05 max(diag) would inherit)
+        rowsq, tot = timed_stage("sumsq", lambda: engine.row_sumsq(J, K))
+        s2 = 1.0 / float(tot.item())
+        # tf32x3 leaves J as its TF32 part and returns the remainder: the
+        # refinement below runs over both, i.e. over the FP32 rows
+        H, lo = timed_stage("gram", lambda: engine.gram(J, K, s2, gram_prec))
+        engine.call("rb_set_diag", engine.ptr(H), H.shape[0], H.shape[0], engine.ptr(rowsq), s2, engine.stream())
         lam = 0.05 * float(H.diagonal().max().item())
         M = J.shape[0]
         di = torch.empty(M, dtype=torch.float64, device=J.device)
@@ -438,10 +445,10 @@ def run_gn_step(cfg, mesh, world, args):
         # solve with FP64 refinement over the stored J, then J^T y
         rinfo = {}
         dmu = timed_stage("solve_refine_jty", lambda: engine.normal_solve(
-            J, K, H, di, mis, lam, s2, None, refine=refine, info=rinfo).cpu().numpy())
+            J, K, H, di, mis, lam, s2, lo, refine=refine, info=rinfo).cpu().numpy())
         state["refine"] = rinfo
         state["det"] = det
-        del J, H
+        del J, H, lo
         if apply:
             apply_update(gcfg["prop"], dmu)
             state["phi"] = phi
@@ -455,6 +462,10 @@ def run_gn_step(cfg, mesh, world, args):
     stages.clear()
     ks = max(1, min(args.steps, 2))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # clocks during the timed GN iterations: the tensor-core product runs at
+    # the 1 kW power cap, where the SM clock settles well below its maximum
+    gclk = ClockSampler(torch.cuda.current_device())
+    gclk.start()
     e0.record()
     for i in range(ks):
         if i == ks - 1:
@@ -462,6 +473,7 @@ def run_gn_step(cfg, mesh, world, args):
         dmu_mixed = step_mixed()
     e1.record()
     torch.cuda.synchronize()
+    gn_clocks = gclk.stop()
     ms = max_over_ranks(e0.elapsed_time(e1) / ks, world)
     mixed_stages = {k: round(v / ks, 2) for k, v in stages.items()}
 
@@ -549,13 +561,49 @@ def run_gn_step(cfg, mesh, world, args):
         tf32x3 = {"ms_per_iter": round(x3ms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
                   "speedup_vs_fp64": round(ms64 / x3ms, 3),
                   "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_x3 - dmu64) / np.linalg.norm(dmu64))}
+    # the same iteration with the Jacobian never stored: node slabs of a
+    # quarter of the mesh recomputed on every pass (the mode a mesh whose J
+    # exceeds HBM takes), same state as the FP64 comparison
+    slab = None
+    if not args.no_fp64_gn:
+        gcfg["prop"] = snap[0].copy()
+
+        def step_slab(width):
+            det, phi, _, _, _ = forward_device(gcfg, x0=snap[1])
+            op = engine.SlabJacobian(mesh, phi, sd, ("mua", "D"), "exact", width)
+            y = det.cpu().numpy().ravel()
+            mis = data - y
+            mis = np.concatenate([mis.real, mis.imag])
+            rowsq, tot = op.row_sumsq()
+            s2 = 1.0 / float(tot.item())
+            H, di, lam = engine.normal_factor_op(op, 0.0, s2, "tf32", lam_rel=0.05, rowsq=rowsq)
+            rinfo = {}
+            dmu = engine.normal_solve(op, op.K, H, di, mis, lam, s2, None, refine=refine, info=rinfo)
+            return dmu.cpu().numpy(), op.passes, rinfo
+
+        width = (mesh.nn + 3) // 4
+        step_slab(width)
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        dmu_s, passes, rinfo_s = step_slab(width)
+        b1.record()
+        torch.cuda.synchronize()
+        sms = max_over_ranks(b0.elapsed_time(b1), world)
+        slab = {"ms_per_iter": round(sms, 1), "slab_nodes": width, "jacobian_passes": passes,
+                "jacobian_slab_bytes": int(8192 * 2 * width * 4),
+                "jacobian_stored_bytes": int(8192 * 2 * mesh.nn * 4),
+                "refine_sweeps": rinfo_s.get("refine_sweeps"),
+                "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_s - dmu64) / np.linalg.norm(dmu64))}
     tflops = gram_flop / (gram_ms * 1e-3) / 1e12 if gram_ms else None
-    pk, pk_src = 1590.0, "fallback bf16 (burst), no MEASURED_PEAKS.json"
+    pk, pk_src, pk_sus = 1590.0, "fallback bf16 (burst), no MEASURED_PEAKS.json", 1400.0
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        v = json.load(open(p)).get("bf16_tflops")
+        mp = json.load(open(p))
+        v = mp.get("bf16_tflops")
         if v:
             pk, pk_src = float(v), "measured bf16 (burst)"
+        pk_sus = float(mp.get("bf16_tflops_sustained") or pk_sus)
     return {
         "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
                     f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, TF32 J J^T + FP64 refinement of the normal "
@@ -573,9 +621,15 @@ def run_gn_step(cfg, mesh, world, args):
                           "achieved": round(tflops, 1) if tflops else None, "unit": "TFLOP/s",
                           "algorithmic_flop": gram_flop, "peak": pk, "peak_source": pk_src,
                           "frac_of_bf16": round(tflops / pk, 4) if (tflops and pk) else None,
-                          "note": "TF32 dense peak is half the BF16 one"},
+                          "sustained_bf16_peak": pk_sus,
+                          "frac_of_sustained_tf32": (round(tflops / (0.5 * pk_sus), 4)
+                                                     if (tflops and pk_sus) else None),
+                          "note": "TF32 dense peak is half the BF16 one; the GN step runs at the power cap, "
+                                  "so the sustained figure is the one its clocks reach"},
+        "clocks": gn_clocks,
         "bf16_form": bf16,
         "tf32x3_form": tf32x3,
+        "slab_recompute_form": slab,
     }
 
 

@@ -502,6 +502,16 @@ int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, voi
              size_t work_bytes, void* stream);
 int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work,
                   size_t work_bytes, void* stream);
+/* rows[m] = sum_k J[m][k]^2 (FP64 accumulation; the exact diagonal of J J^T
+ * for the stored rows), and *total = sum_m rows[m] when total != NULL (the
+ * Frobenius sum of rb_sumsq, same pass).  A diagonal taken from the
+ * tensor-core product carries its input rounding (TF32 ~1e-3 relative), which
+ * a regularisation relative to the largest diagonal entry would inherit. */
+int rb_row_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream);
+int rb_row_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total,
+                      void* stream);
+/* H[i][i] = alpha d[i] */
+int rb_set_diag(double* H, int64_t M, int64_t ldh, const double* d, double alpha, void* stream);
 int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream);
 /* FP64 iterative refinement of the normal equations (alpha J J^T + lambda I) y = r
  * around the tensor-core factor (the refinement residual r - alpha J (J^T y)

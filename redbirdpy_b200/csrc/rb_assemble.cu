@@ -254,14 +254,17 @@ __device__ __forceinline__ cdouble shfl_xor_s(cdouble v, int o) {
   return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
 }
 
-// Table-driven assembly: one warp per row.  Lane u < ek evaluates the row's
-// u-th incident tet and stages its 4 values; the diagonal (every tet
-// contributes its (li, li) value) is a butterfly sum across the lanes; lane
-// s then owns CSR slot s and sums the staged values of the tets in its
-// contributor mask in ascending tet order.  The slot's column index and
-// mask of the first 32 slots are loaded before the tets, so that their
+// Table-driven assembly.  A warp holds R rows at once, L = 32 / R lanes per
+// row; lane l of a row evaluates its incident tets l, l + L, ... (at most
+// 32 / L of them, a row having at most 32 when the tables exist) and stages
+// each tet's 4 values for the row in shared memory, so that R x (32 / L)
+// independent load chains are in flight per warp.  The diagonal (every tet
+// contributes its (li, li) value) is a butterfly sum across the row's lanes;
+// then lane l owns CSR slots l, l + L, ... of its row and sums the staged
+// values of the tets in the slot's contributor mask in ascending tet order.
+// The slot's column index and mask are loaded before the tets, so that their
 // latency overlaps the tet loads.
-template <bool CPLX, int KIND>
+template <bool CPLX, int KIND, int R>
 __global__ void __launch_bounds__(kAsmWarps * 32)
 femlhs_tab_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, const double* __restrict__ ddd,
                   const double* __restrict__ dco, const uint32_t* __restrict__ inc_slot,
@@ -269,49 +272,69 @@ femlhs_tab_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, const
                   typename AsmVal<CPLX>::T* __restrict__ val64, typename AsmVal<CPLX>::T32* __restrict__ val32,
                   typename AsmVal<CPLX>::T* __restrict__ dinv64, typename AsmVal<CPLX>::T32* __restrict__ dinv32) {
   typedef typename AsmVal<CPLX>::T T;
-  __shared__ T s_vals[kAsmWarps][32][4];
-  __shared__ uint32_t s_ps[kAsmWarps][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int L = 32 / R;  // lanes per row
+  __shared__ T s_vals[kAsmWarps][R][32][4];
+  __shared__ uint32_t s_ps[kAsmWarps][R][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, h = lane / L, j = lane % L;
   const int64_t warps = (int64_t)gridDim.x * kAsmWarps;
-  for (int64_t row = blockIdx.x * (int64_t)kAsmWarps + w; row < m.nn; row += warps) {
-    const int32_t rb = m.indptr[row], rn = m.indptr[row + 1] - rb;
-    const int32_t eb = m.node_eptr[row], ek = m.node_eptr[row + 1] - eb;
-    const int32_t fb = m.node_fptr[row], fk = m.node_fptr[row + 1] - fb;
-    const int32_t col0 = (lane < rn) ? m.indices[rb + lane] : -1;
-    const uint32_t msk0 = (lane < rn) ? slot_mask[rb + lane] : 0u;
-    T d = s_zero(T());
-    if (lane < ek) {
-      const int64_t e = m.node_elist[eb + lane];
-      const uint32_t ps = inc_slot[eb + lane];
-      const int4 en = reinterpret_cast<const int4*>(m.elem)[e];
-      T v[4];
-      tet_row<CPLX, KIND>(m, o, evol, ddd, dco, wc, e, en, row, v);
-      const int li = (en.y == row) ? 1 : (en.z == row) ? 2 : (en.w == row) ? 3 : 0;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        s_vals[w][lane][j] = v[j];
-        if (j == li) d = v[j];
-      }
-      s_ps[w][lane] = ps;
+  for (int64_t grp = blockIdx.x * (int64_t)kAsmWarps + w; grp * R < m.nn; grp += warps) {
+    const int64_t row = grp * R + h;
+    int32_t rb = 0, rn = 0, eb = 0, ek = 0, fb = 0, fk = 0;
+    if (row < m.nn) {
+      rb = m.indptr[row];
+      rn = m.indptr[row + 1] - rb;
+      eb = m.node_eptr[row];
+      ek = m.node_eptr[row + 1] - eb;
+      fb = m.node_fptr[row];
+      fk = m.node_fptr[row + 1] - fb;
     }
-    // diagonal: every incident tet contributes its (li, li) entry
+    const int32_t col0 = (j < rn) ? m.indices[rb + j] : -1;
+    const uint32_t msk0 = (j < rn) ? slot_mask[rb + j] : 0u;
+    int64_t e[R];
+    uint32_t ps[R];
+    int4 en[R];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) d = s_add(d, shfl_xor_s(d, off));
+    for (int i = 0; i < R; ++i) {
+      const int u = j + L * i;
+      e[i] = (u < ek) ? m.node_elist[eb + u] : 0;
+      ps[i] = (u < ek) ? inc_slot[eb + u] : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) en[i] = reinterpret_cast<const int4*>(m.elem)[e[i]];
+    T d = s_zero(T());
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int u = j + L * i;
+      if (u < ek) {
+        T v[4];
+        tet_row<CPLX, KIND>(m, o, evol, ddd, dco, wc, e[i], en[i], row, v);
+        const int li = (en[i].y == row) ? 1 : (en[i].z == row) ? 2 : (en[i].w == row) ? 3 : 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          s_vals[w][h][u][q] = v[q];
+          if (q == li) d = s_add(d, v[q]);
+        }
+        s_ps[w][h][u] = ps[i];
+      }
+    }
+    // diagonal: butterfly over the row's lanes (offsets below L stay in them)
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) d = s_add(d, shfl_xor_s(d, off));
     __syncwarp();
-    for (int32_t sl = lane; sl < rn; sl += 32) {
-      const int32_t col = (sl == lane) ? col0 : m.indices[rb + sl];
+    for (int32_t sl = j; sl < rn; sl += L) {
+      const int32_t col = (sl == j) ? col0 : m.indices[rb + sl];
       T acc = s_zero(T());
       if (col == row) {
         acc = d;
       } else {
-        uint32_t msk = (sl == lane) ? msk0 : slot_mask[rb + sl];
+        uint32_t msk = (sl == j) ? msk0 : slot_mask[rb + sl];
         while (msk) {
           const int u = __ffs(msk) - 1;
           msk &= msk - 1;
-          const uint32_t ps = s_ps[w][u];
-          const int j = ((ps & 255u) == (uint32_t)sl) ? 0 : (((ps >> 8) & 255u) == (uint32_t)sl) ? 1
-                        : (((ps >> 16) & 255u) == (uint32_t)sl) ? 2 : 3;
-          acc = s_add(acc, s_vals[w][u][j]);
+          const uint32_t p = s_ps[w][h][u];
+          const int q = ((p & 255u) == (uint32_t)sl) ? 0 : (((p >> 8) & 255u) == (uint32_t)sl) ? 1
+                        : (((p >> 16) & 255u) == (uint32_t)sl) ? 2 : 3;
+          acc = s_add(acc, s_vals[w][h][u][q]);
         }
       }
       // Robin boundary: area*bc on the diagonal, half of it off the diagonal
@@ -332,9 +355,14 @@ femlhs_tab_kernel(rb_mesh m, rb_optics o, const double* __restrict__ evol, const
         if (dinv32) dinv32[row] = narrow(r);
       }
     }
-    __syncwarp();  // the staged values are rewritten for the next row
+    __syncwarp();  // the staged values are rewritten for the next rows
   }
 }
+
+// rows per warp of the table-driven assembly (measured on the 3M-tet box,
+// one pass of the grid: 1 row 0.37 ms, 2 rows 0.29 ms at CW; 4 rows do not
+// fit the complex kernel's staging in 48 KB of static shared memory)
+constexpr int kTabRowsPerWarp = 2;
 
 template <bool CPLX, int KIND>
 int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, const double* ddd, double* dco,
@@ -347,10 +375,15 @@ int launch_femlhs(const rb_mesh& m, const rb_optics& o, const double* evol, cons
   dcoeff_kernel<<<(unsigned)std::min<int64_t>(ceil_div(np, 256), 148 * 16), 256, 0, st>>>(np, o.mua, o.musp, dco);
   RB_LAUNCH_CHECK();
   unsigned g = (unsigned)std::min<int64_t>(ceil_div(m.nn, kAsmWarps), 148 * 64);
-  if (m.inc_slot && m.slot_mask)
-    femlhs_tab_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, m.inc_slot, m.slot_mask, bc,
-                                                                  wc, (T*)v64, (T32*)v32, (T*)d64, (T32*)d32);
-  else
+  if (m.inc_slot && m.slot_mask) {
+    // one pass of the grid over the rows, in row order: the tets a row shares
+    // with the rows a grid plane away are then still in L2 when those come
+    constexpr int R = kTabRowsPerWarp;
+    const unsigned g2 = (unsigned)ceil_div(ceil_div(m.nn, R), kAsmWarps);
+    femlhs_tab_kernel<CPLX, KIND, R><<<g2, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, m.inc_slot, m.slot_mask,
+                                                                      bc, wc, (T*)v64, (T32*)v32, (T*)d64,
+                                                                      (T32*)d32);
+  } else
     femlhs_rows_kernel<CPLX, KIND><<<g, kAsmWarps * 32, 0, st>>>(m, o, evol, ddd, dco, bc, wc, (T*)v64, (T32*)v32,
                                                                    (T*)d64, (T32*)d32);
   RB_LAUNCH_CHECK();

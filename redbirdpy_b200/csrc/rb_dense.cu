@@ -481,6 +481,37 @@ __global__ void sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int
   }
 }
 
+// out[m] = sum_k J[m][k]^2 in FP64: a block per row, a fixed-order
+// reduction (the diagonal of J J^T without the tensor cores' input rounding)
+template <typename JT>
+__global__ void row_sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+                                 double* __restrict__ out) {
+  __shared__ double red[32];
+  for (int64_t m = blockIdx.x; m < M; m += gridDim.x) {
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+      const double v = jval(J[m * ldj + k]);
+      s += v * v;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+      t = warp_sum(t);
+      if (threadIdx.x == 0) out[m] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// H[i][i] = alpha d[i]
+__global__ void set_diag_kernel(double* __restrict__ H, int64_t M, int64_t ldh, const double* __restrict__ d,
+                                double alpha) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < M) H[i * ldh + i] = alpha * d[i];
+}
+
 __global__ void sum_parts_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
   __shared__ double red[32];
   double s = 0.0;
@@ -708,6 +739,40 @@ int rb_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* out, voi
 int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out, void* work, size_t work_bytes,
                   void* stream) {
   return sumsq_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, out, work, work_bytes, stream);
+}
+
+}  // extern "C"
+
+template <typename JT>
+static int row_sumsq_run(const JT* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream) {
+  if (!J || !rows || M < 1 || K < 1 || ldj < K || M > INT32_MAX) return fail(RB_EARG, "rb_row_sumsq: bad arguments");
+  cudaStream_t st = as_stream(stream);
+  const unsigned nb = (unsigned)std::min<int64_t>(M, 148 * 16);
+  row_sumsq_kernel<JT><<<nb, 256, 0, st>>>(J, M, K, ldj, rows);
+  RB_LAUNCH_CHECK();
+  if (total) {
+    sum_parts_kernel<<<1, 1024, 0, st>>>(rows, (int)M, total);
+    RB_LAUNCH_CHECK();
+  }
+  return RB_OK;
+}
+
+extern "C" {
+
+int rb_row_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream) {
+  return row_sumsq_run(J, M, K, ldj, rows, total, stream);
+}
+
+int rb_row_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total,
+                      void* stream) {
+  return row_sumsq_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, rows, total, stream);
+}
+
+int rb_set_diag(double* H, int64_t M, int64_t ldh, const double* d, double alpha, void* stream) {
+  if (!H || !d || M < 1 || ldh < M) return fail(RB_EARG, "rb_set_diag: bad arguments");
+  set_diag_kernel<<<(unsigned)ceil_div(M, 256), 256, 0, as_stream(stream)>>>(H, M, ldh, d, alpha);
+  RB_LAUNCH_CHECK();
+  return RB_OK;
 }
 
 }  // extern "C"

@@ -926,6 +926,17 @@ def sumsq(J, K):
     return out
 
 
+def row_sumsq(J, K):
+    """(rows, total): FP64 sums of squares of J's rows (the exact diagonal of
+    J J^T for the stored rows) and their sum (the Frobenius sum), one pass."""
+    M = J.shape[0]
+    rows = torch.empty(M, dtype=torch.float64, device=J.device)
+    total = torch.empty(1, dtype=torch.float64, device=J.device)
+    fn = "rb_row_sumsq_bf16" if J.dtype == torch.bfloat16 else "rb_row_sumsq"
+    call(fn, ptr(J), M, K, J.shape[1], ptr(rows), ptr(total), stream())
+    return rows, total
+
+
 def gram(J, K, alpha=1.0, precision="tf32"):
     """H = alpha J J^T (M x M FP64) on the tensor cores.  precision 'tf32'
     (one pass) or 'tf32x3' (split hi/lo, three passes; J is left as hi and
@@ -977,14 +988,18 @@ def norm2(x):
     return float(out.item()) ** 0.5
 
 
-def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None):
+def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None, rowsq=None):
     """The tensor-core half of reginvunder (recon.py:474-483): H = alpha J J^T
     (+ lam I, lam relative to the largest diagonal entry with ``lam_rel``),
     unit-diagonal normalisation (_normalize_diag, recon.py:784-789), FP64
-    Cholesky in place.  Returns (H, di, lo, lam)."""
+    Cholesky in place.  ``rowsq`` (row_sumsq's rows) replaces the product's
+    diagonal by the exact one, so that a relative lam and the normalisation
+    carry no tensor-core input rounding.  Returns (H, di, lo, lam)."""
     M, ldj = J.shape
     dev = J.device
     H, lo = gram(J, K, alpha, precision)
+    if rowsq is not None:
+        call("rb_set_diag", ptr(H), M, M, ptr(rowsq), float(alpha), stream())
     if lam_rel is not None:
         lam = float(lam_rel) * float(H.diagonal().max().item())
     di = torch.empty(M, dtype=torch.float64, device=dev)
@@ -993,6 +1008,161 @@ def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None):
     work = torch.empty(wb, dtype=torch.uint8, device=dev)
     call("rb_cholesky", ptr(H), M, M, ptr(work), wb, stream())
     return H, di, lo, float(lam)
+
+
+class StoredJacobian:
+    """The passes normal_solve makes over a J held in HBM (FP32 or BF16
+    rows; ``lo`` the split remainder of a tf32x3 factorisation)."""
+
+    def __init__(self, J, K, lo=None):
+        self.J, self.K, self.lo = J, K, lo
+        self.rows = J.shape[0]
+
+    def jt(self, y, alpha=1.0):
+        return gemv_t(self.J, self.K, y, alpha, lo=self.lo)
+
+    def jt_then_j(self, y):
+        """(u, J u) with u = J^T y: two passes over J."""
+        u = gemv_t(self.J, self.K, y, 1.0, lo=self.lo)
+        return u, gemv_n(self.J, self.K, u, 1.0, 0.0, lo=self.lo)
+
+
+class SlabJacobian:
+    """The GN matrix J = [J_p1 | J_p2 ...] (rows x K, K = len(params) * nn)
+    never held whole, for meshes whose Jacobian does not fit in HBM: node
+    slabs of ``width`` columns per parameter are recomputed from the stored
+    fields (rb_jac_range, redbirdpy's jac in column blocks,
+    forward.py:509-569) on every pass, so a pass costs one Jacobian build
+    and the memory is rows x len(params) x width.  Offers the same passes as
+    StoredJacobian plus the Frobenius sum and the tensor-core product."""
+
+    def __init__(self, mesh, phi, sd, params=("mua",), mode="reference", width=4096, dtype=torch.float32):
+        self.mesh, self.phi, self.params, self.dtype = mesh, phi, tuple(params), dtype
+        self.cols, self.det0, self.ndet, psrc, pdet, self.colsd, self.ps, self.pd, self.gnsd = _pair_dev(sd, phi.device)
+        if len(self.cols) > 128 or self.ndet > 64:
+            raise ValueError("rb_jac stages at most 128 phi columns and 64 detectors per call")
+        nsd = len(psrc)
+        self.cplx = phi.is_complex()
+        self.rows = 2 * nsd if self.cplx else nsd
+        self.nn = mesh.nn
+        self.K = len(self.params) * self.nn
+        self.width = int(max(1, min(width, self.nn)))
+        self.bf = dtype == torch.bfloat16
+        pad = _pad8 if self.bf else _pad4
+        self._pad = pad
+        self.buf = torch.empty(self.rows * pad(len(self.params) * self.width), dtype=dtype, device=phi.device)
+        if self.bf:
+            self.out_kind = _lib.RB_JAC_SPLIT_BF16 if self.cplx else _lib.RB_JAC_BF16
+        else:
+            self.out_kind = _lib.RB_JAC_SPLIT_F32 if self.cplx else _lib.RB_F32
+        self.phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
+                         torch.complex64: _lib.RB_C64}[phi.dtype]
+        self.whats = []
+        for name in self.params:
+            if name == "mua":
+                self.whats.append(_lib.RB_JAC_MUA_REF if mode == "reference" else _lib.RB_JAC_MUA_NODAL)
+            elif name == "D":
+                self.whats.append(_lib.RB_JAC_D)
+            else:
+                raise ValueError(f"unknown parameter {name}")
+        self.passes = 0
+
+    def ranges(self):
+        for a in range(0, self.nn, self.width):
+            yield a, min(self.nn, a + self.width)
+
+    def slab(self, a, b):
+        """J restricted to nodes a..b-1 (every parameter), rows x pad(P c),
+        columns [p1 nodes a..b-1 | p2 nodes a..b-1 ...]; the buffer is reused."""
+        c = b - a
+        ks = len(self.params) * c
+        ld = self._pad(ks)
+        Js = self.buf[: self.rows * ld].view(self.rows, ld)
+        if ld > ks:
+            Js[:, ks:].zero_()
+        m = self.mesh
+        for p, w in enumerate(self.whats):
+            sub = Js[:, p * c:]
+            call("rb_jac_range", ctypes.byref(m.struct), w, ptr(self.phi), self.phi_kind, self.phi.shape[1],
+                 ptr(self.colsd), len(self.cols), self.det0, self.ndet, ptr(self.ps), ptr(self.pd), self.gnsd,
+                 ptr(sub), ld, self.out_kind, m.rmax, m.emax, ptr(m.evol), ptr(m.ddd if w == _lib.RB_JAC_D else None),
+                 a, c, stream())
+        return Js, ks
+
+    def _pieces(self, a, b):
+        """K-space slices of a slab's columns, in the slab's column order."""
+        return [slice(p * self.nn + a, p * self.nn + b) for p in range(len(self.params))]
+
+    def row_sumsq(self):
+        """(rows, total) as engine.row_sumsq, summed over the slabs."""
+        rows = torch.zeros(self.rows, dtype=torch.float64, device=self.phi.device)
+        tot = torch.zeros(1, dtype=torch.float64, device=self.phi.device)
+        for a, b in self.ranges():
+            Js, ks = self.slab(a, b)
+            r_s, t_s = row_sumsq(Js, ks)
+            call("rb_axpby", self.rows, 1.0, ptr(r_s), 1.0, ptr(rows), stream())
+            call("rb_axpby", 1, 1.0, ptr(t_s), 1.0, ptr(tot), stream())
+        self.passes += 1
+        return rows, tot
+
+    def sumsq(self):
+        return self.row_sumsq()[1]
+
+    def gram(self, alpha=1.0, precision="tf32"):
+        """H = alpha sum over slabs of J_s J_s^T (FP64 accumulation of the
+        tensor-core products of each slab)."""
+        M = self.rows
+        H = torch.zeros((M, M), dtype=torch.float64, device=self.phi.device)
+        for a, b in self.ranges():
+            Js, ks = self.slab(a, b)
+            Hs, _ = gram(Js, ks, alpha, precision)
+            call("rb_axpby", M * M, 1.0, ptr(Hs), 1.0, ptr(H), stream())
+        self.passes += 1
+        return H
+
+    def jt(self, y, alpha=1.0):
+        out = torch.empty(self.K, dtype=torch.float64, device=self.phi.device)
+        for a, b in self.ranges():
+            Js, ks = self.slab(a, b)
+            us = gemv_t(Js, ks, y, alpha)
+            c = b - a
+            for p, sl in enumerate(self._pieces(a, b)):
+                out[sl] = us[p * c:(p + 1) * c]
+        self.passes += 1
+        return out
+
+    def jt_then_j(self, y):
+        """(u, J u) with u = J^T y in one pass: per slab u_s = J_s^T y, then
+        the slab's share J_s u_s while J_s is still in HBM."""
+        M = self.rows
+        u = torch.empty(self.K, dtype=torch.float64, device=self.phi.device)
+        Ju = torch.zeros(M, dtype=torch.float64, device=self.phi.device)
+        for a, b in self.ranges():
+            Js, ks = self.slab(a, b)
+            us = gemv_t(Js, ks, y, 1.0)
+            gemv_n(Js, ks, us, 1.0, 1.0, out=Ju)
+            c = b - a
+            for p, sl in enumerate(self._pieces(a, b)):
+                u[sl] = us[p * c:(p + 1) * c]
+        self.passes += 1
+        return u, Ju
+
+
+def normal_factor_op(op, lam, alpha=1.0, precision="tf32", lam_rel=None, rowsq=None):
+    """normal_factor for a SlabJacobian: the product summed over its slabs."""
+    M = op.rows
+    dev = op.phi.device
+    H = op.gram(alpha, precision)
+    if rowsq is not None:
+        call("rb_set_diag", ptr(H), M, M, ptr(rowsq), float(alpha), stream())
+    if lam_rel is not None:
+        lam = float(lam_rel) * float(H.diagonal().max().item())
+    di = torch.empty(M, dtype=torch.float64, device=dev)
+    call("rb_reginv_prepare", ptr(H), M, M, float(lam), ptr(di), stream())
+    wb = _lib.lib().rb_cholesky_work_bytes()
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    call("rb_cholesky", ptr(H), M, M, ptr(work), wb, stream())
+    return H, di, float(lam)
 
 
 def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1e-14, info=None, return_y=False):
@@ -1006,8 +1176,9 @@ def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1
     passes over J per sweep), and y += C^-1 residual with the factor C as the
     preconditioner, until ||residual|| <= refine_tol ||r||.  ``info`` (a dict)
     receives the sweeps done and the last relative residual."""
-    M = J.shape[0]
-    dev = J.device
+    op = J if isinstance(J, (StoredJacobian, SlabJacobian)) else StoredJacobian(J, K, lo)
+    M = op.rows
+    dev = H.device
     rr = torch.as_tensor(np.ascontiguousarray(r, dtype=np.float64), device=dev) if not torch.is_tensor(r) else r
 
     def precond(v):
@@ -1020,32 +1191,42 @@ def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1
 
     y = precond(rr)
     sweeps, rel = 0, None
+    u_now = None  # J^T y for the current y, when a residual pass left it
     if refine:
         rnorm = norm2(rr) or 1.0
-        u = torch.empty(K, dtype=torch.float64, device=dev)
         res = torch.empty(M, dtype=torch.float64, device=dev)
         for it in range(int(refine)):
-            gemv_t(J, K, y, 1.0, out=u, lo=lo)  # u = J^T y
+            u, Ju = op.jt_then_j(y)
             res.copy_(rr)
-            gemv_n(J, K, u, -float(alpha), 1.0, out=res, lo=lo)  # res = r - alpha J u
+            call("rb_axpby", M, -float(alpha), ptr(Ju), 1.0, ptr(res), stream())  # res = r - alpha J J^T y
             call("rb_axpby", M, -float(lam), ptr(y), 1.0, ptr(res), stream())  # res -= lam y
             rel = norm2(res) / rnorm
             if rel <= refine_tol:
+                u_now = u
                 break
             call("rb_axpby", M, 1.0, ptr(precond(res)), 1.0, ptr(y), stream())
             sweeps = it + 1
     if info is not None:
         info.update(refine_sweeps=sweeps, refine_relres=rel, lam=float(lam))
-    return y if return_y else gemv_t(J, K, y, alpha, lo=lo)
+    if return_y:
+        return y
+    if u_now is not None:  # the last residual pass already formed J^T y
+        out = torch.empty_like(u_now)
+        call("rb_axpby", u_now.numel(), float(alpha), ptr(u_now), 0.0, ptr(out), stream())
+        return out
+    return op.jt(y, alpha)
 
 
 def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None, refine=3, refine_tol=1e-14,
-                        info=None):
+                        info=None, rowsq=None):
     """reginvunder (recon.py:429-509) for the rows of J (scaled by sqrt(alpha)):
     H = alpha J J^T + lam I on the tensor cores, unit-diagonal normalisation,
     FP64 Cholesky, FP64 refinement (normal_solve); returns alpha J^T y on the
-    device (K-vector, FP64)."""
-    H, di, lo, lam = normal_factor(J, K, lam, alpha, precision, lam_rel)
+    device (K-vector, FP64).  J is a stored matrix or a SlabJacobian."""
+    if isinstance(J, SlabJacobian):  # J recomputed slab by slab on every pass
+        H, di, lam = normal_factor_op(J, lam, alpha, precision, lam_rel, rowsq)
+        return normal_solve(J, K, H, di, r, lam, alpha, None, refine, refine_tol, info)
+    H, di, lo, lam = normal_factor(J, K, lam, alpha, precision, lam_rel, rowsq)
     return normal_solve(J, K, H, di, r, lam, alpha, lo, refine, refine_tol, info)
 
 

@@ -331,6 +331,24 @@ def _apply_param(cfg, recon, key, dx):
 
 
 # --------------------------------------------------------------- GN driver
+def _slab_width(jac_slab, mesh, phi, sd, nparams, dtype):
+    """Node slab width of a recomputed Jacobian, or 0 to store it whole."""
+    if jac_slab is None or jac_slab is False:
+        return 0
+    if not isinstance(jac_slab, str):
+        return int(jac_slab)
+    rows = int(np.count_nonzero(np.asarray(sd)[:, 2] == 1)) if np.asarray(sd).shape[1] >= 3 else len(sd)
+    rows *= 2 if phi.is_complex() else 1
+    esz = 2 if dtype == torch.bfloat16 else 4
+    full = rows * (nparams * mesh.nn + 8) * esz
+    free = torch.cuda.mem_get_info(phi.device)[0]
+    if full <= 0.5 * free:
+        return 0
+    # slabs of a quarter of the free memory (the gram's staging copy and
+    # the split remainder of tf32x3 come on top of the slab itself)
+    return max(1024, int(0.25 * free / (rows * nparams * esz)))
+
+
 def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     """Gauss-Newton reconstruction (recon.py:39-335) with the forward model,
     Jacobian and normal equations on the GPU.  Returns
@@ -344,7 +362,11 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     coefficients from ``extin=`` / ``cfg['extin']`` or redbirdpy's spectra),
     one mesh or a separate reconstruction mesh (``recon['node']``,
     ``recon['elem']``, ``recon['mapid']``, ``recon['mapweight']``),
-    reform 'real', 'reim' or 'logphase'.  Structural priors raise
+    reform 'real', 'reim' or 'logphase'.  On one mesh and wavelength with
+    reform 'real', a Jacobian larger than half the free HBM is not stored:
+    ``jac_slab`` (default 'auto'; an int sets the node slab width) makes
+    every pass over J recompute it slab by slab from the stored fields, and
+    the returned 'mua' entry is then that operator.  Structural priors raise
     NotImplementedError."""
     from .forward import jacchrome  # noqa: F401  (the same weights, as numpy / tensors)
     from .property import CHROMOPHORES, extinction, updateprop
@@ -360,6 +382,10 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     gram_prec = kwargs.get("gram", "tf32")
     lambda_rule = kwargs.get("lambda_rule", "fixed")
     refine = kwargs.get("refine", 3)
+    # Jacobian storage: 'auto' stores J when it fits in half the free HBM and
+    # otherwise recomputes it in node slabs; an int forces slabs that wide;
+    # None/False always stores it
+    jac_slab = kwargs.get("jac_slab", "auto")
     extin = kwargs.get("extin", cfg.get("extin"))
     # each forward solve starts from the previous iterate's fields (the
     # refinement then only removes what the property update changed)
@@ -414,8 +440,13 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
         sds = [sd.get(wv, sd) if isinstance(sd, dict) else sd for wv in wavelengths]
         if fast:
             params = ("mua",) if param == "mua" else ("mua", "D")
-            J, K = engine.jacobian_matrix(mesh, phis[0], sds[0], params, jac_mode,
-                                          dtype=torch.bfloat16 if gram_prec == "bf16" else torch.float32)
+            jdt = torch.bfloat16 if gram_prec == "bf16" else torch.float32
+            width = _slab_width(jac_slab, mesh, phis[0], sds[0], len(params), jdt)
+            if width:  # J recomputed in node slabs on every pass instead of stored
+                J = engine.SlabJacobian(mesh, phis[0], sds[0], params, jac_mode, width, jdt)
+                K = J.K
+            else:
+                J, K = engine.jacobian_matrix(mesh, phis[0], sds[0], params, jac_mode, dtype=jdt)
             misfit = y0s[0] - dets[0].cpu().numpy().ravel()
             if np.iscomplexobj(misfit):
                 misfit = np.concatenate([np.real(misfit), np.imag(misfit)])
@@ -431,18 +462,24 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
                 weights = {wv: np.ones(1) for wv in wavelengths}
             J, K, misfit = _stacked_matrix(mesh, phis, sds, dets, y0s, wavelengths, weights, nq, remap, reform)
         resid[it] = np.sum(np.abs(misfit))
-        scale2 = 1.0 / float(engine.sumsq(J, K).item())  # blockscale^2 (recon.py:235-240)
-        if J.shape[0] >= K:  # overdetermined: (J^T J + lambda I)^-1 J^T r on the host-side path
+        slabs = isinstance(J, engine.SlabJacobian)
+        # row sums of squares: the Frobenius block scale and the exact
+        # diagonal of J J^T in one pass
+        rowsq, ssq = J.row_sumsq() if slabs else engine.row_sumsq(J, K)
+        scale2 = 1.0 / float(ssq.item())  # blockscale^2 (recon.py:235-240)
+        if slabs and J.rows >= K:
+            raise NotImplementedError("an overdetermined system is solved on the host path: it needs J stored")
+        if not slabs and J.shape[0] >= K:  # overdetermined: (J^T J + lambda I)^-1 J^T r on the host-side path
             Js = J[:, :K].float().cpu().numpy().astype(np.float64) * np.sqrt(scale2)
             dmu = reginvover(Js, misfit, lambda_) * np.sqrt(scale2)
         else:
             rinfo = {}
             if lambda_rule == "maxdiag":
                 dmu = engine.reginv_under_device(J, K, misfit, 0.0, scale2, gram_prec, lam_rel=lambda_,
-                                                 refine=refine, info=rinfo)
+                                                 refine=refine, info=rinfo, rowsq=rowsq)
             else:
                 dmu = engine.reginv_under_device(J, K, misfit, lambda_, scale2, gram_prec, refine=refine,
-                                                 info=rinfo)
+                                                 info=rinfo, rowsq=rowsq)
             dmu = dmu.cpu().numpy()
         upd = {}
         for b, key in enumerate(keys):
@@ -470,9 +507,12 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
             resid = resid[: it + 1]
             break
     recon["lambda"] = lambda_
-    Jout = J[:, :K]
-    if Jout.numel() * 4 < 2 ** 31:
-        Jout = Jout.float().cpu().numpy()
+    if isinstance(J, engine.SlabJacobian):
+        Jout = J  # never stored whole: the operator that recomputes its slabs
+    else:
+        Jout = J[:, :K]
+        if Jout.numel() * 4 < 2 ** 31:
+            Jout = Jout.float().cpu().numpy()
     if len(wavelengths) == 1:
         det_out, phi_out = dets[0].cpu().numpy(), phis[0].cpu().numpy()
     else:

@@ -358,3 +358,67 @@ def test_reform_recon_matches_reference(golden, form):
     for k, key in enumerate(("dmu0", "dmu1")):
         err = np.abs(upd[k]["mua"] - g[key]).max() / np.abs(g[key]).max()
         assert err < 2e-6, (key, err)
+
+
+@pytest.mark.parametrize("case,param", [("nodal_cw", "mua"), ("nodal_fd", "mua+D")])
+def test_runrecon_with_recomputed_jacobian_slabs(golden, case, param):
+    """A GN loop whose Jacobian is never stored (node slabs recomputed on
+    every pass: the Frobenius sum, the tensor-core product, each refinement
+    residual and the update) against the same loop with J stored."""
+    m = golden(case)
+    out = {}
+    for slab in (None, 97):
+        cfg = cfg_from(m)
+        truth = cfg["prop"].copy()
+        bump = np.linalg.norm(cfg["node"] - np.array([20.0, 20.0, 6.0]), axis=1) < 8
+        truth[bump, 0] *= 1.5
+        cfg_t = dict(cfg)
+        cfg_t.pop("_b200", None)
+        cfg_t["prop"] = truth
+        det0, _ = rbb.run(cfg_t)
+        recon = {"prop": cfg["prop"].copy()}
+        res = rbb.run(cfg, recon, det0, m["sd"], maxiter=2, lambda_=0.05, report=False, param=param,
+                      jac_slab=slab)
+        out[slab] = res
+    (r0, s0, _, u0, J0, _, _), (r1, s1, _, u1, J1, _, _) = out[None], out[97]
+    from redbirdpy_b200.engine import SlabJacobian
+
+    assert isinstance(J1["mua"], SlabJacobian) and J1["mua"].passes >= 3
+    np.testing.assert_allclose(s1, s0, rtol=1e-9)
+    for a, b in zip(u0, u1):
+        for key in a:
+            e = np.abs(a[key] - b[key]).max() / np.abs(a[key]).max()
+            assert e <= 1e-7, (key, e)
+    np.testing.assert_allclose(r1["prop"], r0["prop"], rtol=1e-9)
+
+
+@pytest.mark.parametrize("precision", ["tf32", "bf16"])
+def test_relative_lambda_uses_the_exact_diagonal(precision):
+    """lam = 0.05 max diag(s J J^T) taken from the FP64 row sums of the stored
+    rows, not from the tensor-core product: the refined update then equals
+    the FP64 solution of the stored rows' system (TF32 or BF16 rows alike)."""
+    rng = np.random.default_rng(11)
+    M, K = 300, 5000
+    A = rng.standard_normal((M, K)) * np.exp(rng.uniform(-2, 2, K))
+    if precision == "bf16":
+        J, K_, Ad = _bf16_rows(A)
+        gram_prec = "bf16"
+    else:
+        J = torch.zeros((M, (K + 3) // 4 * 4), dtype=torch.float32, device="cuda")
+        J[:, :K] = torch.as_tensor(A, dtype=torch.float32, device="cuda")
+        Ad = J[:, :K].double().cpu().numpy()
+        gram_prec = "tf32"
+    rows, tot = engine.row_sumsq(J, K)
+    np.testing.assert_allclose(rows.cpu().numpy(), np.sum(Ad * Ad, axis=1), rtol=1e-12)
+    np.testing.assert_allclose(float(tot.item()), np.sum(Ad * Ad), rtol=1e-12)
+    s2 = 1.0 / float(tot.item())
+    r = rng.standard_normal(M)
+    info = {}
+    got = engine.reginv_under_device(J, K, r, 0.0, s2, gram_prec, lam_rel=0.05, rowsq=rows, refine=12,
+                                     info=info).cpu().numpy()
+    H = s2 * Ad @ Ad.T
+    lam = 0.05 * H.diagonal().max()
+    y = np.linalg.solve(H + lam * np.eye(M), r)
+    ref = s2 * Ad.T @ y
+    assert abs(info["lam"] - lam) <= 1e-12 * lam
+    assert np.abs(got - ref).max() <= 1e-8 * np.abs(ref).max(), info
