@@ -168,9 +168,17 @@ def run_b200(args):
     from redbirdpy_b200 import engine
 
     rank, world, local = dist_setup(args.gpus)
+    # meshprep of the 3M-tet box (reorientation, faces, areas, volumes, CSR
+    # pattern and incidence on the device), after a small one that loads the
+    # library and creates the context
+    rbb.meshprep(workload_cfg(spacing=10.0))
+    torch.cuda.synchronize()
     cfg = workload_cfg()
+    t0 = time.perf_counter()
     cfg, sd = rbb.meshprep(cfg)
     mesh = engine.mesh_of(cfg)
+    torch.cuda.synchronize()
+    meshprep_s = time.perf_counter() - t0
     optics = engine.Optics.from_cfg(mesh, cfg)
     nrhs = cfg["srcpos"].shape[0] + cfg["detpos"].shape[0]
 
@@ -326,6 +334,11 @@ def run_b200(args):
         "e2e": {"value": round(world * nrhs / e2e_s, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk,
+        "meshprep": {"seconds": round(meshprep_s, 3),
+                     "what": "rbb.meshprep + device mesh (reorientation, boundary faces, areas, tet and node "
+                             "volumes, incidence, CSR pattern, assembly tables) of the 3M-tet box, host arrays in",
+                     "reference_seconds": 95, "reference_source": "the survey's probe of redbirdpy's meshprep "
+                                                                  "(numpy fallbacks, _femnz loop) at this size"},
     }
     # each section starts with torch's cached device memory released: the GN
     # section leaves tens of GB of Jacobian blocks in the allocator's cache
@@ -413,7 +426,7 @@ def run_gn_step(cfg, mesh, world, args):
     state = {"phi": None}
     refine = 3  # FP64 refinement sweeps of the normal equations (at most)
 
-    def step_mixed(jdtype=torch.float32, apply=True, gram_prec="tf32"):
+    def step_mixed(jdtype=torch.float32, apply=True, gram_prec="bf16"):
         # one iteration of the GN loop: the forward solve starts from the
         # previous iterate's fields, and the update is applied at the end
         det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg, x0=state["phi"]))
@@ -425,11 +438,16 @@ def run_gn_step(cfg, mesh, world, args):
         # row sums of squares: the Frobenius scale and the exact diagonal of
         # J J^T (the product's own diagonal carries the TF32 input rounding,
         # which lam = 0.05 max(diag) would inherit)
-        rowsq, tot = timed_stage("sumsq", lambda: engine.row_sumsq(J, K))
+        bfc = gram_prec == "bf16" and J.dtype == torch.float32
+        sums = timed_stage("sumsq", lambda: engine.row_sumsq(J, K, bf16_copy=bfc))
+        rowsq, tot = sums[0], sums[1]
         s2 = 1.0 / float(tot.item())
         # tf32x3 leaves J as its TF32 part and returns the remainder: the
-        # refinement below runs over both, i.e. over the FP32 rows
-        H, lo = timed_stage("gram", lambda: engine.gram(J, K, s2, gram_prec))
+        # refinement below runs over both, i.e. over the FP32 rows; 'bf16'
+        # forms the product from the BF16 copy made in the same pass as the
+        # row sums and refines over the FP32 rows
+        H, lo = timed_stage("gram", lambda: engine.gram(sums[2] if bfc else J, K, s2, gram_prec))
+        del sums
         engine.call("rb_set_diag", engine.ptr(H), H.shape[0], H.shape[0], engine.ptr(rowsq), s2, engine.stream())
         lam = 0.05 * float(H.diagonal().max().item())
         M = J.shape[0]
@@ -529,38 +547,27 @@ def run_gn_step(cfg, mesh, world, args):
     tiles = nbt * (nbt + 1) // 2  # 256 x 256 tiles on or above the diagonal
     gram_flop = tiles * 256 * 256 * K * 2
     gram_ms = mixed_stages.get("gram")
-    # the BF16 form of the same iteration (Jacobian rows rounded to BF16, the
-    # kind::f16 MMA): same state as the FP64 comparison
-    bf16 = tf32x3 = None
+    # the same iteration with the product in TF32 (kind::tf32 on the FP32
+    # rows themselves), same state as the FP64 comparison
+    tf32 = None
     if not args.no_fp64_gn:
         gcfg["prop"] = snap[0].copy()
         state["phi"] = snap[1]
-        step_mixed(torch.bfloat16, apply=False)  # first call of the BF16 kernels
+        step_mixed(apply=False, gram_prec="tf32")  # first call of the TF32 kernels
         torch.cuda.synchronize()
         stages.clear()
         b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         b0.record()
-        dmu_b = step_mixed(torch.bfloat16, apply=False)
+        dmu_t = step_mixed(apply=False, gram_prec="tf32")
         b1.record()
         torch.cuda.synchronize()
-        bms = max_over_ranks(b0.elapsed_time(b1), world)
-        bf16 = {"ms_per_iter": round(bms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
-                "speedup_vs_fp64": round(ms64 / bms, 3), "iters_per_s": round(1e3 / bms, 4) * world,
-                "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_b - dmu64) / np.linalg.norm(dmu64)),
+        tms = max_over_ranks(b0.elapsed_time(b1), world)
+        tf32 = {"ms_per_iter": round(tms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
+                "speedup_vs_fp64": round(ms64 / tms, 3), "iters_per_s": round(1e3 / tms, 4) * world,
+                "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_t - dmu64) / np.linalg.norm(dmu64)),
                 "gram_tflops": round(tiles_flop(mesh) / (stages["gram"] * 1e-3) / 1e12, 1),
-                "note": "BF16 Jacobian rows: the refinement converges to the BF16-rounded J's system"}
-        # split-TF32 J J^T (three products, hi/lo), same state
-        step_mixed(apply=False, gram_prec="tf32x3")
-        torch.cuda.synchronize()
-        stages.clear()
-        b0.record()
-        dmu_x3 = step_mixed(apply=False, gram_prec="tf32x3")
-        b1.record()
-        torch.cuda.synchronize()
-        x3ms = max_over_ranks(b0.elapsed_time(b1), world)
-        tf32x3 = {"ms_per_iter": round(x3ms, 1), "breakdown_ms": {k: round(v, 2) for k, v in stages.items()},
-                  "speedup_vs_fp64": round(ms64 / x3ms, 3),
-                  "dmu_rel_err_vs_fp64": float(np.linalg.norm(dmu_x3 - dmu64) / np.linalg.norm(dmu64))}
+                "refinement": dict(state.get("refine", {})),
+                "note": "J J^T on the FP32 rows in TF32 (kind::tf32); the FP64 refinement runs over the same rows"}
     # the same iteration with the Jacobian never stored: node slabs of a
     # quarter of the mesh recomputed on every pass (the mode a mesh whose J
     # exceeds HBM takes), same state as the FP64 comparison
@@ -576,7 +583,7 @@ def run_gn_step(cfg, mesh, world, args):
             mis = np.concatenate([mis.real, mis.imag])
             rowsq, tot = op.row_sumsq()
             s2 = 1.0 / float(tot.item())
-            H, di, lam = engine.normal_factor_op(op, 0.0, s2, "tf32", lam_rel=0.05, rowsq=rowsq)
+            H, di, lam = engine.normal_factor_op(op, 0.0, s2, "bf16", lam_rel=0.05, rowsq=rowsq)
             rinfo = {}
             dmu = engine.normal_solve(op, op.K, H, di, mis, lam, s2, None, refine=refine, info=rinfo)
             return dmu.cpu().numpy(), op.passes, rinfo
@@ -606,9 +613,10 @@ def run_gn_step(cfg, mesh, world, args):
         pk_sus = float(mp.get("bf16_tflops_sustained") or pk_sus)
     return {
         "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
-                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, TF32 J J^T + FP64 refinement of the normal "
-                    f"equations; GN iterations 2..{ks + 1} of the loop (forward warm-started "
-                    f"from the previous iterate's fields), iteration 1 untimed",
+                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, J J^T on the tensor cores from their BF16 "
+                    f"copy (made in the row-sum pass) + FP64 refinement of the normal equations over the FP32 rows; "
+                    f"lam = 0.05 max diag(J J^T) from the exact row sums; GN iterations 2..{ks + 1} of the loop "
+                    f"(forward warm-started from the previous iterate's fields), iteration 1 untimed",
         "iters_per_s": round(1e3 / ms, 4) * world, "ms_per_iter": round(ms, 1), "breakdown_ms": mixed_stages,
         "fp64_iters_per_s": round(1e3 / ms64, 4) * world if ms64 else None,
         "fp64_ms_per_iter": round(ms64, 1) if ms64 else None,
@@ -616,19 +624,17 @@ def run_gn_step(cfg, mesh, world, args):
         "dmu_rel_err_vs_fp64": err,
         "forward_det_max_rel_err_vs_fp64": det_err,
         "refinement": refine_info,
-        "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel (tcgen05 kind::tf32, FP32 accumulation "
-                                                       "drained to FP64, 256x256 tiles)",
+        "roofline_gram": {"bound": "tensor", "kernel": "gram_tf32_kernel<true> (tcgen05 kind::f16, BF16 A and B, "
+                                                       "FP32 accumulation drained to FP64, 256x256 tiles)",
                           "achieved": round(tflops, 1) if tflops else None, "unit": "TFLOP/s",
                           "algorithmic_flop": gram_flop, "peak": pk, "peak_source": pk_src,
-                          "frac_of_bf16": round(tflops / pk, 4) if (tflops and pk) else None,
-                          "sustained_bf16_peak": pk_sus,
-                          "frac_of_sustained_tf32": (round(tflops / (0.5 * pk_sus), 4)
-                                                     if (tflops and pk_sus) else None),
-                          "note": "TF32 dense peak is half the BF16 one; the GN step runs at the power cap, "
-                                  "so the sustained figure is the one its clocks reach"},
+                          "frac": round(tflops / pk, 4) if (tflops and pk) else None,
+                          "sustained_peak": pk_sus,
+                          "frac_of_sustained": round(tflops / pk_sus, 4) if (tflops and pk_sus) else None,
+                          "note": "the GN step runs at the 1 kW power cap (sw_power_cap), where the clocks reach "
+                                  "the sustained figure"},
         "clocks": gn_clocks,
-        "bf16_form": bf16,
-        "tf32x3_form": tf32x3,
+        "tf32_form": tf32,
         "slab_recompute_form": slab,
     }
 
@@ -766,7 +772,7 @@ def run_adjoint(world, args):
     out["jacobian"] = {"rows": int(J.shape[0]), "cols": int(K), "ms": round(jms, 3),
                        "write_gbs": round(jbytes / (jms * 1e-3) / 1e9, 1),
                        "frac_of_hbm": round(jbytes / (jms * 1e-3) / 1e9 / peak, 4),
-                       "note": "includes the zero fill of J (torch) and both parameter launches"}
+                       "note": "both parameter launches (rb_jac: mua_nodal, D) and the clear of the row padding"}
     return out
 
 

@@ -510,6 +510,11 @@ int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out,
 int rb_row_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream);
 int rb_row_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total,
                       void* stream);
+/* rb_row_sumsq of FP32 rows that also writes them rounded to BF16 (row
+ * stride ldb >= K, a multiple of 8; padding zeroed) in the same pass: the
+ * operand of rb_gram_bf16 when the refinement runs over the FP32 rows. */
+int rb_row_sumsq_to_bf16(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* bf,
+                         int64_t ldb, void* stream);
 /* H[i][i] = alpha d[i] */
 int rb_set_diag(double* H, int64_t M, int64_t ldh, const double* d, double alpha, void* stream);
 int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* stream);

@@ -141,6 +141,7 @@ _SIGS = {
     "rb_row_sumsq": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _vp]),
     "rb_row_sumsq_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _vp]),
     "rb_set_diag": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, _vp]),
+    "rb_row_sumsq_to_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp]),
     "rb_gemv_n": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
     "rb_gemv_n_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
     "rb_axpby": (ctypes.c_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),

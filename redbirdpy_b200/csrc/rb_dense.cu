@@ -483,16 +483,23 @@ __global__ void sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int
 
 // out[m] = sum_k J[m][k]^2 in FP64: a block per row, a fixed-order
 // reduction (the diagonal of J J^T without the tensor cores' input rounding)
+// With bf != NULL the pass also writes the rows rounded to BF16 (row stride
+// ldb, the padding columns K..ldb-1 zeroed): the operand of a BF16 product
+// whose refinement runs over the FP32 rows.
 template <typename JT>
 __global__ void row_sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
-                                 double* __restrict__ out) {
+                                 double* __restrict__ out, __nv_bfloat16* __restrict__ bf, int64_t ldb) {
   __shared__ double red[32];
   for (int64_t m = blockIdx.x; m < M; m += gridDim.x) {
     double s = 0.0;
     for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-      const double v = jval(J[m * ldj + k]);
+      const JT x = J[m * ldj + k];
+      const double v = jval(x);
       s += v * v;
+      if (bf) bf[m * ldb + k] = __float2bfloat16_rn((float)v);
     }
+    if (bf)
+      for (int64_t k = K + threadIdx.x; k < ldb; k += blockDim.x) bf[m * ldb + k] = __float2bfloat16_rn(0.f);
     s = warp_sum(s);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -744,11 +751,13 @@ int rb_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* out,
 }  // extern "C"
 
 template <typename JT>
-static int row_sumsq_run(const JT* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream) {
+static int row_sumsq_run(const JT* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* stream,
+                         __nv_bfloat16* bf = nullptr, int64_t ldb = 0) {
   if (!J || !rows || M < 1 || K < 1 || ldj < K || M > INT32_MAX) return fail(RB_EARG, "rb_row_sumsq: bad arguments");
+  if (bf && (ldb < K || ldb % 8)) return fail(RB_EARG, "rb_row_sumsq_to_bf16: ldb must be >= K and a multiple of 8");
   cudaStream_t st = as_stream(stream);
   const unsigned nb = (unsigned)std::min<int64_t>(M, 148 * 16);
-  row_sumsq_kernel<JT><<<nb, 256, 0, st>>>(J, M, K, ldj, rows);
+  row_sumsq_kernel<JT><<<nb, 256, 0, st>>>(J, M, K, ldj, rows, bf, ldb);
   RB_LAUNCH_CHECK();
   if (total) {
     sum_parts_kernel<<<1, 1024, 0, st>>>(rows, (int)M, total);
@@ -766,6 +775,12 @@ int rb_row_sumsq(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows
 int rb_row_sumsq_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total,
                       void* stream) {
   return row_sumsq_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, rows, total, stream);
+}
+
+int rb_row_sumsq_to_bf16(const float* J, int64_t M, int64_t K, int64_t ldj, double* rows, double* total, void* bf,
+                         int64_t ldb, void* stream) {
+  if (!bf) return fail(RB_EARG, "rb_row_sumsq_to_bf16: null output");
+  return row_sumsq_run(J, M, K, ldj, rows, total, stream, reinterpret_cast<__nv_bfloat16*>(bf), ldb);
 }
 
 int rb_set_diag(double* H, int64_t M, int64_t ldh, const double* d, double alpha, void* stream) {

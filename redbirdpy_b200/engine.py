@@ -926,12 +926,22 @@ def sumsq(J, K):
     return out
 
 
-def row_sumsq(J, K):
+def row_sumsq(J, K, bf16_copy=False):
     """(rows, total): FP64 sums of squares of J's rows (the exact diagonal of
-    J J^T for the stored rows) and their sum (the Frobenius sum), one pass."""
+    J J^T for the stored rows) and their sum (the Frobenius sum), one pass.
+    ``bf16_copy`` (FP32 J): the same pass also returns J rounded to BF16
+    (rows, total, Jb), the operand of a BF16 product whose refinement runs
+    over the FP32 rows."""
     M = J.shape[0]
     rows = torch.empty(M, dtype=torch.float64, device=J.device)
     total = torch.empty(1, dtype=torch.float64, device=J.device)
+    if bf16_copy:
+        if J.dtype != torch.float32:
+            raise ValueError("a BF16 copy is made from FP32 rows")
+        Jb = torch.empty((M, _pad8(K)), dtype=torch.bfloat16, device=J.device)
+        call("rb_row_sumsq_to_bf16", ptr(J), M, K, J.shape[1], ptr(rows), ptr(total), ptr(Jb), Jb.shape[1],
+             stream())
+        return rows, total, Jb
     fn = "rb_row_sumsq_bf16" if J.dtype == torch.bfloat16 else "rb_row_sumsq"
     call(fn, ptr(J), M, K, J.shape[1], ptr(rows), ptr(total), stream())
     return rows, total
@@ -940,7 +950,10 @@ def row_sumsq(J, K):
 def gram(J, K, alpha=1.0, precision="tf32"):
     """H = alpha J J^T (M x M FP64) on the tensor cores.  precision 'tf32'
     (one pass) or 'tf32x3' (split hi/lo, three passes; J is left as hi and
-    the returned lo completes it); a BF16 J takes the BF16 MMA."""
+    the returned lo completes it); a BF16 J takes the BF16 MMA, and so does
+    'bf16' with FP32 rows (on a BF16 copy of them)."""
+    if precision == "bf16" and J.dtype == torch.float32:  # the product from a BF16 copy
+        J = row_sumsq(J, K, bf16_copy=True)[2]
     M, ldj = J.shape
     H = torch.empty((M, M), dtype=torch.float64, device=J.device)
     lo = None
@@ -988,16 +1001,19 @@ def norm2(x):
     return float(out.item()) ** 0.5
 
 
-def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None, rowsq=None):
+def normal_factor(J, K, lam, alpha=1.0, precision="tf32", lam_rel=None, rowsq=None, Jb=None):
     """The tensor-core half of reginvunder (recon.py:474-483): H = alpha J J^T
     (+ lam I, lam relative to the largest diagonal entry with ``lam_rel``),
     unit-diagonal normalisation (_normalize_diag, recon.py:784-789), FP64
     Cholesky in place.  ``rowsq`` (row_sumsq's rows) replaces the product's
     diagonal by the exact one, so that a relative lam and the normalisation
-    carry no tensor-core input rounding.  Returns (H, di, lo, lam)."""
+    carry no tensor-core input rounding.  ``Jb`` (J rounded to BF16, from
+    row_sumsq) is the product's operand when given: a BF16 factor of the
+    FP32 rows' system, which normal_solve then refines over those rows.
+    Returns (H, di, lo, lam)."""
     M, ldj = J.shape
     dev = J.device
-    H, lo = gram(J, K, alpha, precision)
+    H, lo = gram(Jb if Jb is not None else J, K, alpha, precision)
     if rowsq is not None:
         call("rb_set_diag", ptr(H), M, M, ptr(rowsq), float(alpha), stream())
     if lam_rel is not None:
@@ -1110,7 +1126,8 @@ class SlabJacobian:
 
     def gram(self, alpha=1.0, precision="tf32"):
         """H = alpha sum over slabs of J_s J_s^T (FP64 accumulation of the
-        tensor-core products of each slab)."""
+        tensor-core products of each slab; 'bf16' with FP32 slabs forms the
+        product from a BF16 copy of each slab)."""
         M = self.rows
         H = torch.zeros((M, M), dtype=torch.float64, device=self.phi.device)
         for a, b in self.ranges():
@@ -1218,7 +1235,7 @@ def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1
 
 
 def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None, refine=3, refine_tol=1e-14,
-                        info=None, rowsq=None):
+                        info=None, rowsq=None, Jb=None):
     """reginvunder (recon.py:429-509) for the rows of J (scaled by sqrt(alpha)):
     H = alpha J J^T + lam I on the tensor cores, unit-diagonal normalisation,
     FP64 Cholesky, FP64 refinement (normal_solve); returns alpha J^T y on the
@@ -1226,7 +1243,7 @@ def reginv_under_device(J, K, r, lam, alpha=1.0, precision="tf32", lam_rel=None,
     if isinstance(J, SlabJacobian):  # J recomputed slab by slab on every pass
         H, di, lam = normal_factor_op(J, lam, alpha, precision, lam_rel, rowsq)
         return normal_solve(J, K, H, di, r, lam, alpha, None, refine, refine_tol, info)
-    H, di, lo, lam = normal_factor(J, K, lam, alpha, precision, lam_rel, rowsq)
+    H, di, lo, lam = normal_factor(J, K, lam, alpha, precision, lam_rel, rowsq, Jb)
     return normal_solve(J, K, H, di, r, lam, alpha, lo, refine, refine_tol, info)
 
 

@@ -379,7 +379,10 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     solverflag = kwargs.get("solverflag", {}) or {}
     param = kwargs.get("param", "mua")
     jac_mode = kwargs.get("jac_mode", "reference" if param == "mua" else "exact")
-    gram_prec = kwargs.get("gram", "tf32")
+    # J J^T on the tensor cores from a BF16 copy of the FP32 rows (twice the
+    # TF32 rate); the FP64 refinement over the FP32 rows makes the update the
+    # FP32 rows' solution whatever the product's precision
+    gram_prec = kwargs.get("gram", "bf16")
     lambda_rule = kwargs.get("lambda_rule", "fixed")
     refine = kwargs.get("refine", 3)
     # Jacobian storage: 'auto' stores J when it fits in half the free HBM and
@@ -440,7 +443,10 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
         sds = [sd.get(wv, sd) if isinstance(sd, dict) else sd for wv in wavelengths]
         if fast:
             params = ("mua",) if param == "mua" else ("mua", "D")
-            jdt = torch.bfloat16 if gram_prec == "bf16" else torch.float32
+            # 'bf16': FP32 rows, a BF16 copy for the product (the refinement
+            # runs over the FP32 rows); 'bf16_rows': the rows themselves in
+            # BF16 (half the memory; the step solves the rounded rows' system)
+            jdt = torch.bfloat16 if gram_prec == "bf16_rows" else torch.float32
             width = _slab_width(jac_slab, mesh, phis[0], sds[0], len(params), jdt)
             if width:  # J recomputed in node slabs on every pass instead of stored
                 J = engine.SlabJacobian(mesh, phis[0], sds[0], params, jac_mode, width, jdt)
@@ -465,7 +471,14 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
         slabs = isinstance(J, engine.SlabJacobian)
         # row sums of squares: the Frobenius block scale and the exact
         # diagonal of J J^T in one pass
-        rowsq, ssq = J.row_sumsq() if slabs else engine.row_sumsq(J, K)
+        Jb = None
+        if slabs:
+            rowsq, ssq = J.row_sumsq()
+        elif gram_prec == "bf16" and J.dtype == torch.float32:
+            rowsq, ssq, Jb = engine.row_sumsq(J, K, bf16_copy=True)
+        else:
+            rowsq, ssq = engine.row_sumsq(J, K)
+        gprec = "bf16" if gram_prec == "bf16_rows" else gram_prec
         scale2 = 1.0 / float(ssq.item())  # blockscale^2 (recon.py:235-240)
         if slabs and J.rows >= K:
             raise NotImplementedError("an overdetermined system is solved on the host path: it needs J stored")
@@ -475,11 +488,12 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
         else:
             rinfo = {}
             if lambda_rule == "maxdiag":
-                dmu = engine.reginv_under_device(J, K, misfit, 0.0, scale2, gram_prec, lam_rel=lambda_,
-                                                 refine=refine, info=rinfo, rowsq=rowsq)
+                dmu = engine.reginv_under_device(J, K, misfit, 0.0, scale2, gprec, lam_rel=lambda_,
+                                                 refine=refine, info=rinfo, rowsq=rowsq, Jb=Jb)
             else:
-                dmu = engine.reginv_under_device(J, K, misfit, lambda_, scale2, gram_prec, refine=refine,
-                                                 info=rinfo, rowsq=rowsq)
+                dmu = engine.reginv_under_device(J, K, misfit, lambda_, scale2, gprec, refine=refine,
+                                                 info=rinfo, rowsq=rowsq, Jb=Jb)
+            del Jb
             dmu = dmu.cpu().numpy()
         upd = {}
         for b, key in enumerate(keys):

@@ -277,17 +277,21 @@ def test_jacobian_bf16_rows(golden, case):
     assert (torch.abs(a - b) <= 2.0 ** -8 * torch.abs(a) + 1e-30).all()
 
 
-def test_runrecon_bf16_matches_reference(golden):
+@pytest.mark.parametrize("gram,tol", [("bf16", 2e-6), ("bf16_rows", 3e-2)])
+def test_runrecon_bf16_matches_reference(golden, gram, tol):
+    """'bf16': the product from a BF16 copy of the FP32 rows, refined over the
+    FP32 rows (the reference's step to the FP32 rows' accuracy); 'bf16_rows':
+    the rows themselves stored in BF16 (the rounded rows' step)."""
     g, m = golden("nodal_gn"), golden("nodal_cw")
     cfg = cfg_from(m)
     cfg["prop"] = g["prop0"].copy()
     recon = {"prop": g["prop0"].copy()}
     recon, resid, cfg, upd, J, det, phi = rbb.run(cfg, recon, g["detphi0"], m["sd"], maxiter=2, lambda_=0.05,
-                                                  report=False, gram="bf16")
-    np.testing.assert_allclose(resid, g["resid"], rtol=1e-2)
+                                                  report=False, gram=gram)
+    np.testing.assert_allclose(resid, g["resid"], rtol=max(tol, 1e-8) if gram == "bf16" else 1e-2)
     for k, key in enumerate(("dmu0", "dmu1")):
         ref = g[key]
-        assert np.abs(upd[k]["mua"] - ref).max() / np.abs(ref).max() < 3e-2, key
+        assert np.abs(upd[k]["mua"] - ref).max() / np.abs(ref).max() < tol, key
 
 
 def _nodal_cfg(m, omega=0.0):
@@ -392,14 +396,16 @@ def test_runrecon_with_recomputed_jacobian_slabs(golden, case, param):
     np.testing.assert_allclose(r1["prop"], r0["prop"], rtol=1e-9)
 
 
-@pytest.mark.parametrize("precision", ["tf32", "bf16"])
+@pytest.mark.parametrize("precision", ["tf32", "bf16", "bf16_of_fp32"])
 def test_relative_lambda_uses_the_exact_diagonal(precision):
     """lam = 0.05 max diag(s J J^T) taken from the FP64 row sums of the stored
     rows, not from the tensor-core product: the refined update then equals
-    the FP64 solution of the stored rows' system (TF32 or BF16 rows alike)."""
+    the FP64 solution of the stored rows' system (TF32 or BF16 rows alike,
+    and FP32 rows whose product comes from their BF16 copy)."""
     rng = np.random.default_rng(11)
     M, K = 300, 5000
     A = rng.standard_normal((M, K)) * np.exp(rng.uniform(-2, 2, K))
+    Jb = None
     if precision == "bf16":
         J, K_, Ad = _bf16_rows(A)
         gram_prec = "bf16"
@@ -407,15 +413,21 @@ def test_relative_lambda_uses_the_exact_diagonal(precision):
         J = torch.zeros((M, (K + 3) // 4 * 4), dtype=torch.float32, device="cuda")
         J[:, :K] = torch.as_tensor(A, dtype=torch.float32, device="cuda")
         Ad = J[:, :K].double().cpu().numpy()
-        gram_prec = "tf32"
-    rows, tot = engine.row_sumsq(J, K)
+        gram_prec = "tf32" if precision == "tf32" else "bf16"
+    if precision == "bf16_of_fp32":
+        rows, tot, Jb = engine.row_sumsq(J, K, bf16_copy=True)
+        np.testing.assert_array_equal(Jb[:, :K].float().cpu().numpy(),
+                                      J[:, :K].to(torch.bfloat16).float().cpu().numpy())
+        assert not Jb[:, K:].float().abs().sum().item()
+    else:
+        rows, tot = engine.row_sumsq(J, K)
     np.testing.assert_allclose(rows.cpu().numpy(), np.sum(Ad * Ad, axis=1), rtol=1e-12)
     np.testing.assert_allclose(float(tot.item()), np.sum(Ad * Ad), rtol=1e-12)
     s2 = 1.0 / float(tot.item())
     r = rng.standard_normal(M)
     info = {}
     got = engine.reginv_under_device(J, K, r, 0.0, s2, gram_prec, lam_rel=0.05, rowsq=rows, refine=12,
-                                     info=info).cpu().numpy()
+                                     info=info, Jb=Jb).cpu().numpy()
     H = s2 * Ad @ Ad.T
     lam = 0.05 * H.diagonal().max()
     y = np.linalg.solve(H + lam * np.eye(M), r)
