@@ -402,6 +402,17 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,
            int32_t rmax, int32_t emax, const double* evol, const double* ddd, void* stream);
+/* Pair products on the tensor cores: rb_jac / rb_jac_range take them
+ * (tcgen05 kind::tf32 with a hi/lo split of both operands, FP32 accuracy)
+ * when the pairs are the full source x detector grid (nsd < 0), the output
+ * is FP32 (RB_F32, or RB_JAC_SPLIT_F32 for complex fields), there are at
+ * most 128 sources and 64 detectors (128 for real fields) and rmax <= 32;
+ * otherwise the SIMT products.  rb_jac_tensor_cores(1) allows the tensor
+ * cores, 0 (the default) keeps the SIMT products.  The tensor-core
+ * kernel's waits are bounded: rb_jac_status synchronises the stream and
+ * returns RB_ECUDA (and clears the word) if one gave up since the last call. */
+int rb_jac_tensor_cores(int32_t on);
+int rb_jac_status(void* stream);
 /* rb_jac for the nodes node0 .. node0+count-1 only: J column c holds node
  * node0 + c (ldj >= count).  A GN step whose full J would not fit in HBM
  * forms its products from node slabs recomputed on demand. */

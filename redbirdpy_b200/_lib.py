@@ -115,6 +115,8 @@ _SIGS = {
     "rb_spmm": (ctypes.c_int, [ctypes.POINTER(RbCsr), _i32, _vp, _vp, _i64, _vp]),
     "rb_jac": (ctypes.c_int, [ctypes.POINTER(RbMesh), _i32, _vp, _i32, _i64, _vp, _i32, _i32, _i32, _vp, _vp,
                               _i64, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
+    "rb_jac_tensor_cores": (ctypes.c_int, [_i32]),
+    "rb_jac_status": (ctypes.c_int, [_vp]),
     "rb_jac_range": (ctypes.c_int, [ctypes.POINTER(RbMesh), _i32, _vp, _i32, _i64, _vp, _i32, _i32, _i32, _vp,
                                     _vp, _i64, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _i64, _i64, _vp]),
     "rb_jac_remap": (ctypes.c_int, [_vp, _i32, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp]),

@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "rb_common.cuh"
+#include "rb_tc.cuh"
 
 namespace rb {
 
@@ -50,40 +51,7 @@ constexpr int kGItems = 4;  // item indices the producer may claim ahead of the 
 constexpr int kGChunk = 128;
 constexpr int kGChunkTf32 = 512;
 constexpr int kGChunkBf16 = 256;  // the same 16384 K with 64 BF16 elements per K-block
-constexpr long long kGWaitLimit = 1LL << 24;  // polls before a wait gives up (seconds)
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-// bounded parity wait: false (and *err set) when the phase never completes
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
-  for (long long i = 0; i < kGWaitLimit; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  atomicExch(err, code);
-  return false;
-}
+constexpr long long kGWaitLimit = kTcWaitLimit;  // polls before a wait gives up (seconds)
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
   asm volatile(
@@ -93,46 +61,17 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
-// shared-memory matrix descriptor: K-major operand, 128-byte swizzle,
-// 8-row groups 1024 bytes apart (stride byte offset), descriptor version 1
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;                    // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1u << 46;                    // version
-  d |= (uint64_t)2u << 61;                    // SWIZZLE_128B
-  return d;
-}
-
 // instruction descriptor: D = F32, both operands K-major, M = 128, N = 256;
 // A = B = TF32 (kind::tf32, format 2) or A = B = BF16 (kind::f16, format 1)
-constexpr uint32_t kGIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kGN >> 3) << 17) |
-                             ((uint32_t)(kGMH >> 4) << 24);
-constexpr uint32_t kGIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGN >> 3) << 17) |
-                                 ((uint32_t)(kGMH >> 4) << 24);
+constexpr uint32_t kGIdesc = umma_idesc(2, kGMH, kGN);
+constexpr uint32_t kGIdescBf16 = umma_idesc(1, kGMH, kGN);
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(kGIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-      : "memory");
+  umma_tf32_i(tmem_d, a, b, kGIdesc, accumulate);
 }
 
-// both operands BF16 (one type for A and B, as kind::f16 requires)
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(kGIdescBf16), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+  umma_bf16_i(tmem_d, a, b, kGIdescBf16, accumulate);
 }
 
 // number of 128-row blocks of tile column bj that touch the upper triangle

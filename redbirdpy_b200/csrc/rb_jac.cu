@@ -17,8 +17,10 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "rb_common.cuh"
+#include "rb_tc.cuh"
 
 namespace rb {
 
@@ -129,11 +131,14 @@ __device__ __forceinline__ void jac_store(void* Jout, int64_t nsd, int64_t ldj, 
   }
 }
 
-template <typename C, typename In, int TN, bool SPLIT, bool GRID, bool BF>
-__global__ void __launch_bounds__(kJacThreads)
-jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
+// Steps 1-3 of a CTA's TN nodes (n0 ..): stage the neighbours' phi rows
+// (every column the pairs use, converted to C), build each node's B_n and
+// C_n = B_n Phi_det in shared memory (layout jac_layout).  Ends with a
+// barrier; step 4 (the pair products) is the caller's.
+template <typename C, typename In, int TN>
+__device__ __forceinline__ void jac_stage(const JacArgs& a, const In* __restrict__ phi, unsigned char* smem,
+                                          int64_t n0) {
   typedef typename JacT<C>::real R;
-  extern __shared__ __align__(16) unsigned char smem[];
   const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax;
   const int SP = jac_phi_stride<C>(rmax, nc), SC = jac_c_stride<C>(rmax, nd);
   const JacSmem L = jac_layout<C>(TN, rmax, nc, nd, emax);
@@ -148,8 +153,6 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   int16_t* slp = reinterpret_cast<int16_t*>(smem + L.lp);
   const int warp = tid_warp(), lane = threadIdx.x & 31;
   constexpr int kWarps = kJacThreads / 32;
-
-  const int64_t n0 = a.node0 + (int64_t)blockIdx.x * TN;
   const int tid = threadIdx.x;
   // 1. rows and incident tets of the TN nodes
   if (tid < TN) {
@@ -253,6 +256,22 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     }
   }
   __syncthreads();
+}
+
+template <typename C, typename In, int TN, bool SPLIT, bool GRID, bool BF>
+__global__ void __launch_bounds__(kJacThreads)
+jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax;
+  const int SP = jac_phi_stride<C>(rmax, nc), SC = jac_c_stride<C>(rmax, nd);
+  const JacSmem L = jac_layout<C>(TN, rmax, nc, nd, emax);
+  const C* sphi = reinterpret_cast<const C*>(smem + L.phi);
+  const C* sC = reinterpret_cast<const C*>(smem + L.C);
+  const int* srn = reinterpret_cast<const int*>(smem + L.nb) + TN * rmax;
+
+  const int64_t n0 = a.node0 + (int64_t)blockIdx.x * TN;
+  const int tid = threadIdx.x;
+  jac_stage<C, In, TN>(a, phi, smem, n0);
   // 4. J[k][n] = sum_a phi[a][src k] C_n[a][det k]
   if constexpr (GRID) {
     // all (source, detector) combinations, k = d * nsrc + s (sdmap's
@@ -338,6 +357,251 @@ __global__ void jac_elem_kernel(const double* __restrict__ evol, const int32_t* 
   }
 }
 
+// ------------------------------------------- step 4 on the tensor cores
+// For the full (source x detector) grid with FP32 output, the pair products
+// of node t, P_t[s][d] = sum_a phi[a][s] C_t[a][d], are one tcgen05 MMA
+// D_t (128 x N) = A_t (128 x K) B_t^T (N x K), K along the node's row:
+//   B_t row n = source n: Re phi[a][n] for a < k8, then Im phi[a][n];
+//   A_t row d (d < ndet): Re C[a][d], then -Im C[a][d];
+//   A_t row 64 + d (complex): Im C[a][d], then Re C[a][d];
+// so that D row d holds Re P[.][d] and D row 64 + d Im P[.][d] (real
+// fields: K = k8, rows d only).  k8 = rmax rounded up to 8.  The operands
+// are written into shared memory in the 128-byte-swizzled K-major layout
+// (rb_tc.cuh) as TF32 pairs x = hi + lo, and D = hi hi + hi lo + lo hi
+// (three MMAs per 8-wide K step) keeps FP32 accuracy.  The TN accumulators
+// (N columns each) stay in tensor memory until the epilogue: a thread owns
+// one D row (one detector, real or imaginary part) and writes, per source,
+// the TN consecutive node columns of that J row at once.
+constexpr int kJtcTN = 4;
+
+struct JtcLayout {
+  size_t ahi, alo, bhi, blo, bar, total;
+  int Kp, N, k8;
+};
+
+template <typename C>
+__host__ __device__ inline JtcLayout jtc_layout(int rmax, int nc, int ndet, int emax, int nsu) {
+  JtcLayout T;
+  T.k8 = (rmax + 7) / 8 * 8;
+  T.Kp = Scalar<C>::is_complex ? 2 * T.k8 : T.k8;
+  T.N = (nsu + 31) / 32 * 32;
+  size_t o = (jac_smem<C>(kJtcTN, rmax, nc, ndet, emax) + 1023) / 1024 * 1024;
+  // a swizzle atom row is 128 bytes (32 TF32) whatever Kp: whole atoms
+  const int atoms = (T.Kp + 31) / 32;
+  const size_t ab = (size_t)128 * 128 * atoms, bb = (size_t)T.N * 128 * atoms;  // multiples of 1024
+  T.ahi = o;
+  T.alo = o + ab;
+  T.bhi = o + 2 * ab;
+  T.blo = o + 2 * ab + bb;
+  T.bar = o + 2 * ab + 2 * bb;
+  T.total = T.bar + 64 + 1024;  // the kernel aligns its base up to 1024 bytes
+  return T;
+}
+
+// byte offset of element (r, k) of a K-major 128-byte-swizzled operand of R
+// rows: K atoms of 32 elements are R x 128-byte blocks one after the other
+__device__ __forceinline__ uint32_t sw128_off(int r, int k, int R) {
+  const int atom = k >> 5, kk = k & 31;
+  return (uint32_t)(atom * R * 128 + (r >> 3) * 1024 + (r & 7) * 128 + (((kk >> 2) ^ (r & 7)) << 4) + ((kk & 3) << 2));
+}
+
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  uint32_t h, l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  hi = __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
+  lo = __uint_as_float(l);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
+template <typename C, typename In>
+__global__ void __launch_bounds__(kJacThreads, 1)
+jac_tc_kernel(JacArgs a, const In* __restrict__ phi, float* __restrict__ Jout, uint32_t tmem_cols,
+              int* __restrict__ err) {
+  constexpr bool CPLX = Scalar<C>::is_complex;
+  constexpr int TN = kJtcTN;
+  extern __shared__ __align__(1024) unsigned char jsm_raw[];
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(jsm_raw) + 1023) & ~uintptr_t(1023));
+  const int rmax = a.rmax, nc = a.nc, nd = a.ndet, emax = a.emax, nsu = a.det0;
+  const JtcLayout T = jtc_layout<C>(rmax, nc, nd, emax, nsu);
+  const JacSmem L = jac_layout<C>(TN, rmax, nc, nd, emax);
+  const int SP = jac_phi_stride<C>(rmax, nc), SC = jac_c_stride<C>(rmax, nd);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T.bar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  int* sflag = reinterpret_cast<int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    mbar_init(smem_u32(bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *sflag = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const int64_t n0 = a.node0 + (int64_t)blockIdx.x * TN;
+  jac_stage<C, In, TN>(a, phi, smem, n0);
+  const C* sphi = reinterpret_cast<const C*>(smem + L.phi);
+  const C* sC = reinterpret_cast<const C*>(smem + L.C);
+  const int* srn = reinterpret_cast<const int*>(smem + L.nb) + TN * rmax;
+  const int Kp = T.Kp, N = T.N, k8 = T.k8;
+  unsigned char* Ahi = smem + T.ahi;
+  unsigned char* Alo = smem + T.alo;
+  unsigned char* Bhi = smem + T.bhi;
+  unsigned char* Blo = smem + T.blo;
+  const uint32_t idesc = umma_idesc(2, 128, (uint32_t)N);
+  int nmma = 0;  // commits issued (parity of the next wait)
+  bool ok = true;
+  for (int t = 0; t < TN && ok; ++t) {
+    const int rn = srn[t];
+    // consecutive threads take consecutive rows of one K column: the staged
+    // C and phi values they read are consecutive in shared memory
+    for (int i = tid; i < 128 * Kp; i += kJacThreads) {
+      const int k = i >> 7, m = i & 127;
+      float x = 0.f;
+      if constexpr (CPLX) {
+        const int hk = k >= k8 ? 1 : 0, q = k - hk * k8;
+        const int d = m < 64 ? m : m - 64;
+        if (q < rn && d < nd) {
+          const C c = sC[(size_t)t * SC + (size_t)q * nd + d];
+          x = (m < 64) ? (hk ? -c.y : c.x) : (hk ? c.x : c.y);
+        }
+      } else {
+        if (k < rn && m < nd) x = sC[(size_t)t * SC + (size_t)k * nd + m];
+      }
+      float h, l;
+      tf32_split(x, h, l);
+      const uint32_t off = sw128_off(m, k, 128);
+      *reinterpret_cast<float*>(Ahi + off) = h;
+      *reinterpret_cast<float*>(Alo + off) = l;
+    }
+    for (int i = tid; i < N * Kp; i += kJacThreads) {
+      const int k = i / N, n = i - k * N;
+      float x = 0.f;
+      if constexpr (CPLX) {
+        const int hk = k >= k8 ? 1 : 0, q = k - hk * k8;
+        if (q < rn && n < nsu) {
+          const C v = sphi[(size_t)t * SP + (size_t)q * nc + n];
+          x = hk ? v.y : v.x;
+        }
+      } else {
+        if (k < rn && n < nsu) x = sphi[(size_t)t * SP + (size_t)k * nc + n];
+      }
+      float h, l;
+      tf32_split(x, h, l);
+      const uint32_t off = sw128_off(n, k, N);
+      *reinterpret_cast<float*>(Bhi + off) = h;
+      *reinterpret_cast<float*>(Blo + off) = l;
+    }
+    // the operands written by the threads become visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t dcol = tmem + (uint32_t)(t * N);
+      const uint32_t ah = smem_u32(Ahi), al = smem_u32(Alo), bh = smem_u32(Bhi), bl = smem_u32(Blo);
+      for (int j = 0; j < Kp / 8; ++j) {
+        const uint32_t ao = (uint32_t)((j >> 2) * 128 * 128 + (j & 3) * 32);
+        const uint32_t bo = (uint32_t)((j >> 2) * N * 128 + (j & 3) * 32);
+        umma_tf32_i(dcol, umma_desc_sw128(ah + ao), umma_desc_sw128(bh + bo), idesc, j > 0 ? 1u : 0u);
+        umma_tf32_i(dcol, umma_desc_sw128(ah + ao), umma_desc_sw128(bl + bo), idesc, 1u);
+        umma_tf32_i(dcol, umma_desc_sw128(al + ao), umma_desc_sw128(bh + bo), idesc, 1u);
+      }
+      umma_commit(smem_u32(bar));
+      // the next node's operands overwrite these: wait for the MMAs to read them
+      if (!mbar_wait(smem_u32(bar), (uint32_t)(nmma & 1), err, 1)) *sflag = 1;
+    }
+    ++nmma;
+    __syncthreads();
+    if (*sflag) ok = false;
+  }
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // warp w reads tensor-memory lanes 32 (w % 4) ..: D row m; warps 0-3
+    // take the first half of the sources, warps 4-7 the second
+    const int q = warp & 3, m = 32 * q + lane, hf = warp >> 2;
+    int d = -1;
+    bool im = false;
+    if (m < nd) {
+      d = m;
+    } else if (CPLX && m >= 64 && m - 64 < nd) {
+      d = m - 64;
+      im = true;
+    }
+    const int64_t c0 = n0 - a.node0;  // J column of the CTA's first node
+    const int nval = (int)((a.nn - n0) < TN ? (a.nn - n0) : TN);
+    for (int s0 = hf * (N / 2); s0 < (hf + 1) * (N / 2); s0 += 16) {
+      uint32_t v[TN][16];
+#pragma unroll
+      for (int t = 0; t < TN; ++t) tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(t * N + s0), v[t]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (d >= 0) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int sidx = s0 + u;
+          if (sidx >= nsu) break;
+          const int64_t row = (im ? a.nsd : 0) + (int64_t)d * nsu + sidx;
+          float* dst = Jout + row * a.ldj + c0;
+          if (nval == TN && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            *reinterpret_cast<float4*>(dst) = make_float4(__uint_as_float(v[0][u]), __uint_as_float(v[1][u]),
+                                                          __uint_as_float(v[2][u]), __uint_as_float(v[3][u]));
+          } else {
+#pragma unroll
+            for (int t = 0; t < TN; ++t)
+              if (t < nval) dst[t] = __uint_as_float(v[t][u]);
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    // a wait gave up: let the MMAs in flight finish before the memory goes
+    mbar_wait(smem_u32(bar), (uint32_t)((nmma - 1) & 1), err, 2);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+
+// the tensor-core path: its error word (a bounded wait that gave up) and the
+// switch that lets a caller take the SIMT products instead
+__device__ int g_jac_tc_err;
+static bool g_jac_tc_on = false;
+
+// launches the tensor-core form when the pairs are the full grid with FP32
+// output and the sizes fit it; returns 1 when it did not apply
+template <typename C, typename In>
+static int launch_jac_tc(const JacArgs& a, const void* phi, void* J, cudaStream_t st, int* launched) {
+  *launched = 0;
+  if (!g_jac_tc_on || !a.grid) return RB_OK;
+  const int nsu = a.det0;
+  if (a.rmax > 32 || nsu < 1 || nsu > 128 || a.ndet > (Scalar<C>::is_complex ? 64 : 128)) return RB_OK;
+  const JtcLayout T = jtc_layout<C>(a.rmax, a.nc, a.ndet, a.emax, nsu);
+  if (T.total > 220 * 1024) return RB_OK;
+  uint32_t cols = 32;
+  while (cols < (uint32_t)(kJtcTN * T.N)) cols <<= 1;
+  if (cols > 512) return RB_OK;
+  int* err = nullptr;
+  RB_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&err), g_jac_tc_err));
+  RB_CUDA_TRY(cudaFuncSetAttribute(jac_tc_kernel<C, In>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T.total));
+  const unsigned g = (unsigned)ceil_div(a.nn - a.node0, kJtcTN);
+  jac_tc_kernel<C, In><<<g, kJacThreads, T.total, st>>>(a, (const In*)phi, (float*)J, cols, err);
+  RB_LAUNCH_CHECK();
+  *launched = 1;
+  return RB_OK;
+}
+
 template <typename C, typename In, bool SPLIT, bool GRID, bool BF>
 static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   int TN = 8;
@@ -365,6 +629,13 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
 
 template <typename C, typename In, bool SPLIT = false, bool BF = false>
 static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
+  // FP32 rows (complex ones split into real and imaginary blocks): the pair
+  // products on the tensor cores when the sizes allow
+  if constexpr (!BF && ((std::is_same<C, cfloat>::value && SPLIT) || std::is_same<C, float>::value)) {
+    int done = 0;
+    RB_TRY((launch_jac_tc<C, In>(a, phi, J, st, &done)));
+    if (done) return RB_OK;
+  }
   if (a.grid) return launch_jac_t<C, In, SPLIT, true, BF>(a, phi, J, st);
   return launch_jac_t<C, In, SPLIT, false, BF>(a, phi, J, st);
 }
@@ -485,6 +756,24 @@ int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind,
   if (!mesh) return fail(RB_EARG, "rb_jac: null argument");
   return rb_jac_range(mesh, what, phi, phi_kind, ld, cols, nc, det0, ndet, pair_src, pair_det, nsd, J, ldj,
                       out_kind, rmax, emax, evol, ddd, 0, mesh->nn, stream);
+}
+
+int rb_jac_tensor_cores(int32_t on) {
+  g_jac_tc_on = on != 0;
+  return RB_OK;
+}
+
+int rb_jac_status(void* stream) {
+  cudaStream_t st = as_stream(stream);
+  RB_CUDA_TRY(cudaStreamSynchronize(st));
+  int h = 0;
+  RB_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_jac_tc_err, sizeof(int)));
+  if (h) {
+    const int zero = 0;
+    RB_CUDA_TRY(cudaMemcpyToSymbol(g_jac_tc_err, &zero, sizeof(int)));
+    return fail(RB_ECUDA, "rb_jac: a tensor-core wait gave up (code %d); the rows are not valid", h);
+  }
+  return RB_OK;
 }
 
 int rb_jac_elem(const rb_mesh* mesh, const double* evol, const void* phi, int32_t phi_kind, int64_t ld,

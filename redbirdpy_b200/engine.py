@@ -828,6 +828,18 @@ def _pair_dev(sd, dev):
     return hit
 
 
+def jac_tensor_cores(on=True):
+    """Allow or forbid (the default) the tensor-core pair products of rb_jac."""
+    call("rb_jac_tensor_cores", int(bool(on)))
+
+
+def _jac_checked():
+    """The outcome of the tensor-core Jacobian launches so far (synchronises;
+    skipped while a CUDA graph is being captured)."""
+    if not torch.cuda.is_current_stream_capturing():
+        call("rb_jac_status", stream())
+
+
 def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=None, evol=None, ddd=None):
     """Adjoint Jacobian rows on the device (nsd x nn), see rb_jac.
     what: 'mua' (reference semantics, forward.py:509-569), 'mua_nodal'
@@ -853,6 +865,8 @@ def jacobian(mesh, phi, sd, what="mua", out_dtype=torch.float32, J=None, ldj=Non
         raise ValueError("rb_jac stages at most 128 phi columns and 64 detectors per call")
     call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0, ndet,
          ptr(ps), ptr(pd), gnsd, ptr(J), ldj, out_kind, mesh.rmax, mesh.emax, ptr(ev), ptr(dd), stream())
+    if J.dtype in (torch.float32, torch.complex64):
+        _jac_checked()
     return J
 
 
@@ -914,6 +928,7 @@ def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torc
         call("rb_jac", ctypes.byref(mesh.struct), w, ptr(phi), phi_kind, phi.shape[1], ptr(colsd), len(cols), det0,
              ndet, ptr(ps), ptr(pd), _grid_nsd(psrc, pdet, det0, ndet), ptr(sub), ldj, out_kind, mesh.rmax,
              mesh.emax, ptr(mesh.evol), ptr(mesh.ddd if w == _lib.RB_JAC_D else None), stream())
+    _jac_checked()
     return J, len(params) * nn
 
 
@@ -1103,6 +1118,7 @@ class SlabJacobian:
                  ptr(self.colsd), len(self.cols), self.det0, self.ndet, ptr(self.ps), ptr(self.pd), self.gnsd,
                  ptr(sub), ld, self.out_kind, m.rmax, m.emax, ptr(m.evol), ptr(m.ddd if w == _lib.RB_JAC_D else None),
                  a, c, stream())
+        _jac_checked()
         return Js, ks
 
     def _pieces(self, a, b):

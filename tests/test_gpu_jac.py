@@ -274,3 +274,59 @@ def test_captured_batch_step_matches_checked_solves():
             e = (torch.abs(a - b).max() / torch.abs(b).max()).item()
             assert e <= 1e-8, (scale, e)
     step.release()
+
+
+@pytest.mark.parametrize("omega", [0.0, 2 * np.pi * 1e8])
+@pytest.mark.parametrize("params", [("mua",), ("mua", "D")])
+def test_jacobian_rows_on_tensor_cores(omega, params):
+    """The pair products on tcgen05 (TF32 hi/lo split) against the SIMT
+    products and the FP64 rows: full source x detector grid, FP32 rows
+    (complex fields split into real and imaginary blocks), the whole mesh and
+    node ranges that start off a multiple of 4."""
+    from redbirdpy_b200.meshgen import kuhn_box, grid_optodes
+
+    node, elem = kuhn_box([40, 40, 20], 2)
+    rng = np.random.default_rng(4)
+    nn = node.shape[0]
+    prop = np.column_stack([rng.uniform(0.008, 0.012, nn), rng.uniform(0.9, 1.1, nn), np.zeros(nn),
+                            np.full(nn, 1.37)])
+    cfg = dict(node=node, elem=elem, prop=prop, srcpos=grid_optodes([8, 32], [8, 32], 4),
+               srcdir=np.array([[0, 0, 1.0]]), detpos=grid_optodes([8, 32], [8, 32], 4, offset=(2, 2)),
+               detdir=np.array([[0, 0, 1.0]]), omega=omega)
+    cfg, sd = rbb.meshprep(cfg)
+    _, phi, _, _, _ = forward_device(cfg, precision="fp64")
+    mesh = engine.mesh_of(cfg)
+    mode = "exact" if len(params) > 1 else "reference"
+    try:
+        engine.jac_tensor_cores(False)
+        Js, K = engine.jacobian_matrix(mesh, phi, sd, params, mode)
+        Js = Js[:, :K].double().cpu().numpy()
+        engine.jac_tensor_cores(True)
+        Jt, _ = engine.jacobian_matrix(mesh, phi, sd, params, mode)
+        Jt = Jt[:, :K].double().cpu().numpy()
+    finally:
+        engine.jac_tensor_cores(False)
+    # FP64 rows of the same quantities
+    ref = []
+    for p in params:
+        w = "mua" if (p == "mua" and mode == "reference") else ("mua_nodal" if p == "mua" else "D")
+        J64 = engine.jacobian(mesh, phi, sd, w, out_dtype=torch.float64).cpu().numpy()
+        ref.append(np.concatenate([J64.real, J64.imag]) if np.iscomplexobj(J64) else J64)
+    ref = np.concatenate(ref, axis=1)
+    scale = np.linalg.norm(ref)
+    assert np.linalg.norm(Jt - ref) <= 1e-6 * scale, np.linalg.norm(Jt - ref) / scale
+    assert np.linalg.norm(Js - ref) <= 1e-6 * scale
+    assert np.abs(Jt - Js).max() <= 1e-5 * np.abs(ref).max()
+    # node ranges (slabs) starting off a multiple of 4, on the tensor cores
+    op = engine.SlabJacobian(mesh, phi, sd, params, mode, width=1001)
+    for a, b in list(op.ranges())[:3]:
+        try:
+            engine.jac_tensor_cores(True)
+            S, ks = op.slab(a, b)
+        finally:
+            engine.jac_tensor_cores(False)
+        S = S[:, :ks].double().cpu().numpy()
+        c = b - a
+        want = np.concatenate([Jt[:, p * nn + a:p * nn + b] for p in range(len(params))], axis=1)
+        assert S.shape == (Jt.shape[0], len(params) * c)
+        np.testing.assert_array_equal(S, want)
