@@ -298,10 +298,26 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
           pv[u] = P[u];
           cv[u] = Cn[u];
         }
+        if constexpr (std::is_same<C, cfloat>::value) {
+          // packed FP32x2 FMAs, two per complex product, in s_fma's order:
+          // (x, y) += (-a.y, a.y) (b.y, b.x), then += (a.x, a.x) (b.x, b.y)
+          float2 ayy[4], axx[4], bsw[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < 4; ++u) {
+            ayy[u] = make_float2(-pv[u].y, pv[u].y);
+            axx[u] = make_float2(pv[u].x, pv[u].x);
+            bsw[u] = make_float2(cv[u].y, cv[u].x);
+          }
 #pragma unroll
-          for (int v = 0; v < 4; ++v) acc[u][v] = s_fma(pv[u], cv[v], acc[u][v]);
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = __ffma2_rn(axx[u], cv[v], __ffma2_rn(ayy[u], bsw[v], acc[u][v]));
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = s_fma(pv[u], cv[v], acc[u][v]);
+        }
       }
 #pragma unroll
       for (int v = 0; v < 4; ++v)
