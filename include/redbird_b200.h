@@ -331,6 +331,10 @@ typedef struct rb_solve_opts {
   const rb_coarse* coarse; /* host pointer; NULL: Jacobi preconditioner only */
   const rb_rowgroups* groups; /* host pointer; NULL: the SpMM walks rows (or row pairs) */
   const rb_instances* instances; /* host pointer; NULL: one system */
+  int32_t spmm_lanes;  /* lanes per row of the per-row SpMM (4, 8, 16 or 32; each
+                          takes ceil(nrhs / lanes) columns, 1, 2 or 4 of them);
+                          0: chosen from nrhs.  Row-pair and row-group
+                          products ignore it. */
 } rb_solve_opts;
 
 typedef struct rb_solve_info {

@@ -59,7 +59,7 @@ class RbSolveOpts(ctypes.Structure):
     _fields_ = [("precision", _i32), ("max_outer", _i32), ("maxiter", _i32), ("check_every", _i32),
                 ("tol", _dbl), ("inner_tol", _dbl), ("profile", _i32), ("use_x0", _i32),
                 ("coarse", ctypes.POINTER(RbCoarse)), ("groups", ctypes.POINTER(RbRowGroups)),
-                ("instances", ctypes.POINTER(RbInstances))]
+                ("instances", ctypes.POINTER(RbInstances)), ("spmm_lanes", _i32)]
 
 
 class RbSolveInfo(ctypes.Structure):

@@ -81,7 +81,8 @@ class DeviceModel:
         at these properties: one solve with host checks, its sweep count and
         the most iterations a sweep took, times ``margin``.  Cached per
         (nn, nnz, columns) bucket so that models of one size share it."""
-        key = (self.mesh.nn, self.mesh.nnz, int(self.B.shape[1]), self.solve_kw.get("precision"))
+        key = (self.mesh.nn, self.mesh.nnz, int(self.B.shape[1]), self.solve_kw.get("precision"),
+               self.solve_kw.get("spmm_lanes", 0))
         hit = _BUDGETS.get(key)
         if hit is not None:
             return hit
@@ -202,6 +203,13 @@ class BatchModel(DeviceModel):
             # carried errors up to 5e-6
             self.solve_kw.setdefault("tol", 1e-17)
         self.status = None
+
+    def tune(self, mua, dcoef):
+        """Pick the solve's launch shapes for this batch with the autotuner
+        (engine.SolveTuner; cached per size bucket) and keep them."""
+        mat = engine.assemble(self.mesh, self.optics(mua.detach(), dcoef.detach()))
+        self.solve_kw.update(engine.solve_tuner.options(mat, self.B, **self.solve_kw))
+        return self.solve_kw
 
     def fields(self, mua, dcoef):
         mat = engine.assemble(self.mesh, self.optics(mua, dcoef))

@@ -1973,7 +1973,18 @@ static int solve_block(const rb_csr& A, const double* B, T64* X, int64_t ldx, in
                        cudaStream_t st) {
   const int64_t n = A.n;
   const Shape sh = pick_shape(n, k, Bps<T>::value);      // inner (FP32 or FP64) vector kernels
-  const Shape shs = pick_spmm_shape<T>(n, k);            // inner SpMM
+  Shape shs = pick_spmm_shape<T>(n, k);                  // inner SpMM
+  if (o.spmm_lanes > 0 && shs.S == 1) {
+    // a caller's (autotuner's) lane count per row: V columns per lane so
+    // that L V covers k, within the layouts the kernels are built for
+    const int L = o.spmm_lanes, V = (int)ceil_div(k, L);
+    if ((L == 4 || L == 8 || L == 16 || L == 32) && (V == 1 || V == 2 || V == 4) && k % V == 0) {
+      shs.L = L;
+      shs.V = V;
+      shs.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(num_sms() * BpsSpmm<T>::value,
+                                                                  ceil_div(n, kBlk / L)));
+    }
+  }
   const Shape sh64 = pick_shape(n, k, BpsSpmm<T64>::value);  // FP64 residual kernels
   const unsigned fg = (unsigned)ceil_div(k, 8);
   const unsigned eg = (unsigned)std::min<int64_t>(ceil_div(n * k, 256), 148 * 16);

@@ -675,11 +675,65 @@ class Instances:
 
 
 # per-instance outcome codes of solve(instances=...)
-INSTANCE_STATUS = {0: "converged", 1: "iteration cap", 2: "breakdown", 3: "non-finite"}
+INSTANCE_STATUS = {0: "converged", 1: "iteration cap", 2: "breakdown", 3: "non-finite", 4: "wait gave up"}
+
+
+class SolveTuner:
+    """Autotuner of the solve's launch shapes: for a system it times one
+    full solve per candidate (lanes per row of the per-row SpMM, which sets
+    the columns a lane takes, and the iterations between host checks) after
+    a warm-up, keeps the fastest, and caches it per size bucket (log2 of the
+    rows, nonzeros per row, columns, real/complex, precision), so that
+    systems of one size share a choice.  The candidates change launch shapes
+    only: every candidate computes the same solution."""
+
+    LANES = (0, 8, 16, 32)
+    CHECKS = (10, 20)
+
+    def __init__(self):
+        self.cache = {}
+        self.timings = {}
+
+    @staticmethod
+    def bucket(mat, k, kw):
+        return (int(np.log2(max(mat.n, 1))), int(round(mat.nnz / max(mat.n, 1))), int(k), bool(mat.is_complex),
+                kw.get("precision", "mixed"))
+
+    def options(self, mat, B, **kw):
+        """The tuned options for solving mat X = B with solve(**kw)."""
+        key = self.bucket(mat, B.shape[1], kw)
+        hit = self.cache.get(key)
+        if hit is not None:
+            return hit
+        kw = {k: v for k, v in kw.items() if k not in ("spmm_lanes", "check_every", "profile", "budget")}
+        cands = [dict(spmm_lanes=lanes, check_every=c) for lanes in self.LANES for c in self.CHECKS]
+        solve(mat, B, **kw, **cands[0])  # warm-up: first launches, plans, caches
+        best, times = None, {}
+        for cand in cands:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, info = solve(mat, B, **kw, **cand)
+            e1.record()
+            torch.cuda.synchronize()
+            if info["flag"] not in (0, None):
+                continue
+            ms = e0.elapsed_time(e1)
+            times[(cand["spmm_lanes"], cand["check_every"])] = ms
+            if best is None or ms < times[(best["spmm_lanes"], best["check_every"])]:
+                best = cand
+        best = best or cands[0]
+        self.cache[key] = best
+        self.timings[key] = times
+        return best
+
+
+solve_tuner = SolveTuner()
 
 
 def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=2000, max_outer=10,
-          check_every=10, profile=False, x0=None, coarse="auto", groups="auto", instances=None, budget=None):
+          check_every=10, profile=False, x0=None, coarse="auto", groups="auto", instances=None, budget=None,
+          spmm_lanes=0):
     """Solve mat X = B for all columns of B (device, nn x k FP64 real).
 
     Returns (X, info dict).  ``precision='mixed'``: FP32 Jacobi-PCG/COCG
@@ -701,7 +755,8 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
     graph); columns that converge early turn the rest into no-ops.  It
     needs ``instances`` (one covering all rows is made when None) and no
     coarse space; ``inst_status`` / ``inst_relres`` are then device tensors
-    and ``flag`` is None until read."""
+    and ``flag`` is None until read.  ``spmm_lanes``: lanes per row of the
+    per-row SpMM (0: chosen from the column count; see SolveTuner)."""
     prec = _lib.RB_FP64 if precision == "fp64" else _lib.RB_MIXED
     n, k = B.shape
     xdt = torch.complex128 if mat.is_complex else torch.float64
@@ -730,7 +785,7 @@ def solve(mat, B, precision="mixed", tol=DEFAULT_TOL, inner_tol=None, maxiter=20
     opts = _lib.RbSolveOpts(prec, int(max_outer), int(maxiter), int(check_every), float(tol), float(inner_tol),
                             int(bool(profile)), int(x0 is not None),
                             ctypes.pointer(cs.struct) if cs is not None else None,
-                            ctypes.pointer(rg.struct) if rg is not None else None, None)
+                            ctypes.pointer(rg.struct) if rg is not None else None, None, int(spmm_lanes))
     inst_status, inst_relres = [], []
     for c0 in range(0, k, 128):
         kb = min(128, k - c0)

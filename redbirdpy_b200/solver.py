@@ -35,7 +35,7 @@ def solver_options(kw):
         opts["tol"] = float(kw["tol"])
     if "refine_tol" in kw:
         opts["tol"] = float(kw["refine_tol"])
-    for k in ("inner_tol", "maxiter", "max_outer", "check_every", "profile", "coarse", "groups"):
+    for k in ("inner_tol", "maxiter", "max_outer", "check_every", "profile", "coarse", "groups", "spmm_lanes"):
         if k in kw:
             opts[k] = kw[k]
     return opts

@@ -330,3 +330,29 @@ def test_jacobian_rows_on_tensor_cores(omega, params):
         want = np.concatenate([Jt[:, p * nn + a:p * nn + b] for p in range(len(params))], axis=1)
         assert S.shape == (Jt.shape[0], len(params) * c)
         np.testing.assert_array_equal(S, want)
+
+
+def test_solve_autotuner_and_lane_layouts():
+    """Every lane layout the autotuner tries solves the batch to the same
+    solution; the tuner returns one of its candidates and caches it per size
+    bucket."""
+    from redbirdpy_b200.adjoint import BatchModel
+    from redbirdpy_b200.meshgen import batch_boxes
+
+    cfgs = [rbb.meshprep(c)[0] for c in batch_boxes(6, seed=5, dims=(12.0, 24.0), spacings=(3.0, 4.0), nopt=(2, 5))]
+    bm = BatchModel(cfgs, precision="mixed")
+    mua = torch.as_tensor(np.concatenate([c["prop"][:, 0] for c in cfgs]), device="cuda")
+    dco = torch.as_tensor(np.concatenate([1.0 / (3.0 * (c["prop"][:, 0] + c["prop"][:, 1])) for c in cfgs]),
+                          device="cuda")
+    mat = engine.assemble(bm.mesh, bm.optics(mua, dco))
+    ref, _ = engine.solve(mat, bm.B, **bm.solve_kw)
+    for lanes in engine.SolveTuner.LANES:
+        X, info = engine.solve(mat, bm.B, **dict(bm.solve_kw, spmm_lanes=lanes))
+        assert info["flag"] == 0 and list(np.unique(info["inst_status"])) == [0]
+        assert (X - ref).abs().max().item() <= 1e-10 * ref.abs().max().item(), lanes
+    kw = bm.tune(mua, dco)
+    assert (kw["spmm_lanes"], kw["check_every"]) in [(a, b) for a in engine.SolveTuner.LANES
+                                                     for b in engine.SolveTuner.CHECKS]
+    key = engine.solve_tuner.bucket(mat, bm.B.shape[1], bm.solve_kw)
+    assert key in engine.solve_tuner.cache and len(engine.solve_tuner.timings[key]) >= 1
+    assert engine.solve_tuner.options(mat, bm.B, **bm.solve_kw) is engine.solve_tuner.cache[key]
