@@ -209,19 +209,30 @@ __global__ void __launch_bounds__(256) trsm_panel_kernel(double* __restrict__ H,
 // 128 threads, 8 x 4 outputs each; the panel is staged k-major in two
 // 32-column halves so that a thread's 8 (and 4) operands are consecutive in
 // shared memory (16-byte loads; rows padded to 66 doubles).
+// The update reaches columns below c_end only; with c_end < M (the columns
+// of the rest of an outer block) the grid is 2-D, x the row tile and y the
+// column tile, and tiles above the diagonal return at once.
 constexpr int kSyrkThreads = 128;
 __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __restrict__ H, int64_t ldh, int64_t M,
-                                                                   int64_t j0, int nb) {
+                                                                   int64_t j0, int nb, int64_t c_end) {
   __shared__ __align__(16) double As[32][kNB + 2];
   __shared__ __align__(16) double Bs[32][kNB + 2];
   const int64_t s0 = j0 + nb;  // first trailing row
-  // blockIdx.x enumerates lower tiles (ti >= tj) in row-major order
-  int64_t t = blockIdx.x, ti = 0;
-  while (t > ti) {
-    t -= ti + 1;
-    ++ti;
+  int64_t ti, tj;
+  if (c_end < M) {
+    ti = blockIdx.x;
+    tj = blockIdx.y;
+    if (tj > ti) return;
+  } else {
+    // blockIdx.x enumerates lower tiles (ti >= tj) in row-major order
+    int64_t t = blockIdx.x;
+    ti = 0;
+    while (t > ti) {
+      t -= ti + 1;
+      ++ti;
+    }
+    tj = t;
   }
-  const int64_t tj = t;
   const int64_t r0 = s0 + ti * kNB, c0 = s0 + tj * kNB;
   const int tid = threadIdx.x;
   const int tr = (tid >> 4) * 8, tc = (tid & 15) * 4;
@@ -267,7 +278,7 @@ __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __res
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int64_t i = r0 + tr + u, j = c0 + tc + v;
-      if (i < M && j < M && j <= i) H[i * ldh + j] -= acc[u][v];
+      if (i < M && j < c_end && j <= i) H[i * ldh + j] -= acc[u][v];
     }
 }
 
@@ -579,17 +590,32 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
   int* err = reinterpret_cast<int*>(work);
   RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
   RB_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem));
-  for (int64_t j0 = 0; j0 < M; j0 += kNB) {
-    const int nb = (int)std::min<int64_t>(kNB, M - j0);
-    potrf_diag_kernel<<<1, 256, 0, st>>>(H, ldh, j0, nb, err);
-    RB_LAUNCH_CHECK();
-    const int64_t rest = M - j0 - nb;
+  // Right-looking in outer blocks of kOuter columns: inside a block each
+  // 64-wide panel is factored (diagonal block, panel solve) and updates only
+  // the rest of the block's columns; the rows and columns right of the block
+  // then take one update of depth kOuter.  The trailing matrix is read and
+  // written once per outer block instead of once per panel.
+  constexpr int64_t kOuter = 4 * kNB;
+  for (int64_t J0 = 0; J0 < M; J0 += kOuter) {
+    const int64_t bend = std::min<int64_t>(J0 + kOuter, M);
+    for (int64_t j0 = J0; j0 < bend; j0 += kNB) {
+      const int nb = (int)std::min<int64_t>(kNB, M - j0);
+      potrf_diag_kernel<<<1, 256, 0, st>>>(H, ldh, j0, nb, err);
+      RB_LAUNCH_CHECK();
+      const int64_t rest = M - j0 - nb;
+      if (rest <= 0) break;
+      trsm_panel_kernel<<<(unsigned)ceil_div(rest, kNB), 256, kTrsmSmem, st>>>(H, ldh, M, j0, nb);
+      RB_LAUNCH_CHECK();
+      if (j0 + nb < bend) {  // the block's later panels
+        const int64_t T = ceil_div(rest, kNB), Tc = ceil_div(bend - (j0 + nb), kNB);
+        syrk_update_kernel<<<dim3((unsigned)T, (unsigned)Tc), kSyrkThreads, 0, st>>>(H, ldh, M, j0, nb, bend);
+        RB_LAUNCH_CHECK();
+      }
+    }
+    const int64_t rest = M - bend;
     if (rest <= 0) break;
-    trsm_panel_kernel<<<(unsigned)ceil_div(rest, kNB), 256, kTrsmSmem, st>>>(
-        H, ldh, M, j0, nb);
-    RB_LAUNCH_CHECK();
     const int64_t T = ceil_div(rest, kNB);
-    syrk_update_kernel<<<(unsigned)(T * (T + 1) / 2), kSyrkThreads, 0, st>>>(H, ldh, M, j0, nb);
+    syrk_update_kernel<<<(unsigned)(T * (T + 1) / 2), kSyrkThreads, 0, st>>>(H, ldh, M, J0, (int)(bend - J0), M);
     RB_LAUNCH_CHECK();
   }
   int herr = 0;
