@@ -431,7 +431,8 @@ def run_gn_step(cfg, mesh, world, args):
         # previous iterate's fields, and the update is applied at the end
         det, phi, _, _, _ = timed_stage("forward", lambda: forward_device(gcfg, x0=state["phi"]))
         J, K = timed_stage("jacobian", lambda: engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact",
-                                                                      dtype=jdtype))
+                                                                      dtype=jdtype,
+                                                                      acc64=jdtype == torch.float32))
         y = det.cpu().numpy().ravel()
         mis = data - y
         mis = np.concatenate([mis.real, mis.imag])
@@ -577,7 +578,7 @@ def run_gn_step(cfg, mesh, world, args):
 
         def step_slab(width):
             det, phi, _, _, _ = forward_device(gcfg, x0=snap[1])
-            op = engine.SlabJacobian(mesh, phi, sd, ("mua", "D"), "exact", width)
+            op = engine.SlabJacobian(mesh, phi, sd, ("mua", "D"), "exact", width, acc64=True)
             y = det.cpu().numpy().ravel()
             mis = data - y
             mis = np.concatenate([mis.real, mis.imag])
@@ -613,7 +614,7 @@ def run_gn_step(cfg, mesh, world, args):
         pk_sus = float(mp.get("bf16_tflops_sustained") or pk_sus)
     return {
         "workload": f"{mesh.ne} tets / {mesh.nn} nodes, omega=2*pi*100MHz, 64x64 complex pairs -> 8192 real rows, "
-                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows, J J^T on the tensor cores from their BF16 "
+                    f"mua+D nodal (K={2 * mesh.nn}), FP32 Jacobian rows (products formed in FP64), J J^T on the tensor cores from their BF16 "
                     f"copy (made in the row-sum pass) + FP64 refinement of the normal equations over the FP32 rows; "
                     f"lam = 0.05 max diag(J J^T) from the exact row sums; GN iterations 2..{ks + 1} of the loop "
                     f"(forward warm-started from the previous iterate's fields), iteration 1 untimed",

@@ -401,7 +401,10 @@ enum rb_jac_what { RB_JAC_MUA_REF = 0, RB_JAC_MUA_NODAL = 1, RB_JAC_D = 2 };
  * (matreform 'real' stacking, redbirdpy/recon.py:532-546) */
 enum rb_jac_split { RB_JAC_SPLIT_F32 = 4, RB_JAC_SPLIT_F64 = 5,
                     RB_JAC_SPLIT_BF16 = 6, /* split rows rounded to BF16 (GN step in BF16) */
-                    RB_JAC_BF16 = 7 /* real rows rounded to BF16 */ };
+                    RB_JAC_BF16 = 7, /* real rows rounded to BF16 */
+                    RB_JAC_SPLIT_F32_ACC64 = 8, /* split FP32 rows whose products are formed
+                                                   in FP64 (only the storage rounds) */
+                    RB_JAC_F32_ACC64 = 9 /* real FP32 rows, products formed in FP64 */ };
 int rb_jac(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi_kind, int64_t ld,
            const int32_t* cols, int32_t nc, int32_t det0, int32_t ndet, const int32_t* pair_src,
            const int32_t* pair_det, int64_t nsd, void* J, int64_t ldj, int32_t out_kind,

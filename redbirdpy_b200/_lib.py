@@ -21,6 +21,7 @@ RB_PROP_NODE, RB_PROP_ELEM = 0, 1
 RB_MIXED, RB_FP64 = 0, 1
 RB_JAC_MUA_REF, RB_JAC_MUA_NODAL, RB_JAC_D = 0, 1, 2
 RB_JAC_SPLIT_F32, RB_JAC_SPLIT_F64, RB_JAC_SPLIT_BF16, RB_JAC_BF16 = 4, 5, 6, 7
+RB_JAC_SPLIT_F32_ACC64, RB_JAC_F32_ACC64 = 8, 9
 
 _i64, _i32, _vp, _dbl, _sz = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_double, ctypes.c_size_t
 

@@ -111,10 +111,18 @@ __host__ __device__ inline size_t jac_smem(int TN, int rmax, int nc, int ndet, i
 
 // one Jacobian entry: complex values split into a real-part and an
 // imaginary-part row block (SPLIT), optionally rounded to BF16 (BF)
-template <typename C, bool SPLIT, bool BF>
+template <typename C, bool SPLIT, bool BF, bool NARROW = false>
 __device__ __forceinline__ void jac_store(void* Jout, int64_t nsd, int64_t ldj, int64_t k, int64_t n, C v) {
   typedef typename JacT<C>::real R;
-  if constexpr (SPLIT) {
+  if constexpr (NARROW) {  // computed in FP64, stored as FP32 rows
+    float* Jf = reinterpret_cast<float*>(Jout);
+    if constexpr (SPLIT) {
+      Jf[k * ldj + n] = (float)v.x;
+      Jf[(nsd + k) * ldj + n] = (float)v.y;
+    } else {
+      Jf[k * ldj + n] = (float)v;
+    }
+  } else if constexpr (SPLIT) {
     if constexpr (BF) {
       __nv_bfloat16* Jb = reinterpret_cast<__nv_bfloat16*>(Jout);
       Jb[k * ldj + n] = __float2bfloat16_rn(v.x);
@@ -258,7 +266,7 @@ __device__ __forceinline__ void jac_stage(const JacArgs& a, const In* __restrict
   __syncthreads();
 }
 
-template <typename C, typename In, int TN, bool SPLIT, bool GRID, bool BF>
+template <typename C, typename In, int TN, bool SPLIT, bool GRID, bool BF, bool NARROW = false>
 __global__ void __launch_bounds__(kJacThreads)
 jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -324,7 +332,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int64_t k = (int64_t)(db * 4 + v) * nsu + sb * 4 + u;
-          jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n - a.node0, acc[u][v]);
+          jac_store<C, SPLIT, BF, NARROW>(Jout, a.nsd, a.ldj, k, n - a.node0, acc[u][v]);
         }
     }
     return;
@@ -343,7 +351,7 @@ jac_kernel(JacArgs a, const In* __restrict__ phi, void* __restrict__ Jout) {
     for (int ia = 0; ia < srn[t]; ++ia) s = s_fma(P[(size_t)ia * nc], Cn[(size_t)ia * nd], s);
     // complex rows are split into a block of real parts and a block of
     // imaginary parts (matreform 'real', recon.py:532-546)
-    jac_store<C, SPLIT, BF>(Jout, a.nsd, a.ldj, k, n - a.node0, s);
+    jac_store<C, SPLIT, BF, NARROW>(Jout, a.nsd, a.ldj, k, n - a.node0, s);
   }
 }
 
@@ -618,7 +626,7 @@ static int launch_jac_tc(const JacArgs& a, const void* phi, void* J, cudaStream_
   return RB_OK;
 }
 
-template <typename C, typename In, bool SPLIT, bool GRID, bool BF>
+template <typename C, typename In, bool SPLIT, bool GRID, bool BF, bool NARROW = false>
 static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   int TN = 8;
   const size_t budget = 110 * 1024;
@@ -628,9 +636,9 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
   const unsigned g = (unsigned)ceil_div(a.nn - a.node0, TN);
 #define RB_JL(TN_)                                                                                     \
   do {                                                                                                 \
-    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID, BF>,                          \
+    RB_CUDA_TRY(cudaFuncSetAttribute(jac_kernel<C, In, TN_, SPLIT, GRID, BF, NARROW>,                  \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
-    jac_kernel<C, In, TN_, SPLIT, GRID, BF><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);           \
+    jac_kernel<C, In, TN_, SPLIT, GRID, BF, NARROW><<<g, kJacThreads, sm, st>>>(a, (const In*)phi, J);   \
   } while (0)
   switch (TN) {
     case 8: RB_JL(8); break;
@@ -643,17 +651,17 @@ static int launch_jac_t(const JacArgs& a, const void* phi, void* J, cudaStream_t
   return RB_OK;
 }
 
-template <typename C, typename In, bool SPLIT = false, bool BF = false>
+template <typename C, typename In, bool SPLIT = false, bool BF = false, bool NARROW = false>
 static int launch_jac(const JacArgs& a, const void* phi, void* J, cudaStream_t st) {
   // FP32 rows (complex ones split into real and imaginary blocks): the pair
   // products on the tensor cores when the sizes allow
-  if constexpr (!BF && ((std::is_same<C, cfloat>::value && SPLIT) || std::is_same<C, float>::value)) {
+  if constexpr (!BF && !NARROW && ((std::is_same<C, cfloat>::value && SPLIT) || std::is_same<C, float>::value)) {
     int done = 0;
     RB_TRY((launch_jac_tc<C, In>(a, phi, J, st, &done)));
     if (done) return RB_OK;
   }
-  if (a.grid) return launch_jac_t<C, In, SPLIT, true, BF>(a, phi, J, st);
-  return launch_jac_t<C, In, SPLIT, false, BF>(a, phi, J, st);
+  if (a.grid) return launch_jac_t<C, In, SPLIT, true, BF, NARROW>(a, phi, J, st);
+  return launch_jac_t<C, In, SPLIT, false, BF, NARROW>(a, phi, J, st);
 }
 
 // lam[r][s] = sum_d phi[r][dcol0 + d] conj(g[det0_i + d][s]) for the instance i of row r
@@ -732,6 +740,16 @@ int rb_jac_range(const rb_mesh* mesh, int32_t what, const void* phi, int32_t phi
   }
   cudaStream_t st = as_stream(stream);
   const bool cin = (phi_kind == RB_C128 || phi_kind == RB_C64);
+  if (out_kind == RB_JAC_SPLIT_F32_ACC64) {  // FP32 rows of products formed in FP64
+    if (!cin) return fail(RB_EARG, "rb_jac: split output needs complex phi");
+    return phi_kind == RB_C64 ? launch_jac<cdouble, cfloat, true, false, true>(a, phi, J, st)
+                              : launch_jac<cdouble, cdouble, true, false, true>(a, phi, J, st);
+  }
+  if (out_kind == RB_JAC_F32_ACC64) {
+    if (cin) return fail(RB_EARG, "rb_jac: RB_JAC_F32_ACC64 needs real phi (complex: RB_JAC_SPLIT_F32_ACC64)");
+    return phi_kind == RB_F32 ? launch_jac<double, float, false, false, true>(a, phi, J, st)
+                              : launch_jac<double, double, false, false, true>(a, phi, J, st);
+  }
   if (out_kind == RB_JAC_SPLIT_BF16) {
     if (!cin) return fail(RB_EARG, "rb_jac: split output needs complex phi");
     return phi_kind == RB_C64 ? launch_jac<cfloat, cfloat, true, true>(a, phi, J, st)

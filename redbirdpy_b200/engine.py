@@ -946,13 +946,15 @@ def _pad8(n):
     return (n + 7) // 8 * 8
 
 
-def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torch.float32):
+def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torch.float32, acc64=False):
     """The real Jacobian of the GN step (FP32, or BF16 with ``dtype``), rows x
     columns = (nsd or 2 nsd) x (len(params) * nn), stored with a row stride
     padded to 16 bytes.
     Complex fields give matreform 'real' stacking [Re; Im] (recon.py:532-546).
     mode 'reference' = redbirdpy's jac for mua (forward.py:509-569);
-    'exact' = derivatives of the node-based assembly ('mua' at fixed D, 'D')."""
+    'exact' = derivatives of the node-based assembly ('mua' at fixed D, 'D').
+    ``acc64``: FP32 rows whose products are formed in FP64 (only the storage
+    rounds: ~6e-8 relative per entry instead of ~3e-7)."""
     cols, det0, ndet, psrc, pdet, _, _ = pair_map(sd)
     nsd = len(psrc)
     cplx = phi.is_complex()
@@ -967,6 +969,8 @@ def jacobian_matrix(mesh, phi, sd, params=("mua",), mode="reference", dtype=torc
         J[:, len(params) * nn:].zero_()
     if bf:
         out_kind = _lib.RB_JAC_SPLIT_BF16 if cplx else _lib.RB_JAC_BF16
+    elif acc64:
+        out_kind = _lib.RB_JAC_SPLIT_F32_ACC64 if cplx else _lib.RB_JAC_F32_ACC64
     else:
         out_kind = _lib.RB_JAC_SPLIT_F32 if cplx else _lib.RB_F32
     phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,
@@ -1122,7 +1126,8 @@ class SlabJacobian:
     and the memory is rows x len(params) x width.  Offers the same passes as
     StoredJacobian plus the Frobenius sum and the tensor-core product."""
 
-    def __init__(self, mesh, phi, sd, params=("mua",), mode="reference", width=4096, dtype=torch.float32):
+    def __init__(self, mesh, phi, sd, params=("mua",), mode="reference", width=4096, dtype=torch.float32,
+                 acc64=False):
         self.mesh, self.phi, self.params, self.dtype = mesh, phi, tuple(params), dtype
         self.cols, self.det0, self.ndet, psrc, pdet, self.colsd, self.ps, self.pd, self.gnsd = _pair_dev(sd, phi.device)
         if len(self.cols) > 128 or self.ndet > 64:
@@ -1139,6 +1144,8 @@ class SlabJacobian:
         self.buf = torch.empty(self.rows * pad(len(self.params) * self.width), dtype=dtype, device=phi.device)
         if self.bf:
             self.out_kind = _lib.RB_JAC_SPLIT_BF16 if self.cplx else _lib.RB_JAC_BF16
+        elif acc64:
+            self.out_kind = _lib.RB_JAC_SPLIT_F32_ACC64 if self.cplx else _lib.RB_JAC_F32_ACC64
         else:
             self.out_kind = _lib.RB_JAC_SPLIT_F32 if self.cplx else _lib.RB_F32
         self.phi_kind = {torch.float64: _lib.RB_F64, torch.complex128: _lib.RB_C128, torch.float32: _lib.RB_F32,

@@ -389,6 +389,9 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
     # otherwise recomputes it in node slabs; an int forces slabs that wide;
     # None/False always stores it
     jac_slab = kwargs.get("jac_slab", "auto")
+    # FP32 Jacobian rows whose products are formed in FP64: the update then
+    # carries only the rows' storage rounding
+    jac_acc64 = kwargs.get("jac_acc64", True)
     extin = kwargs.get("extin", cfg.get("extin"))
     # each forward solve starts from the previous iterate's fields (the
     # refinement then only removes what the property update changed)
@@ -448,11 +451,12 @@ def runrecon(cfg, recon, detphi0, sd=None, **kwargs):
             # BF16 (half the memory; the step solves the rounded rows' system)
             jdt = torch.bfloat16 if gram_prec == "bf16_rows" else torch.float32
             width = _slab_width(jac_slab, mesh, phis[0], sds[0], len(params), jdt)
+            acc64 = jdt == torch.float32 and jac_acc64
             if width:  # J recomputed in node slabs on every pass instead of stored
-                J = engine.SlabJacobian(mesh, phis[0], sds[0], params, jac_mode, width, jdt)
+                J = engine.SlabJacobian(mesh, phis[0], sds[0], params, jac_mode, width, jdt, acc64=acc64)
                 K = J.K
             else:
-                J, K = engine.jacobian_matrix(mesh, phis[0], sds[0], params, jac_mode, dtype=jdt)
+                J, K = engine.jacobian_matrix(mesh, phis[0], sds[0], params, jac_mode, dtype=jdt, acc64=acc64)
             misfit = y0s[0] - dets[0].cpu().numpy().ravel()
             if np.iscomplexobj(misfit):
                 misfit = np.concatenate([np.real(misfit), np.imag(misfit)])

@@ -356,3 +356,30 @@ def test_solve_autotuner_and_lane_layouts():
     key = engine.solve_tuner.bucket(mat, bm.B.shape[1], bm.solve_kw)
     assert key in engine.solve_tuner.cache and len(engine.solve_tuner.timings[key]) >= 1
     assert engine.solve_tuner.options(mat, bm.B, **bm.solve_kw) is engine.solve_tuner.cache[key]
+
+
+@pytest.mark.parametrize("omega", [0.0, 2 * np.pi * 1e8])
+def test_jacobian_rows_formed_in_fp64(omega):
+    """FP32 rows whose products are formed in FP64 equal the FP64 rows
+    rounded to FP32 (only the storage rounds)."""
+    from redbirdpy_b200.meshgen import kuhn_box, grid_optodes
+
+    node, elem = kuhn_box([40, 40, 20], 2)
+    rng = np.random.default_rng(6)
+    nn = node.shape[0]
+    prop = np.column_stack([rng.uniform(0.008, 0.012, nn), rng.uniform(0.9, 1.1, nn), np.zeros(nn),
+                            np.full(nn, 1.37)])
+    cfg = dict(node=node, elem=elem, prop=prop, srcpos=grid_optodes([8, 32], [8, 32], 4),
+               srcdir=np.array([[0, 0, 1.0]]), detpos=grid_optodes([8, 32], [8, 32], 4, offset=(2, 2)),
+               detdir=np.array([[0, 0, 1.0]]), omega=omega)
+    cfg, sd = rbb.meshprep(cfg)
+    _, phi, _, _, _ = forward_device(cfg, precision="fp64")
+    mesh = engine.mesh_of(cfg)
+    J, K = engine.jacobian_matrix(mesh, phi, sd, ("mua", "D"), "exact", acc64=True)
+    J = J[:, :K].double().cpu().numpy()
+    ref = []
+    for w in ("mua_nodal", "D"):
+        J64 = engine.jacobian(mesh, phi, sd, w, out_dtype=torch.float64).cpu().numpy()
+        ref.append(np.concatenate([J64.real, J64.imag]) if np.iscomplexobj(J64) else J64)
+    ref = np.concatenate(ref, axis=1)
+    np.testing.assert_array_equal(J, ref.astype(np.float32).astype(np.float64))
