@@ -282,57 +282,77 @@ __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __res
     }
 }
 
-// the diagonal-block step of the triangular solves with the block's inverse
-// X (kept by rb_cholesky in the block's strict upper triangle):
-// mode 0: v = X v (solves L_kk y = v), mode 1: v = X^T v (solves L_kk^T y = v).
-// Output i is summed by the 4 lanes of a quad (terms t = q, q + 4, ...) and
-// the quad's partial sums are added in a fixed order.
-__global__ void __launch_bounds__(256) tri_block_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
-                                                        double* __restrict__ x, int mode) {
-  __shared__ double v[kNB];
+// The triangular solves of rb_chol_solve apply the diagonal blocks' inverses
+// X (kept by rb_cholesky in each block's strict upper triangle):
+// mode 0: y = X v (solves L_kk y = v), mode 1: y = X^T v (solves L_kk^T y = v).
+// y = X v (mode 0) or X^T v (mode 1) of diagonal block k0 into shared memory,
+// by all 256 threads of the block (a quad per output, fixed order), v read
+// from src[k0 ..]
+__device__ __forceinline__ void tri_block_apply(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
+                                                const double* __restrict__ src, int mode, double* v, double* y) {
   const int tid = threadIdx.x;
   const int i = tid >> 2, q = tid & 3;
-  if (tid < nb) v[tid] = x[k0 + tid];
+  if (tid < nb) v[tid] = src[k0 + tid];
   __syncthreads();
   double s = 0.0;
   if (i < nb) {
-    if (mode == 0) {  // y[i] = sum_{t <= i} X[i][t] v[t],  X[i][t] = L[k0 + t][k0 + i] (t < i)
+    if (mode == 0) {
       for (int t = q; t <= i; t += 4)
         s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + t) * ldh + k0 + i], v[t], s);
-    } else {  // y[i] = sum_{t >= i} X[t][i] v[t],  X[t][i] = L[k0 + i][k0 + t] (t > i)
+    } else {
       for (int t = i + q; t < nb; t += 4)
         s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + i) * ldh + k0 + t], v[t], s);
     }
   }
   s += __shfl_xor_sync(0xffffffffu, s, 1);
   s += __shfl_xor_sync(0xffffffffu, s, 2);
-  if (i < nb && q == 0) x[k0 + i] = s;
+  if (i < nb && q == 0) y[i] = s;
+  __syncthreads();
 }
 
-// forward: x[r] -= sum_{c in block} L[r][k0+c] x[k0+c] for r >= k0+nb (warp per row)
-__global__ void fwd_update_kernel(const double* __restrict__ L, int64_t ldh, int64_t M, int64_t k0, int nb,
-                                  double* __restrict__ x) {
+// One forward step of L y = b, fused: every block solves diagonal block k0
+// (y = X v, v = x[k0 ..]) itself, block 0 stores y in w, and each block
+// subtracts L[r][k0 ..] y from its 8 rows r below the block (a warp per row).
+__global__ void __launch_bounds__(256) fwd_solve_kernel(const double* __restrict__ L, int64_t ldh, int64_t M,
+                                                        int64_t k0, int nb, double* __restrict__ x,
+                                                        double* __restrict__ w) {
+  __shared__ double v[kNB], y[kNB];
+  tri_block_apply(L, ldh, k0, nb, x, 0, v, y);
+  if (blockIdx.x == 0 && threadIdx.x < nb) w[k0 + threadIdx.x] = y[threadIdx.x];
   const int lane = threadIdx.x & 31;
   const int64_t r = k0 + nb + blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= M) return;
   double s = 0.0;
-  for (int c = lane; c < nb; c += 32) s += L[r * ldh + k0 + c] * x[k0 + c];
+  for (int c = lane; c < nb; c += 32) s += L[r * ldh + k0 + c] * y[c];
   s = warp_sum(s);
   if (lane == 0) x[r] -= s;
 }
 
-// backward: x[j] -= sum_{r in block} L[k0+r][j] x[k0+r] for j < k0 (thread per column)
-__global__ void bwd_update_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb, double* __restrict__ x) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j >= k0) return;
+// One backward step of L^T x = y, fused: every block solves diagonal block
+// k0 (v = w[k0 ..], the forward solution less the later blocks' terms),
+// block 0 stores the result in x, and each block subtracts L[k0 + r][j] y[r]
+// from its 32 columns j < k0 of w (8 warps over the block's rows, summed in
+// a fixed order).
+__global__ void __launch_bounds__(256) bwd_solve_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
+                                                        double* __restrict__ w, double* __restrict__ x) {
+  __shared__ double v[kNB], y[kNB], part[8][32];
+  tri_block_apply(L, ldh, k0, nb, w, 1, v, y);
+  if (blockIdx.x == 0 && threadIdx.x < nb) x[k0 + threadIdx.x] = y[threadIdx.x];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int64_t j = blockIdx.x * 32 + lane;
   double s = 0.0;
-  for (int r = 0; r < nb; ++r) s += L[(k0 + r) * ldh + j] * x[k0 + r];
-  x[j] -= s;
+  if (j < k0)
+    for (int r = wp; r < nb; r += 8) s = fma(L[(k0 + r) * ldh + j], y[r], s);
+  part[wp][lane] = s;
+  __syncthreads();
+  if (wp == 0 && j < k0) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += part[q][lane];
+    w[j] -= t;
+  }
 }
 
-// out[k] = alpha * sum_m J[m][k] y[m] + beta out[k]   (coalesced along k).
-// Rows are split over gridDim.y slabs; each slab writes a partial sum and the
-// last kernel adds the slabs in fixed order (deterministic, no atomics).
 constexpr int kGemvSlabs = 16;
 
 __device__ __forceinline__ double jval(float v) { return v; }
@@ -628,19 +648,22 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
 int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stream) {
   if (!L || !x || M < 1 || ldh < M) return fail(RB_EARG, "rb_chol_solve: bad arguments");
   cudaStream_t st = as_stream(stream);
+  // one launch per diagonal block and direction: each block of a launch
+  // solves the 64 x 64 diagonal step itself and then its share of the update
+  double* w = nullptr;  // the forward solution, consumed by the backward steps
+  RB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&w), sizeof(double) * M, st));
   for (int64_t k0 = 0; k0 < M; k0 += kNB) {  // L y = b
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
-    tri_block_kernel<<<1, 256, 0, st>>>(L, ldh, k0, nb, x, 0);
     const int64_t rest = M - k0 - nb;
-    if (rest > 0) fwd_update_kernel<<<(unsigned)ceil_div(rest, 8), 256, 0, st>>>(L, ldh, M, k0, nb, x);
+    fwd_solve_kernel<<<(unsigned)std::max<int64_t>(1, ceil_div(rest, 8)), 256, 0, st>>>(L, ldh, M, k0, nb, x, w);
     RB_LAUNCH_CHECK();
   }
   for (int64_t k0 = ((M - 1) / kNB) * kNB; k0 >= 0; k0 -= kNB) {  // L^T x = y
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
-    tri_block_kernel<<<1, 256, 0, st>>>(L, ldh, k0, nb, x, 1);
-    if (k0 > 0) bwd_update_kernel<<<(unsigned)ceil_div(k0, 256), 256, 0, st>>>(L, ldh, k0, nb, x);
+    bwd_solve_kernel<<<(unsigned)std::max<int64_t>(1, ceil_div(k0, 32)), 256, 0, st>>>(L, ldh, k0, nb, w, x);
     RB_LAUNCH_CHECK();
   }
+  RB_CUDA_TRY(cudaFreeAsync(w, st));
   return RB_OK;
 }
 
