@@ -120,8 +120,13 @@ class BatchModel(DeviceModel):
     and the block-diagonal matrix keeps the instances' fields apart.  All
     instances share omega and the boundary reflection coefficient."""
 
-    def __init__(self, cfgs, precision="mixed", **solver_kw):
+    def __init__(self, cfgs, precision="mixed", strict=True, **solver_kw):
+        """``strict``: a forward solve in which any instance fails raises
+        (the reference's error behaviour); with ``strict=False`` the outcome
+        of every instance is only recorded in ``status`` (see fields)."""
         from .utility import getoptodes
+
+        self.strict = strict
 
         if not cfgs:
             raise ValueError("BatchModel needs at least one instance")
@@ -212,12 +217,29 @@ class BatchModel(DeviceModel):
         return self.solve_kw
 
     def fields(self, mua, dcoef):
+        """Fields of every instance.  An instance whose properties hold a
+        non-finite value or a non-positive D is solved on stand-in properties
+        (mua 0.01/mm, D 1/3.03 mm) so that its rows cannot spoil the shared
+        Krylov scalars of the others, and its status is set to 3
+        (non-finite); its values are not valid."""
+        inst = self.instances.row_inst.long()
+        bad_row = ~(torch.isfinite(mua) & torch.isfinite(dcoef) & (dcoef > 0))
+        bad_inst = torch.zeros(self.ninst, dtype=torch.int32, device=mua.device)
+        bad_inst.index_add_(0, inst, bad_row.to(torch.int32))
+        bad_inst = bad_inst > 0
+        iso = bad_inst[inst]
+        mua = torch.where(iso, torch.full_like(mua, 0.01), mua)
+        dcoef = torch.where(iso, torch.full_like(dcoef, 1.0 / 3.03), dcoef)
         mat = engine.assemble(self.mesh, self.optics(mua, dcoef))
         phi, info = engine.solve(mat, self.B, **self.solve_kw)
         self.status, self.relres = info["inst_status"], info["inst_relres"]
         if info["flag"] is None:  # fixed budget: read the status words later
+            self.status = torch.where(bad_inst, torch.full_like(self.status, 3), self.status)
             return phi, mat
+        self.status = np.where(bad_inst.cpu().numpy(), 3, self.status).astype(np.int32)
         bad = np.flatnonzero(self.status)
+        if bad.size and not self.strict:
+            return phi, mat
         if bad.size:
             desc = ", ".join(f"{i}: {engine.INSTANCE_STATUS[int(self.status[i])]}" for i in bad[:8])
             raise RuntimeError(f"forward solve failed for {bad.size} instance(s) ({desc})")

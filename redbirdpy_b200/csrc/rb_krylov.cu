@@ -1197,20 +1197,28 @@ __global__ void __launch_bounds__(kFinThreads) fin_beta_kernel(int64_t k, int nb
 
 // --------------------------------------------------- refinement kernels
 
+// refinement state before the first sweep from ||b||^2: a zero column is
+// done (exactly zero solution); a non-finite one is done with the
+// non-finite outcome (3), never counted as converged
+__device__ __forceinline__ OuterState outer_start(double s) {
+  OuterState o;
+  const bool fin = isfinite(s);
+  o.bnorm = sqrt(s);
+  // no previous sweep yet: the first residual can never count as stagnation
+  o.relres = !fin ? s : (s > 0.0) ? 1e300 : 0.0;
+  o.prev = 1e300;
+  o.scale = 0.0;
+  o.itol2 = -1.0;
+  o.active = fin && s > 0.0;
+  o.done = !fin ? 3 : (s > 0.0) ? 0 : 1;
+  return o;
+}
+
 __global__ void fin_bnorm_kernel(int64_t k, int nb, const double* part, OuterState* os) {
   RB_FIN_WARP();
   const double s = sum_part<double>(part, nb, k, c, lane).x;
   if (lane) return;
-  OuterState o;
-  o.bnorm = sqrt(s);
-  // no previous sweep yet: the first residual can never count as stagnation
-  o.relres = (s > 0.0) ? 1e300 : 0.0;
-  o.prev = 1e300;
-  o.scale = 0.0;
-  o.itol2 = -1.0;
-  o.active = s > 0.0;
-  o.done = (s > 0.0) ? 0 : 1;
-  os[c] = o;
+  os[c] = outer_start(s);
 }
 
 // A sweep normally solves its correction to inner_tol.  The sweep that will
@@ -1343,16 +1351,7 @@ seg_norm_kernel(int64_t ninst, int64_t k, const int64_t* __restrict__ row_ptr, c
 __global__ void seg_bnorm_kernel(int64_t m, const double* __restrict__ s2, OuterState* __restrict__ seg) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= m) return;
-  const double s = s2[j];
-  OuterState o;
-  o.bnorm = sqrt(s);
-  o.relres = (s > 0.0) ? 1e300 : 0.0;
-  o.prev = 1e300;
-  o.scale = 0.0;
-  o.itol2 = -1.0;
-  o.active = s > 0.0;
-  o.done = (s > 0.0) ? 0 : 1;
-  seg[j] = o;
+  seg[j] = outer_start(s2[j]);
 }
 
 // the rules of fin_outer_kernel, per (instance, column)

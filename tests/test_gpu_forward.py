@@ -483,3 +483,17 @@ def test_device_meshprep_matches_host_restatement_on_a_shuffled_mesh():
     np.testing.assert_array_equal(cfg["area"], ut._elemvolume(node, cfg["face"]))
     np.testing.assert_allclose(cfg["evol"], ut._elemvolume(node, r), rtol=1e-15)
     np.testing.assert_allclose(cfg["nvol"], ut._nodevolume(node.shape[0], r, cfg["evol"]), rtol=1e-14)
+
+
+def test_femsolve_non_finite_rhs_column_is_flagged():
+    """A NaN right-hand-side column ends with flag 2, not as converged; the
+    other columns still solve."""
+    from scipy.sparse.linalg import splu
+
+    A = spd(200, 3)
+    B = np.random.default_rng(1).standard_normal((200, 4))
+    B[5, 2] = np.nan
+    x, flag = rbb.femsolve(A, B)
+    assert flag == 2
+    ref = splu(A.tocsc()).solve(np.nan_to_num(B[:, [0, 1, 3]]))
+    np.testing.assert_allclose(x[:, [0, 1, 3]], ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())

@@ -383,3 +383,32 @@ def test_jacobian_rows_formed_in_fp64(omega):
         ref.append(np.concatenate([J64.real, J64.imag]) if np.iscomplexobj(J64) else J64)
     ref = np.concatenate(ref, axis=1)
     np.testing.assert_array_equal(J, ref.astype(np.float32).astype(np.float64))
+
+
+def test_batch_isolates_an_instance_with_non_finite_properties():
+    """One instance's properties turn NaN: it alone reports status 3, and the
+    other instances' detector values equal those of the clean batch."""
+    from redbirdpy_b200.adjoint import BatchModel, detector_values
+    from redbirdpy_b200.meshgen import batch_boxes
+
+    cfgs = [rbb.meshprep(c)[0] for c in batch_boxes(6, seed=5, dims=(12.0, 24.0), spacings=(3.0, 4.0), nopt=(2, 5))]
+    bm = BatchModel(cfgs, precision="mixed", strict=False)
+    mua = torch.as_tensor(np.concatenate([c["prop"][:, 0] for c in cfgs]), device="cuda")
+    dco = torch.as_tensor(np.concatenate([1.0 / (3.0 * (c["prop"][:, 0] + c["prop"][:, 1])) for c in cfgs]),
+                          device="cuda")
+    with torch.no_grad():
+        clean = [p.clone() for p in bm.split(detector_values(bm, mua, dco))]
+        assert list(np.unique(bm.status)) == [0]
+        bad = mua.clone()
+        bad[int(bm.node_off[2]) + 3] = float("nan")
+        parts = bm.split(detector_values(bm, bad, dco))
+    assert int(bm.status[2]) == 3
+    assert all(int(bm.status[i]) == 0 for i in range(len(cfgs)) if i != 2)
+    for i in range(len(cfgs)):
+        if i != 2:
+            e = (torch.abs(parts[i] - clean[i]) / torch.abs(clean[i])).max().item()
+            assert e <= 1e-6, (i, e)
+    strict = BatchModel(cfgs, precision="mixed")
+    with pytest.raises(RuntimeError, match="non-finite"):
+        detector_values(strict, bad, dco)
+
