@@ -11,10 +11,11 @@
 // the same bits as the per-row kernels).  On the tetrahedral box a 2 x 2 x 2
 // group needs 5.7 x rows per matrix row against 14.2 nonzeros (10.5 for the
 // row-pair kernel); L2 -> SM traffic drops from 2.13 to 1.38 GB per
-// 128-column product and the kernel runs 220 us against 229 us on the
+// 128-column product and the kernel runs 210 us against 229 us on the
 // 3M-tet box: the gathers are bounded by the misses an SM keeps in flight,
 // not by their count (measured: the same kernel without its FMAs takes
-// 175 us; with x resident in L2 the time per row is unchanged).
+// 175 us; with x resident in L2 the time per row is unchanged), so the
+// occupancy that holds the most warps gathering at once wins.
 //
 // Lane layout: lane l owns columns [4 l, 4 l + 4).
 #pragma once
@@ -64,8 +65,11 @@ __global__ void rg_coef_kernel(int64_t ng, const int32_t* __restrict__ rows, con
 template <typename T> struct BlkOn { static constexpr bool value = std::is_same<T, float>::value; };
 template <typename T> struct BlkCfg;
 // FP32: 128 columns as 32 lanes x 4
+// U = 4 gathers in flight per warp at 3 blocks per SM (80 registers) beat
+// U = 8 at 2 blocks (118 registers): 0.210 against 0.221 ms on the 3M-tet box;
+// U = 2 at 4 blocks spills (0.229 ms)
 template <> struct BlkCfg<float> {
-  static constexpr int V = 4, U = 8, BPS = 2;
+  static constexpr int V = 4, U = 4, BPS = 3;
 };
 
 template <typename T> static bool blk_cols_ok(int64_t n, int64_t k) {
@@ -134,8 +138,20 @@ spmm_blk_kernel(int64_t k, RowGroupsDev rg, const T* __restrict__ X, T* __restri
       for (int j = 0; j < cntp; j += U) {
         alignas(16) int32_t oo[U];
         ldv_s<int32_t, U>(&s_off[wid][j], oo);
-        alignas(8) uint8_t pmv[U];
-        *reinterpret_cast<uint2*>(pmv) = *reinterpret_cast<const uint2*>(&s_pm[wid][j]);
+        uint8_t pmv[U];
+        if constexpr (U == 8) {
+          alignas(8) uint8_t t8[8];
+          *reinterpret_cast<uint2*>(t8) = *reinterpret_cast<const uint2*>(&s_pm[wid][j]);
+#pragma unroll
+          for (int u = 0; u < 8; ++u) pmv[u] = t8[u];
+        } else if constexpr (U == 4) {
+          const uint32_t w4 = *reinterpret_cast<const uint32_t*>(&s_pm[wid][j]);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) pmv[u] = (uint8_t)(w4 >> (8 * u));
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; ++u) pmv[u] = s_pm[wid][j + u];
+        }
         if (on) {
           alignas(16) T xv[U][V];
 #pragma unroll
