@@ -276,12 +276,13 @@ def run_b200(args):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / ke, world)
     # what one runforward call uploads: the optode positions (located on the
-    # device every call) and the label property table (mua, musp, g rows)
-    # expanded per tet on the device; the mesh and the per-tet labels are
+    # device every call), the per-tet labels (int32) and the label property
+    # table (mua, musp, g rows) expanded per tet on the device; the mesh is
     # uploaded once and kept on the device across calls (as redbirdpy keeps
     # the prepared mesh in cfg)
     props = np.atleast_2d(cfg["prop"])
-    h2d = int(cfg["srcpos"].size * 8 + cfg["detpos"].size * 8 + props.shape[0] * min(3, props.shape[1]) * 8)
+    h2d = int(cfg["srcpos"].size * 8 + cfg["detpos"].size * 8 + np.size(cfg["seg"]) * 4
+              + props.shape[0] * min(3, props.shape[1]) * 8)
     d2h = det_h.nbytes + phi_h.nbytes
 
     # DRAM bytes per launch from an earlier ncu capture of this workload,

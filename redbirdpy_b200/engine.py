@@ -132,14 +132,17 @@ class DeviceMesh:
         return self._evol
 
     def labels(self, seg):
-        """Device int32 copy of a per-tet label array, cached by content (a
-        CRC of its bytes: an array edited in place, or a new array that takes
-        a freed one's id, is uploaded again)."""
-        a = np.ascontiguousarray(seg)
-        key = (a.shape, a.dtype.str, zlib.crc32(memoryview(a).cast("B")))
-        if self._labels[0] != key:
-            self._labels = (key, _i32(a.ravel(), self.device))
-        return self._labels[1]
+        """Device int32 copy of a per-tet label array, uploaded on every call
+        into a buffer kept on the mesh (4 bytes per tet: cheaper than a
+        checksum of the array, and an array edited in place can never be
+        mistaken for the one uploaded before)."""
+        a = np.ascontiguousarray(np.asarray(seg).ravel(), dtype=np.int32)
+        buf = self._labels[1]
+        if buf is None or buf.numel() != a.size:
+            buf = torch.empty(a.size, dtype=torch.int32, device=self.device)
+            self._labels = (None, buf)
+        buf.copy_(torch.from_numpy(a))
+        return buf
 
     def coarse_space(self, target):
         """The CoarseSpace of about ``target`` aggregates (cached per target)."""
