@@ -7,10 +7,12 @@
 //   out = alpha * J^T y   (J FP32 M x K rows, y FP64)              (gemv_t)
 //   sum(J^2)              (Frobenius block scaling, recon.py:235)   (sumsq)
 #include <algorithm>
+#include <mutex>
 
 #include <cuda_bf16.h>
 
 #include "rb_common.cuh"
+#include "rb_tc.cuh"
 
 namespace rb {
 
@@ -54,84 +56,90 @@ __device__ __forceinline__ void load_lower(const double* __restrict__ H, int64_t
 }
 
 // Factor the nb x nb diagonal block at (j0, j0) (lower, L11) and form its
-// inverse X = L11^-1.  256 threads; thread (j = tid / 4, q = tid % 4) owns
-// column j, rows q, q + 4, ..., so the 4 owners of a column are 4 lanes of
-// one warp and exchange through shuffles.  Column c is scaled by its owners
-// (the pivot comes from the lane holding the diagonal), published to shared
-// memory (two buffers, so one barrier per column), and every thread updates
-// its entries right of c.  X is formed column by column by forward
-// substitution (the 4 owners of column j sum their own rows' terms, fixed
-// order) and stored transposed in the block's strict upper triangle:
+// inverse X = L11^-1.  256 threads; the block's lower triangle sits in
+// shared memory.  Column c: every thread reads the pivot and forms its
+// reciprocal square root itself (no hand-off), 64 threads scale the column,
+// and after a barrier the rank-1 update of the columns right of c is spread
+// over all threads (each owns the same ~9 entries of the triangle in every
+// step).  X is then formed column by column by forward substitution (thread
+// (j = tid / 4, q = tid % 4) owns column j, rows q, q + 4, ...; the quad's
+// terms in four interleaved chains, added in fixed order) and stored
+// transposed in the block's strict upper triangle:
 // H[j0 + j][j0 + i] = X[i][j], i > j (the diagonal of X is 1 / L[i][i]).
 // The panel solve and rb_chol_solve then apply X as a product.
+constexpr int kTri = kNB * (kNB + 1) / 2;     // entries of the lower triangle
+constexpr int kTriOwn = (kTri + 255) / 256;  // per thread
 __global__ void __launch_bounds__(256) potrf_diag_kernel(double* __restrict__ H, int64_t ldh, int64_t j0, int nb,
                                                          int* __restrict__ err) {
-  __shared__ double col[2][kNB];
   __shared__ double Ls[kNB][kNB + 1];
+  __shared__ double rdiag[kNB];
   const int tid = threadIdx.x;
-  const int j = tid >> 2, q = tid & 3;
-  const int lane = tid & 31;
-  const unsigned quad = 0xFu << (lane & ~3);
-  double a[kNB / 4];
-#pragma unroll
-  for (int u = 0; u < kNB / 4; ++u) {
-    const int i = q + 4 * u;
-    a[u] = (i < nb && j < nb && i >= j) ? H[(j0 + i) * ldh + j0 + j] : 0.0;
+  for (int e = tid; e < kNB * kNB; e += 256) {
+    const int i = e / kNB, j = e % kNB;
+    Ls[i][j] = (i < nb && j <= i) ? H[(j0 + i) * ldh + j0 + j] : 0.0;
   }
+  // owned entries e = tid + 256 v of the row-major lower triangle, (i, j)
+  // packed as i * 256 + j (-1: none)
+  int own[kTriOwn];
+#pragma unroll
+  for (int v = 0; v < kTriOwn; ++v) {
+    const int e = tid + 256 * v;
+    if (e < kTri) {
+      int i = (int)((sqrtf(8.f * (float)e + 1.f) - 1.f) * 0.5f);
+      while (i * (i + 1) / 2 > e) --i;
+      while ((i + 1) * (i + 2) / 2 <= e) ++i;
+      own[v] = i * 256 + (e - i * (i + 1) / 2);
+    } else {
+      own[v] = -1;
+    }
+  }
+  __syncthreads();
   for (int c = 0; c < nb; ++c) {
-    double* cc = col[c & 1];
-    if (j == c) {  // the 4 owners of column c (one quad of one warp)
-      double d = 0.0;
+    // one reciprocal square root per column on the pivot chain: the pivot
+    // is d / sqrt(d), and the column is scaled by 1 / sqrt(d) (as LAPACK's
+    // dpotf2 scales by the reciprocal)
+    const double d = Ls[c][c];
+    const bool ok = d > 0.0 && isfinite(d);
+    const double rp = ok ? rsqrt(d) : 1.0;
+    if (tid == 0 && !ok) atomicExch(err, (int)(j0 + c) + 1);
+    if (tid > c && tid < nb) Ls[tid][c] *= rp;
+    __syncthreads();
+    // every thread has read the pivot: its entry takes L[c][c] now (the
+    // update below reads only entries below it in column c)
+    if (tid == c) Ls[c][c] = ok ? d * rp : 1.0;
 #pragma unroll
-      for (int u = 0; u < kNB / 4; ++u)
-        if (q + 4 * u == c) d = a[u];
-      d = __shfl_sync(quad, d, (lane & ~3) | (c & 3));
-      const bool ok = d > 0.0 && isfinite(d);
-      const double piv = ok ? sqrt(d) : 1.0;
-      if (!ok && q == 0) atomicExch(err, (int)(j0 + c) + 1);
-#pragma unroll
-      for (int u = 0; u < kNB / 4; ++u) {
-        const int i = q + 4 * u;
-        if (i >= c && i < nb) {
-          a[u] = (i == c) ? piv : a[u] / piv;
-          cc[i] = a[u];
-        }
-      }
+    for (int v = 0; v < kTriOwn; ++v) {
+      const int i = own[v] >> 8, j = own[v] & 255;
+      if (own[v] >= 0 && j > c && i < nb) Ls[i][j] = fma(-Ls[i][c], Ls[j][c], Ls[i][j]);
     }
     __syncthreads();
-    if (j > c && j < nb) {
-      const double lj = cc[j];
-#pragma unroll
-      for (int u = 0; u < kNB / 4; ++u) {
-        const int i = q + 4 * u;
-        if (i >= j && i < nb) a[u] = fma(-cc[i], lj, a[u]);
-      }
-    }
   }
-  // L11 back to H (lower) and to shared memory for the inverse
-#pragma unroll
-  for (int u = 0; u < kNB / 4; ++u) {
-    const int i = q + 4 * u;
-    Ls[i][j] = (i >= j && i < nb && j < nb) ? a[u] : 0.0;
-    if (i >= j && i < nb && j < nb) H[(j0 + i) * ldh + j0 + j] = a[u];
+  // L11 back to H (lower, whole rows)
+  for (int e = tid; e < kNB * kNB; e += 256) {
+    const int i = e / kNB, j = e % kNB;
+    if (i < nb && j <= i) H[(j0 + i) * ldh + j0 + j] = Ls[i][j];
   }
+  if (tid < nb) rdiag[tid] = 1.0 / Ls[tid][tid];  // the 64 reciprocals at once, off the chain below
   __syncthreads();
   // X = L11^-1, column j by the quad of column j: X[j][j] = 1 / L[j][j],
   // X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i]
+  const int j = tid >> 2, q = tid & 3;
   double x[kNB / 4];
 #pragma unroll
   for (int u = 0; u < kNB / 4; ++u) x[u] = 0.0;
   for (int i = 0; i < nb; ++i) {
-    double part = 0.0;
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int u = 0; u < kNB / 4; ++u) {
       const int k = q + 4 * u;
-      if (k >= j && k < i) part = fma(Ls[i][k], x[u], part);
+      if (k >= j && k < i) p[u & 3] = fma(Ls[i][k], x[u], p[u & 3]);
     }
+    double part = (p[0] + p[1]) + (p[2] + p[3]);
     part += __shfl_xor_sync(0xffffffffu, part, 1);
     part += __shfl_xor_sync(0xffffffffu, part, 2);
     if (i >= j && j < nb) {
-      const double xi = (i == j) ? 1.0 / Ls[i][i] : -part / Ls[i][i];
+      const double ri = rdiag[i];
+      const double xi = (i == j) ? ri : -part * ri;
 #pragma unroll
       for (int u = 0; u < kNB / 4; ++u)
         if (q + 4 * u == i) x[u] = xi;
@@ -205,21 +213,66 @@ __global__ void __launch_bounds__(256) trsm_panel_kernel(double* __restrict__ H,
     }
 }
 
-// trailing update A22 -= L21 L21^T on 64 x 64 tiles of the lower triangle.
-// 128 threads, 8 x 4 outputs each; the panel is staged k-major in two
-// 32-column halves so that a thread's 8 (and 4) operands are consecutive in
-// shared memory (16-byte loads; rows padded to 66 doubles).
-// The update reaches columns below c_end only; with c_end < M (the columns
-// of the rest of an outer block) the grid is 2-D, x the row tile and y the
-// column tile, and tiles above the diagonal return at once.
+// trailing update A22 -= L21 L21^T on 64 x 64 tiles of the lower triangle,
+// on the FP64 tensor cores (mma.sync m8n8k4 .f64: D = A B + C, every
+// product and sum in FP64).  128 threads: warp w owns the 32 x 32 quarter
+// (w / 2, w % 2) of the tile as 4 x 4 MMA tiles of 8 x 8.  The panel's rows
+// stream through shared memory in 32-column stages, double-buffered with
+// cp.async (16-byte copies when every row start is 16-byte aligned, else
+// 8-byte copies), rows kept k-contiguous with a stride of 36 doubles so that
+// the fragment loads (8 rows x 4 k per warp) take the minimum two
+// wavefronts.  Rows past M are zero-filled by the copy (source size 0).
+// The panel is columns j0 .. j0 + nb; the tiles start at row and column s0
+// and reach columns below c_end only.  With tri = 0 (a band of columns) the
+// grid is 2-D, x the row tile and y the column tile, and tiles above the
+// diagonal return at once; with tri = 1 (a whole trailing triangle)
+// blockIdx.x enumerates the lower tiles.
 constexpr int kSyrkThreads = 128;
+constexpr int kSyK = 32;             // panel columns per stage
+constexpr int kSyLd = kSyK + 4;      // shared row stride (doubles)
+constexpr int kSyrkSmem = 2 * 2 * kNB * kSyLd * (int)sizeof(double);  // 2 stages x (A, B): 73,728 bytes
+
+__device__ __forceinline__ void cp_async_f64(uint32_t dst, const double* src, int bytes, int src_bytes) {
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// one stage of the panel: rows r0.. (A) and c0.. (B), columns kk.. of the
+// panel (kc of them), into the shared buffers
+template <int CH>
+__device__ __forceinline__ void syrk_stage(const double* __restrict__ H, int64_t ldh, int64_t M, int64_t r0,
+                                           int64_t c0, int64_t kcol, int kc, double* As, double* Bs) {
+  constexpr int PER = kSyK * (int)sizeof(double) / CH;  // copies per row
+  for (int e = threadIdx.x; e < 2 * kNB * PER; e += kSyrkThreads) {
+    const int m = e / (kNB * PER), rem = e % (kNB * PER);
+    const int i = rem / PER, kq = (rem % PER) * (CH / (int)sizeof(double));
+    const int64_t row = (m == 0 ? r0 : c0) + i;
+    const bool in = row < M && kq < kc;
+    const double* src = in ? H + row * ldh + kcol + kq : H;
+    double* dst = (m == 0 ? As : Bs) + i * kSyLd + kq;
+    cp_async_f64(smem_u32(dst), src, CH, in ? min(CH, (kc - kq) * (int)sizeof(double)) : 0);
+  }
+}
+
+template <int CH>
 __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __restrict__ H, int64_t ldh, int64_t M,
-                                                                   int64_t j0, int nb, int64_t c_end) {
-  __shared__ __align__(16) double As[32][kNB + 2];
-  __shared__ __align__(16) double Bs[32][kNB + 2];
-  const int64_t s0 = j0 + nb;  // first trailing row
-  int64_t ti, tj;
-  if (c_end < M) {
+                                                                   int64_t j0, int nb, int64_t s0, int64_t c_end,
+                                                                   int tri) {
+  extern __shared__ __align__(16) double sy[];
+  int64_t ti, tj;  // tile (ti, tj) covers rows s0 + 64 ti .., columns s0 + 64 tj ..
+  if (!tri) {
     ti = blockIdx.x;
     tj = blockIdx.y;
     if (tj > ti) return;
@@ -234,74 +287,81 @@ __global__ void __launch_bounds__(kSyrkThreads) syrk_update_kernel(double* __res
     tj = t;
   }
   const int64_t r0 = s0 + ti * kNB, c0 = s0 + tj * kNB;
-  const int tid = threadIdx.x;
-  const int tr = (tid >> 4) * 8, tc = (tid & 15) * 4;
-  double acc[8][4];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int wm = (w >> 1) * 32, wn = (w & 1) * 32;
+  const int g = lane >> 2, t4 = lane & 3;
+  double acc[4][4][2];
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
+  for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
-  for (int k0 = 0; k0 < nb; k0 += 32) {
-    const int kc = min(32, nb - k0);
-    __syncthreads();
-#pragma unroll 4
-    for (int e = tid; e < kNB * 32; e += kSyrkThreads) {
-      const int i = e >> 5, k = e & 31;
-      As[k][i] = (r0 + i < M && k < kc) ? H[(r0 + i) * ldh + j0 + k0 + k] : 0.0;
-      Bs[k][i] = (c0 + i < M && k < kc) ? H[(c0 + i) * ldh + j0 + k0 + k] : 0.0;
+    for (int n = 0; n < 4; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+  const int nst = (nb + kSyK - 1) / kSyK;
+  auto bufA = [&](int s) { return sy + (s & 1) * 2 * kNB * kSyLd; };
+  auto bufB = [&](int s) { return sy + (s & 1) * 2 * kNB * kSyLd + kNB * kSyLd; };
+  syrk_stage<CH>(H, ldh, M, r0, c0, j0, min(kSyK, nb), bufA(0), bufB(0));
+  cp_async_commit();
+  for (int s = 0; s < nst; ++s) {
+    if (s + 1 < nst) {
+      syrk_stage<CH>(H, ldh, M, r0, c0, j0 + (int64_t)(s + 1) * kSyK, min(kSyK, nb - (s + 1) * kSyK), bufA(s + 1),
+                     bufB(s + 1));
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
-    for (int k = 0; k < kc; ++k) {
-      double a[8], b[4];
-      const double2* pa = reinterpret_cast<const double2*>(&As[k][tr]);
-      const double2* pb = reinterpret_cast<const double2*>(&Bs[k][tc]);
+    const double* A = bufA(s) + (wm + g) * kSyLd + t4;
+    const double* B = bufB(s) + (wn + g) * kSyLd + t4;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const double2 x = pa[u];
-        a[2 * u] = x.x;
-        a[2 * u + 1] = x.y;
-      }
+    for (int ks = 0; ks < kSyK; ks += 4) {
+      double a[4], b[4];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const double2 x = pb[u];
-        b[2 * u] = x.x;
-        b[2 * u + 1] = x.y;
-      }
+      for (int m = 0; m < 4; ++m) a[m] = A[m * 8 * kSyLd + ks];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
+      for (int n = 0; n < 4; ++n) b[n] = B[n * 8 * kSyLd + ks];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) dmma_8x8x4(acc[m][n][0], acc[m][n][1], a[m], b[n]);
     }
+    __syncthreads();  // the buffer is refilled by the stage after next
   }
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
+  for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int64_t i = r0 + tr + u, j = c0 + tc + v;
-      if (i < M && j < c_end && j <= i) H[i * ldh + j] -= acc[u][v];
-    }
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t i = r0 + wm + m * 8 + g, j = c0 + wn + n * 8 + 2 * t4 + h;
+        if (i < M && j < c_end && j <= i) H[i * ldh + j] -= acc[m][n][h];
+      }
 }
 
 // The triangular solves of rb_chol_solve apply the diagonal blocks' inverses
 // X (kept by rb_cholesky in each block's strict upper triangle):
 // mode 0: y = X v (solves L_kk y = v), mode 1: y = X^T v (solves L_kk^T y = v).
 // y = X v (mode 0) or X^T v (mode 1) of diagonal block k0 into shared memory,
-// by all 256 threads of the block (a quad per output, fixed order), v read
-// from src[k0 ..]
+// by all 256 threads of the block: the block's 64 x 64 entries are staged in
+// shared memory first (whole rows, coalesced), then a quad sums each output
+// from there in a fixed order; v is read from src[k0 ..]
 __device__ __forceinline__ void tri_block_apply(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
-                                                const double* __restrict__ src, int mode, double* v, double* y) {
+                                                const double* __restrict__ src, int mode, double* v, double* y,
+                                                double (*Xs)[kNB + 1]) {
   const int tid = threadIdx.x;
-  const int i = tid >> 2, q = tid & 3;
+#pragma unroll 4
+  for (int e = tid; e < kNB * kNB; e += 256) {
+    const int r = e / kNB, c = e % kNB;
+    Xs[r][c] = (r < nb && c < nb) ? L[(k0 + r) * ldh + k0 + c] : 0.0;
+  }
   if (tid < nb) v[tid] = src[k0 + tid];
   __syncthreads();
+  const int i = tid >> 2, q = tid & 3;
   double s = 0.0;
   if (i < nb) {
-    if (mode == 0) {
-      for (int t = q; t <= i; t += 4)
-        s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + t) * ldh + k0 + i], v[t], s);
-    } else {
-      for (int t = i + q; t < nb; t += 4)
-        s = fma(t == i ? 1.0 / L[(k0 + i) * ldh + k0 + i] : L[(k0 + i) * ldh + k0 + t], v[t], s);
+    if (mode == 0) {  // X[i][t], t < i, sits at (t, i)
+      for (int t = q; t <= i; t += 4) s = fma(t == i ? 1.0 / Xs[i][i] : Xs[t][i], v[t], s);
+    } else {  // X[t][i], t > i, sits at (i, t)
+      for (int t = i + q; t < nb; t += 4) s = fma(t == i ? 1.0 / Xs[i][i] : Xs[i][t], v[t], s);
     }
   }
   s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -312,20 +372,37 @@ __device__ __forceinline__ void tri_block_apply(const double* __restrict__ L, in
 
 // One forward step of L y = b, fused: every block solves diagonal block k0
 // (y = X v, v = x[k0 ..]) itself, block 0 stores y in w, and each block
-// subtracts L[r][k0 ..] y from its 8 rows r below the block (a warp per row).
+// subtracts L[r][k0 ..] y from its kSolveRows rows r below the block (rows
+// split over the 8 warps; lane c sums columns c and c + 32, then a warp sum
+// per row).
+constexpr int kSolveRows = 32;
 __global__ void __launch_bounds__(256) fwd_solve_kernel(const double* __restrict__ L, int64_t ldh, int64_t M,
                                                         int64_t k0, int nb, double* __restrict__ x,
                                                         double* __restrict__ w) {
   __shared__ double v[kNB], y[kNB];
-  tri_block_apply(L, ldh, k0, nb, x, 0, v, y);
+  __shared__ double Xs[kNB][kNB + 1];
+  tri_block_apply(L, ldh, k0, nb, x, 0, v, y, Xs);
   if (blockIdx.x == 0 && threadIdx.x < nb) w[k0 + threadIdx.x] = y[threadIdx.x];
-  const int lane = threadIdx.x & 31;
-  const int64_t r = k0 + nb + blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (r >= M) return;
-  double s = 0.0;
-  for (int c = lane; c < nb; c += 32) s += L[r * ldh + k0 + c] * y[c];
-  s = warp_sum(s);
-  if (lane == 0) x[r] -= s;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  constexpr int RW = kSolveRows / 8;  // rows per warp
+  const int64_t rb = k0 + nb + blockIdx.x * (int64_t)kSolveRows + wp * RW;
+  const double y0 = lane < nb ? y[lane] : 0.0, y1 = lane + 32 < nb ? y[lane + 32] : 0.0;
+  double s[RW];
+#pragma unroll
+  for (int u = 0; u < RW; ++u) {
+    const int64_t r = rb + u;
+    s[u] = 0.0;
+    if (r < M) {
+      const double* Lr = L + r * ldh + k0;
+      if (lane < nb) s[u] = Lr[lane] * y0;
+      if (lane + 32 < nb) s[u] = fma(Lr[lane + 32], y1, s[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < RW; ++u) {
+    const double t = warp_sum(s[u]);
+    if (lane == 0 && rb + u < M) x[rb + u] -= t;
+  }
 }
 
 // One backward step of L^T x = y, fused: every block solves diagonal block
@@ -336,7 +413,8 @@ __global__ void __launch_bounds__(256) fwd_solve_kernel(const double* __restrict
 __global__ void __launch_bounds__(256) bwd_solve_kernel(const double* __restrict__ L, int64_t ldh, int64_t k0, int nb,
                                                         double* __restrict__ w, double* __restrict__ x) {
   __shared__ double v[kNB], y[kNB], part[8][32];
-  tri_block_apply(L, ldh, k0, nb, w, 1, v, y);
+  __shared__ double Xs[kNB][kNB + 1];
+  tri_block_apply(L, ldh, k0, nb, w, 1, v, y, Xs);
   if (blockIdx.x == 0 && threadIdx.x < nb) x[k0 + threadIdx.x] = y[threadIdx.x];
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int64_t j = blockIdx.x * 32 + lane;
@@ -374,6 +452,15 @@ __device__ __forceinline__ void ld4(const __nv_bfloat16* p, double (&v)[4]) {
   v[1] = __bfloat162float(a.y);
   v[2] = __bfloat162float(b.x);
   v[3] = __bfloat162float(b.y);
+}
+
+// four consecutive entries of a row as FP32 (BF16 widened exactly)
+__device__ __forceinline__ float4 ld4f(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 ld4f(const __nv_bfloat16* p) {
+  const uint2 x = __ldcs(reinterpret_cast<const uint2*>(p));
+  const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&x.x);
+  const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&x.y);
+  return make_float4(__bfloat162float(a.x), __bfloat162float(a.y), __bfloat162float(b.x), __bfloat162float(b.y));
 }
 
 // J stored as FP32 or BF16 (JT).  A thread owns 4 consecutive columns (one
@@ -425,34 +512,45 @@ __global__ void gemv_t_sum_kernel(const double* __restrict__ part, int slabs, in
   out[k] = alpha * s + (beta != 0.0 ? beta * out[k] : 0.0);
 }
 
-// out[m] = alpha sum_k J[m][k] x[k] + beta out[m] for 4 rows per block: the
-// FP32 (or BF16) rows stream from DRAM once, x (FP64) from L2 once per 4 rows;
-// each thread keeps 4 partial sums per row (k chunks of 4), then a fixed-order
-// block reduction: the result is the same bits on every run.
-constexpr int kGemvNRows = 4;
+// out[m] = alpha sum_k J[m][k] x[k] + beta out[m] in two passes.  Block
+// (cx, ry) takes the 1024 columns [1024 cx, 1024 cx + 1024) (4 per thread,
+// one vector load per row) of kGemvNRows rows, so a warp reads whole 512-byte
+// row segments and the block's rows stream side by side; each row's block
+// sum (fixed-order warp and block reduction) goes to part[m][cx], and
+// gemv_n_sum_kernel adds a row's parts (lane-strided, then a warp sum).
+// The result is the same bits on every run.
+constexpr int kGemvNRows = 16;
+constexpr int kGemvNCols = 1024;
 template <typename JT>
-__global__ void __launch_bounds__(256) gemv_n_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
-                                                     const double* __restrict__ x, double alpha, double beta,
-                                                     double* __restrict__ out) {
+__global__ void __launch_bounds__(256) gemv_n_part_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
+                                                          const double* __restrict__ x, double* __restrict__ part,
+                                                          int64_t nchunk) {
   __shared__ double red[kGemvNRows][8];
-  const int64_t m0 = (int64_t)blockIdx.x * kGemvNRows;
-  double s[kGemvNRows];
+  const int64_t k = (int64_t)blockIdx.x * kGemvNCols + 4 * threadIdx.x;
+  const int64_t m0 = (int64_t)blockIdx.y * kGemvNRows;
+  double xv[4];
 #pragma unroll
-  for (int r = 0; r < kGemvNRows; ++r) s[r] = 0.0;
-  for (int64_t k = 4 * (int64_t)threadIdx.x; k < K; k += 4 * (int64_t)blockDim.x) {
-    double xv[4];
+  for (int j = 0; j < 4; ++j) xv[j] = (k + j < K) ? x[k + j] : 0.0;
+  // every row's load is issued before the first product
+  float4 v[kGemvNRows];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) xv[j] = (k + j < K) ? x[k + j] : 0.0;
+  for (int r = 0; r < kGemvNRows; ++r)
+    v[r] = (k < K && m0 + r < M) ? ld4f(J + (m0 + r) * ldj + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (k + 3 >= K) {  // the padded row's entries past K are dropped (they may hold anything)
 #pragma unroll
     for (int r = 0; r < kGemvNRows; ++r) {
-      if (m0 + r < M) {
-        double v[4];
-        ld4(J + (m0 + r) * ldj + k, v);  // padded row: entries past K are read, then skipped
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (k + j < K) s[r] = fma(v[j], xv[j], s[r]);
-      }
+      if (k + 1 >= K) v[r].y = 0.f;
+      if (k + 2 >= K) v[r].z = 0.f;
+      if (k + 3 >= K) v[r].w = 0.f;
     }
+  }
+  double s[kGemvNRows];
+#pragma unroll
+  for (int r = 0; r < kGemvNRows; ++r) {
+    s[r] = fma((double)v[r].x, xv[0], 0.0);
+    s[r] = fma((double)v[r].y, xv[1], s[r]);
+    s[r] = fma((double)v[r].z, xv[2], s[r]);
+    s[r] = fma((double)v[r].w, xv[3], s[r]);
   }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -463,10 +561,22 @@ __global__ void __launch_bounds__(256) gemv_n_kernel(const JT* __restrict__ J, i
   __syncthreads();
   if (threadIdx.x < kGemvNRows && m0 + threadIdx.x < M) {
     double t = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[threadIdx.x][q];
-    const int64_t m = m0 + threadIdx.x;
-    out[m] = alpha * t + (beta != 0.0 ? beta * out[m] : 0.0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += red[threadIdx.x][q];
+    part[(m0 + threadIdx.x) * nchunk + blockIdx.x] = t;
   }
+}
+
+// a warp per row: out[m] = alpha sum_c part[m][c] + beta out[m]
+__global__ void gemv_n_sum_kernel(const double* __restrict__ part, int64_t nchunk, int64_t M, double alpha,
+                                  double beta, double* __restrict__ out) {
+  const int64_t m = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (m >= M) return;
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int64_t c = lane; c < nchunk; c += 32) s += part[m * nchunk + c];
+  s = warp_sum(s);
+  if (lane == 0) out[m] = alpha * s + (beta != 0.0 ? beta * out[m] : 0.0);
 }
 
 // per-block partial sums of x . y (FP64), fixed order
@@ -583,6 +693,43 @@ __global__ void split_tf32_kernel(float* __restrict__ J, float* __restrict__ lo,
     }
 }
 
+// The two streams of rb_cholesky's look-ahead, per device, created once:
+// the panel stream at the device's highest priority, the bulk-update stream
+// at the default one; both non-blocking.
+struct CholStreams {
+  cudaStream_t panel = nullptr, rest = nullptr;
+};
+static int chol_streams(CholStreams* out) {
+  static std::mutex mu;
+  static CholStreams per_dev[64];
+  int dev = 0;
+  RB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(RB_ESIZE, "rb_cholesky: device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  CholStreams& c = per_dev[dev];
+  if (!c.panel) {
+    int least = 0, greatest = 0;
+    RB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    RB_CUDA_TRY(cudaStreamCreateWithPriority(&c.panel, cudaStreamNonBlocking, greatest));
+    RB_CUDA_TRY(cudaStreamCreateWithPriority(&c.rest, cudaStreamNonBlocking, least));
+  }
+  *out = c;
+  return RB_OK;
+}
+
+// events without timing, destroyed with the set
+struct EventSet {
+  cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+  int n = 0;
+  int make(int k) {
+    for (; n < k; ++n) RB_CUDA_TRY(cudaEventCreateWithFlags(&e[n], cudaEventDisableTiming));
+    return RB_OK;
+  }
+  ~EventSet() {
+    for (int i = 0; i < n; ++i) cudaEventDestroy(e[i]);
+  }
+};
+
 }  // namespace rb
 
 using namespace rb;
@@ -610,34 +757,74 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
   int* err = reinterpret_cast<int*>(work);
   RB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
   RB_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem));
+  // 16-byte panel copies when every row of H starts on a 16-byte boundary
+  const bool ch16 = (reinterpret_cast<uintptr_t>(H) % 16 == 0) && (ldh % 2 == 0);
+  auto syrk = ch16 ? syrk_update_kernel<16> : syrk_update_kernel<8>;
+  RB_CUDA_TRY(cudaFuncSetAttribute(syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, kSyrkSmem));
   // Right-looking in outer blocks of kOuter columns: inside a block each
   // 64-wide panel is factored (diagonal block, panel solve) and updates only
-  // the rest of the block's columns; the rows and columns right of the block
-  // then take one update of depth kOuter.  The trailing matrix is read and
-  // written once per outer block instead of once per panel.
+  // the rest of the block's columns; the trailing matrix then takes one
+  // update of depth kOuter per outer block.  Look-ahead: that update is
+  // split into the next block's column band (on the panel stream, so the
+  // next block can start at once) and the rest of the trailing triangle (on
+  // a second stream, overlapping the next block's serial panel work).  The
+  // panel stream has the higher priority, so its small launches take SMs as
+  // the bulk update's CTAs retire.  Ordering: the rest update of block b
+  // waits for block b's panels (event ev_p); the band update of block b + 1,
+  // which writes tiles the rest update of block b also writes, waits for it
+  // (event ev_r).  Both streams fork from and join back into the caller's.
+  CholStreams cs;
+  RB_TRY(chol_streams(&cs));
+  cudaStream_t sp = cs.panel, sr = cs.rest;
+  EventSet ev;
+  RB_TRY(ev.make(4));
+  cudaEvent_t ev_in = ev.e[0], ev_p = ev.e[1], ev_r = ev.e[2], ev_out = ev.e[3];
+  RB_CUDA_TRY(cudaEventRecord(ev_in, st));
+  RB_CUDA_TRY(cudaStreamWaitEvent(sp, ev_in, 0));
+  RB_CUDA_TRY(cudaStreamWaitEvent(sr, ev_in, 0));
+  bool rest_queued = false;
   constexpr int64_t kOuter = 4 * kNB;
   for (int64_t J0 = 0; J0 < M; J0 += kOuter) {
     const int64_t bend = std::min<int64_t>(J0 + kOuter, M);
     for (int64_t j0 = J0; j0 < bend; j0 += kNB) {
       const int nb = (int)std::min<int64_t>(kNB, M - j0);
-      potrf_diag_kernel<<<1, 256, 0, st>>>(H, ldh, j0, nb, err);
+      potrf_diag_kernel<<<1, 256, 0, sp>>>(H, ldh, j0, nb, err);
       RB_LAUNCH_CHECK();
       const int64_t rest = M - j0 - nb;
       if (rest <= 0) break;
-      trsm_panel_kernel<<<(unsigned)ceil_div(rest, kNB), 256, kTrsmSmem, st>>>(H, ldh, M, j0, nb);
+      trsm_panel_kernel<<<(unsigned)ceil_div(rest, kNB), 256, kTrsmSmem, sp>>>(H, ldh, M, j0, nb);
       RB_LAUNCH_CHECK();
       if (j0 + nb < bend) {  // the block's later panels
         const int64_t T = ceil_div(rest, kNB), Tc = ceil_div(bend - (j0 + nb), kNB);
-        syrk_update_kernel<<<dim3((unsigned)T, (unsigned)Tc), kSyrkThreads, 0, st>>>(H, ldh, M, j0, nb, bend);
+        syrk<<<dim3((unsigned)T, (unsigned)Tc), kSyrkThreads, kSyrkSmem, sp>>>(H, ldh, M, j0, nb, j0 + nb, bend, 0);
         RB_LAUNCH_CHECK();
       }
     }
     const int64_t rest = M - bend;
     if (rest <= 0) break;
-    const int64_t T = ceil_div(rest, kNB);
-    syrk_update_kernel<<<(unsigned)(T * (T + 1) / 2), kSyrkThreads, 0, st>>>(H, ldh, M, J0, (int)(bend - J0), M);
-    RB_LAUNCH_CHECK();
+    const int depth = (int)(bend - J0);
+    const int64_t band_end = std::min<int64_t>(bend + kOuter, M);
+    RB_CUDA_TRY(cudaEventRecord(ev_p, sp));  // block J0's panels are final
+    if (rest_queued) RB_CUDA_TRY(cudaStreamWaitEvent(sp, ev_r, 0));
+    {  // the next block's columns [bend, band_end), all rows below bend
+      const int64_t T = ceil_div(rest, kNB), Tc = ceil_div(band_end - bend, kNB);
+      syrk<<<dim3((unsigned)T, (unsigned)Tc), kSyrkThreads, kSyrkSmem, sp>>>(H, ldh, M, J0, depth, bend, band_end,
+                                                                              0);
+      RB_LAUNCH_CHECK();
+    }
+    if (band_end < M) {  // the trailing triangle right of the band
+      const int64_t T = ceil_div(M - band_end, kNB);
+      RB_CUDA_TRY(cudaStreamWaitEvent(sr, ev_p, 0));
+      syrk<<<(unsigned)(T * (T + 1) / 2), kSyrkThreads, kSyrkSmem, sr>>>(H, ldh, M, J0, depth, band_end, M, 1);
+      RB_LAUNCH_CHECK();
+      RB_CUDA_TRY(cudaEventRecord(ev_r, sr));
+      rest_queued = true;
+    }
   }
+  RB_CUDA_TRY(cudaEventRecord(ev_out, sr));
+  RB_CUDA_TRY(cudaStreamWaitEvent(st, ev_out, 0));
+  RB_CUDA_TRY(cudaEventRecord(ev_out, sp));
+  RB_CUDA_TRY(cudaStreamWaitEvent(st, ev_out, 0));
   int herr = 0;
   RB_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   RB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -655,7 +842,8 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
   for (int64_t k0 = 0; k0 < M; k0 += kNB) {  // L y = b
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
     const int64_t rest = M - k0 - nb;
-    fwd_solve_kernel<<<(unsigned)std::max<int64_t>(1, ceil_div(rest, 8)), 256, 0, st>>>(L, ldh, M, k0, nb, x, w);
+    fwd_solve_kernel<<<(unsigned)std::max<int64_t>(1, ceil_div(rest, kSolveRows)), 256, 0, st>>>(L, ldh, M, k0, nb,
+                                                                                                 x, w);
     RB_LAUNCH_CHECK();
   }
   for (int64_t k0 = ((M - 1) / kNB) * kNB; k0 >= 0; k0 -= kNB) {  // L^T x = y
@@ -697,9 +885,17 @@ static int gemv_n_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const doub
   if ((reinterpret_cast<uintptr_t>(J) & (4 * sizeof(JT) - 1)) || (ldj % 4) || ldj < ceil_div(K, 4) * 4)
     return fail(RB_EARG, "rb_gemv_n: J rows must start on %d-byte boundaries and hold K rounded up to 4 entries",
                 (int)(4 * sizeof(JT)));
-  gemv_n_kernel<JT><<<(unsigned)ceil_div(M, kGemvNRows), 256, 0, as_stream(stream)>>>(J, M, K, ldj, x, alpha, beta,
-                                                                                       out);
+  if (ceil_div(M, kGemvNRows) > 65535) return fail(RB_ESIZE, "rb_gemv_n: too many rows");
+  cudaStream_t st = as_stream(stream);
+  const int64_t nchunk = ceil_div(K, kGemvNCols);
+  double* part = nullptr;  // M x nchunk row parts (stream-ordered allocation)
+  RB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * M * nchunk, st));
+  gemv_n_part_kernel<JT><<<dim3((unsigned)nchunk, (unsigned)ceil_div(M, kGemvNRows)), 256, 0, st>>>(J, M, K, ldj, x,
+                                                                                                   part, nchunk);
   RB_LAUNCH_CHECK();
+  gemv_n_sum_kernel<<<(unsigned)ceil_div(M, 8), 256, 0, st>>>(part, nchunk, M, alpha, beta, out);
+  RB_LAUNCH_CHECK();
+  RB_CUDA_TRY(cudaFreeAsync(part, st));
   return RB_OK;
 }
 

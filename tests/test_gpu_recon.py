@@ -138,7 +138,7 @@ def test_matreform_matches_reference(golden):
         rbb.matreform(g["Jc"], g["y0"], g["y1"], "nope")
 
 
-@pytest.mark.parametrize("M", [5, 64, 65, 300, 1030])
+@pytest.mark.parametrize("M", [5, 64, 65, 300, 1030, 1152, 1153, 2101, 4096])
 def test_cholesky_and_solve(M):
     import ctypes
 
@@ -154,6 +154,34 @@ def test_cholesky_and_solve(M):
     x = torch.as_tensor(b.copy(), device="cuda")
     engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.stream())
     np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("M,K", [(5, 3), (70, 1030), (1000, 4097)])
+def test_gemv_passes_over_padded_rows(M, K):
+    """J x and J^T y over FP32 (and BF16) rows padded to a multiple of 4
+    with NaN past K: FP64 accumulation, the padding never read into a sum,
+    the beta term applied."""
+    rng = np.random.default_rng(M + K)
+    ldj = (K + 3) // 4 * 4
+    J = np.full((M, ldj), np.nan, dtype=np.float32)
+    J[:, :K] = rng.standard_normal((M, K))
+    x, y = rng.standard_normal(K), rng.standard_normal(M)
+    Jd = torch.as_tensor(J, device="cuda")
+    xd, yd = torch.as_tensor(x, device="cuda"), torch.as_tensor(y, device="cuda")
+    Jk = J[:, :K].astype(np.float64)
+    ref_n = Jk @ x
+    np.testing.assert_allclose(engine.gemv_n(Jd, K, xd, 2.0).cpu().numpy(), 2.0 * ref_n, rtol=1e-11,
+                               atol=1e-12 * np.abs(ref_n).max())
+    out = torch.ones(M, dtype=torch.float64, device="cuda")
+    engine.gemv_n(Jd, K, xd, 1.0, 3.0, out=out)
+    np.testing.assert_allclose(out.cpu().numpy(), 3.0 + ref_n, rtol=1e-11, atol=1e-12 * np.abs(ref_n).max())
+    ref_t = Jk.T @ y
+    np.testing.assert_allclose(engine.gemv_t(Jd, K, yd, 0.5).cpu().numpy(), 0.5 * ref_t, rtol=1e-11,
+                               atol=1e-12 * np.abs(ref_t).max())
+    Jb = Jd.to(torch.bfloat16)
+    Jbk = Jb.float().cpu().numpy()[:, :K].astype(np.float64)
+    np.testing.assert_allclose(engine.gemv_n(Jb, K, xd).cpu().numpy(), Jbk @ x, rtol=1e-11,
+                               atol=1e-12 * np.abs(ref_n).max())
 
 
 @pytest.mark.parametrize("M,cond", [(300, 1e8), (1030, 1e10)])
