@@ -627,20 +627,55 @@ __global__ void sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int
 // With bf != NULL the pass also writes the rows rounded to BF16 (row stride
 // ldb, the padding columns K..ldb-1 zeroed): the operand of a BF16 product
 // whose refinement runs over the FP32 rows.
-template <typename JT>
+template <typename JT, bool VEC>
 __global__ void row_sumsq_kernel(const JT* __restrict__ J, int64_t M, int64_t K, int64_t ldj,
                                  double* __restrict__ out, __nv_bfloat16* __restrict__ bf, int64_t ldb) {
   __shared__ double red[32];
   for (int64_t m = blockIdx.x; m < M; m += gridDim.x) {
     double s = 0.0;
-    for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-      const JT x = J[m * ldj + k];
-      const double v = jval(x);
-      s += v * v;
-      if (bf) bf[m * ldb + k] = __float2bfloat16_rn((float)v);
+    int64_t kpad = K;  // first column of the BF16 row's zero padding
+    if constexpr (VEC) {
+      // 4 columns per thread and chunk: one 16-byte (BF16: 8-byte) load and
+      // one 8-byte store; four chunks' loads are issued before their sums
+      kpad = (K + 3) / 4 * 4;
+      constexpr int U = 4;
+      const int64_t step = 4 * (int64_t)blockDim.x;
+      for (int64_t k0 = 4 * (int64_t)threadIdx.x; k0 < K; k0 += U * step) {
+        float4 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t k = k0 + u * step;
+          v[u] = k < K ? ld4f(J + m * ldj + k) : make_float4(0.f, 0.f, 0.f, 0.f);  // inside the row (ldj % 4 == 0)
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t k = k0 + u * step;
+          if (k >= K) break;
+          if (k + 1 >= K) v[u].y = 0.f;  // entries past K are dropped
+          if (k + 2 >= K) v[u].z = 0.f;
+          if (k + 3 >= K) v[u].w = 0.f;
+          s = fma((double)v[u].x, (double)v[u].x, s);
+          s = fma((double)v[u].y, (double)v[u].y, s);
+          s = fma((double)v[u].z, (double)v[u].z, s);
+          s = fma((double)v[u].w, (double)v[u].w, s);
+          if (bf) {
+            __nv_bfloat162 lo = __floats2bfloat162_rn(v[u].x, v[u].y), hi = __floats2bfloat162_rn(v[u].z, v[u].w);
+            uint2 w;
+            w.x = *reinterpret_cast<uint32_t*>(&lo);
+            w.y = *reinterpret_cast<uint32_t*>(&hi);
+            *reinterpret_cast<uint2*>(bf + m * ldb + k) = w;
+          }
+        }
+      }
+    } else {
+      for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+        const double v = jval(J[m * ldj + k]);
+        s = fma(v, v, s);
+        if (bf) bf[m * ldb + k] = __float2bfloat16_rn((float)v);
+      }
     }
     if (bf)
-      for (int64_t k = K + threadIdx.x; k < ldb; k += blockDim.x) bf[m * ldb + k] = __float2bfloat16_rn(0.f);
+      for (int64_t k = kpad + threadIdx.x; k < ldb; k += blockDim.x) bf[m * ldb + k] = __float2bfloat16_rn(0.f);
     s = warp_sum(s);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -1002,7 +1037,13 @@ static int row_sumsq_run(const JT* J, int64_t M, int64_t K, int64_t ldj, double*
   if (bf && (ldb < K || ldb % 8)) return fail(RB_EARG, "rb_row_sumsq_to_bf16: ldb must be >= K and a multiple of 8");
   cudaStream_t st = as_stream(stream);
   const unsigned nb = (unsigned)std::min<int64_t>(M, 148 * 16);
-  row_sumsq_kernel<JT><<<nb, 256, 0, st>>>(J, M, K, ldj, rows, bf, ldb);
+  // vector path: rows start on 4-entry boundaries (and, for the copy, the BF16 rows on 8-byte ones)
+  const bool vec = (reinterpret_cast<uintptr_t>(J) % (4 * sizeof(JT)) == 0) && ldj % 4 == 0 &&
+                   (!bf || reinterpret_cast<uintptr_t>(bf) % 8 == 0);
+  if (vec)
+    row_sumsq_kernel<JT, true><<<nb, 256, 0, st>>>(J, M, K, ldj, rows, bf, ldb);
+  else
+    row_sumsq_kernel<JT, false><<<nb, 256, 0, st>>>(J, M, K, ldj, rows, bf, ldb);
   RB_LAUNCH_CHECK();
   if (total) {
     sum_parts_kernel<<<1, 1024, 0, st>>>(rows, (int)M, total);
