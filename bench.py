@@ -525,7 +525,9 @@ def run_gn_step(cfg, mesh, world, args):
         work = torch.empty(wb, dtype=torch.uint8, device=J.device)
         engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), wb, engine.stream())
         t = di * torch.as_tensor(mis, device=J.device)
-        engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.stream())
+        cwb = engine._lib.lib().rb_chol_solve_work_bytes(M)
+        cwork = torch.empty(cwb, dtype=torch.uint8, device=J.device)
+        engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(t), engine.ptr(cwork), cwb, engine.stream())
         dmu = torch.mv(J.T, di * t) * s2
         return dmu.cpu().numpy()
 

@@ -509,7 +509,9 @@ int rb_split_tf32(float* J, float* lo, int64_t M, int64_t K, int64_t ldj, void* 
 int rb_reginv_prepare(double* H, int64_t M, int64_t ldh, double lambda, double* di, void* stream);
 size_t rb_cholesky_work_bytes(void);
 int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes, void* stream);
-int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stream);
+/* rb_chol_solve's workspace: M doubles (the forward solution) */
+size_t rb_chol_solve_work_bytes(int64_t M);
+int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* work, size_t work_bytes, void* stream);
 size_t rb_gemv_t_work_bytes(int64_t K);
 int rb_gemv_t(const float* J, int64_t M, int64_t K, int64_t ldj, const double* y, double alpha,
               double beta, double* out, void* work, size_t work_bytes, void* stream);
@@ -545,10 +547,13 @@ int rb_vec_mul(const double* a, const double* b, double* out, int64_t n, void* s
  *                                  a multiple of 4 entries; x FP64, K entries)
  *   y = a x + b y                  rb_axpby
  *   x . y                          rb_dot (the residual norms) */
+/* rb_gemv_n's workspace: the per-row parts of each 1024-column chunk
+ * (M x ceil(K / 1024) doubles) */
+size_t rb_gemv_n_work_bytes(int64_t M, int64_t K);
 int rb_gemv_n(const float* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
-              double* out, void* stream);
+              double* out, void* work, size_t work_bytes, void* stream);
 int rb_gemv_n_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
-                   double* out, void* stream);
+                   double* out, void* work, size_t work_bytes, void* stream);
 int rb_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
 /* *out = x . y (FP64, device scalar; fixed-order reduction) */
 size_t rb_dot_work_bytes(void);

@@ -133,7 +133,8 @@ _SIGS = {
     "rb_reginv_prepare": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _vp, _vp]),
     "rb_cholesky_work_bytes": (_sz, []),
     "rb_cholesky": (ctypes.c_int, [_vp, _i64, _i64, _vp, _sz, _vp]),
-    "rb_chol_solve": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
+    "rb_chol_solve_work_bytes": (_sz, [_i64]),
+    "rb_chol_solve": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _sz, _vp]),
     "rb_gemv_t_work_bytes": (_sz, [_i64]),
     "rb_gemv_t": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
     "rb_gemv_t_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
@@ -145,8 +146,9 @@ _SIGS = {
     "rb_row_sumsq_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _vp]),
     "rb_set_diag": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, _vp]),
     "rb_row_sumsq_to_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp]),
-    "rb_gemv_n": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
-    "rb_gemv_n_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp]),
+    "rb_gemv_n_work_bytes": (_sz, [_i64, _i64]),
+    "rb_gemv_n": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
+    "rb_gemv_n_bf16": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, _dbl, _vp, _vp, _sz, _vp]),
     "rb_axpby": (ctypes.c_int, [_i64, _dbl, _vp, _dbl, _vp, _vp]),
     "rb_dot_work_bytes": (_sz, []),
     "rb_dot": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _sz, _vp]),

@@ -867,13 +867,15 @@ int rb_cholesky(double* H, int64_t M, int64_t ldh, void* work, size_t work_bytes
   return RB_OK;
 }
 
-int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stream) {
-  if (!L || !x || M < 1 || ldh < M) return fail(RB_EARG, "rb_chol_solve: bad arguments");
+size_t rb_chol_solve_work_bytes(int64_t M) { return (size_t)std::max<int64_t>(M, 1) * sizeof(double); }
+
+int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* work, size_t work_bytes, void* stream) {
+  if (!L || !x || !work || M < 1 || ldh < M) return fail(RB_EARG, "rb_chol_solve: bad arguments");
+  if (work_bytes < rb_chol_solve_work_bytes(M)) return fail(RB_EARG, "rb_chol_solve: workspace too small");
   cudaStream_t st = as_stream(stream);
   // one launch per diagonal block and direction: each block of a launch
   // solves the 64 x 64 diagonal step itself and then its share of the update
-  double* w = nullptr;  // the forward solution, consumed by the backward steps
-  RB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&w), sizeof(double) * M, st));
+  double* w = reinterpret_cast<double*>(work);  // the forward solution, consumed by the backward steps
   for (int64_t k0 = 0; k0 < M; k0 += kNB) {  // L y = b
     const int nb = (int)std::min<int64_t>(kNB, M - k0);
     const int64_t rest = M - k0 - nb;
@@ -886,7 +888,6 @@ int rb_chol_solve(const double* L, int64_t M, int64_t ldh, double* x, void* stre
     bwd_solve_kernel<<<(unsigned)std::max<int64_t>(1, ceil_div(k0, 32)), 256, 0, st>>>(L, ldh, k0, nb, w, x);
     RB_LAUNCH_CHECK();
   }
-  RB_CUDA_TRY(cudaFreeAsync(w, st));
   return RB_OK;
 }
 
@@ -915,35 +916,39 @@ static int gemv_t_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const doub
 
 template <typename JT>
 static int gemv_n_run(const JT* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
-                      double* out, void* stream) {
+                      double* out, void* work, size_t work_bytes, void* stream) {
   if (!J || !x || !out || M < 1 || K < 1 || ldj < K) return fail(RB_EARG, "rb_gemv_n: bad arguments");
   if ((reinterpret_cast<uintptr_t>(J) & (4 * sizeof(JT) - 1)) || (ldj % 4) || ldj < ceil_div(K, 4) * 4)
     return fail(RB_EARG, "rb_gemv_n: J rows must start on %d-byte boundaries and hold K rounded up to 4 entries",
                 (int)(4 * sizeof(JT)));
   if (ceil_div(M, kGemvNRows) > 65535) return fail(RB_ESIZE, "rb_gemv_n: too many rows");
+  if (!work || work_bytes < rb_gemv_n_work_bytes(M, K)) return fail(RB_EARG, "rb_gemv_n: workspace too small");
   cudaStream_t st = as_stream(stream);
   const int64_t nchunk = ceil_div(K, kGemvNCols);
-  double* part = nullptr;  // M x nchunk row parts (stream-ordered allocation)
-  RB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * M * nchunk, st));
+  double* part = reinterpret_cast<double*>(work);  // M x nchunk row parts
   gemv_n_part_kernel<JT><<<dim3((unsigned)nchunk, (unsigned)ceil_div(M, kGemvNRows)), 256, 0, st>>>(J, M, K, ldj, x,
                                                                                                    part, nchunk);
   RB_LAUNCH_CHECK();
   gemv_n_sum_kernel<<<(unsigned)ceil_div(M, 8), 256, 0, st>>>(part, nchunk, M, alpha, beta, out);
   RB_LAUNCH_CHECK();
-  RB_CUDA_TRY(cudaFreeAsync(part, st));
   return RB_OK;
 }
 
 extern "C" {
 
+size_t rb_gemv_n_work_bytes(int64_t M, int64_t K) {
+  return (size_t)std::max<int64_t>(M, 1) * (size_t)std::max<int64_t>(ceil_div(K, kGemvNCols), 1) * sizeof(double);
+}
+
 int rb_gemv_n(const float* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
-              double* out, void* stream) {
-  return gemv_n_run(J, M, K, ldj, x, alpha, beta, out, stream);
+              double* out, void* work, size_t work_bytes, void* stream) {
+  return gemv_n_run(J, M, K, ldj, x, alpha, beta, out, work, work_bytes, stream);
 }
 
 int rb_gemv_n_bf16(const void* J, int64_t M, int64_t K, int64_t ldj, const double* x, double alpha, double beta,
-                   double* out, void* stream) {
-  return gemv_n_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, x, alpha, beta, out, stream);
+                   double* out, void* work, size_t work_bytes, void* stream) {
+  return gemv_n_run(reinterpret_cast<const __nv_bfloat16*>(J), M, K, ldj, x, alpha, beta, out, work, work_bytes,
+                    stream);
 }
 
 size_t rb_dot_work_bytes(void) { return 64 * sizeof(double) + 256; }

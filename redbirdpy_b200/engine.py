@@ -1063,9 +1063,11 @@ def gemv_n(J, K, x, alpha=1.0, beta=0.0, out=None, lo=None):
     if out is None:
         out = torch.empty(M, dtype=torch.float64, device=J.device)
     fn = "rb_gemv_n_bf16" if J.dtype == torch.bfloat16 else "rb_gemv_n"
-    call(fn, ptr(J), M, K, ldj, ptr(x), float(alpha), float(beta), ptr(out), stream())
+    wb = _lib.lib().rb_gemv_n_work_bytes(M, K)
+    work = torch.empty(wb, dtype=torch.uint8, device=J.device)
+    call(fn, ptr(J), M, K, ldj, ptr(x), float(alpha), float(beta), ptr(out), ptr(work), wb, stream())
     if lo is not None:
-        call("rb_gemv_n", ptr(lo), M, K, ldj, ptr(x), float(alpha), 1.0, ptr(out), stream())
+        call("rb_gemv_n", ptr(lo), M, K, ldj, ptr(x), float(alpha), 1.0, ptr(out), ptr(work), wb, stream())
     return out
 
 
@@ -1279,10 +1281,13 @@ def normal_solve(J, K, H, di, r, lam, alpha=1.0, lo=None, refine=3, refine_tol=1
     dev = H.device
     rr = torch.as_tensor(np.ascontiguousarray(r, dtype=np.float64), device=dev) if not torch.is_tensor(r) else r
 
+    cwb = _lib.lib().rb_chol_solve_work_bytes(M)
+    cwork = torch.empty(cwb, dtype=torch.uint8, device=dev)
+
     def precond(v):
         t = torch.empty(M, dtype=torch.float64, device=dev)
         call("rb_vec_mul", ptr(di), ptr(v), ptr(t), M, stream())
-        call("rb_chol_solve", ptr(H), M, M, ptr(t), stream())
+        call("rb_chol_solve", ptr(H), M, M, ptr(t), ptr(cwork), cwb, stream())
         out = torch.empty(M, dtype=torch.float64, device=dev)
         call("rb_vec_mul", ptr(di), ptr(t), ptr(out), M, stream())
         return out

@@ -152,7 +152,9 @@ def test_cholesky_and_solve(M):
     L = np.tril(H.cpu().numpy())
     np.testing.assert_allclose(L, np.linalg.cholesky(A), rtol=1e-10, atol=1e-12 * np.abs(L).max())
     x = torch.as_tensor(b.copy(), device="cuda")
-    engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.stream())
+    cwb = engine._lib.lib().rb_chol_solve_work_bytes(M)
+    cwork = torch.empty(cwb, dtype=torch.uint8, device="cuda")
+    engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.ptr(cwork), cwb, engine.stream())
     np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-12)
 
 
@@ -199,7 +201,9 @@ def test_cholesky_solve_ill_conditioned(M, cond):
     work = torch.empty(engine._lib.lib().rb_cholesky_work_bytes(), dtype=torch.uint8, device="cuda")
     engine.call("rb_cholesky", engine.ptr(H), M, M, engine.ptr(work), work.numel(), engine.stream())
     x = torch.as_tensor(b.copy(), device="cuda")
-    engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.stream())
+    cwb = engine._lib.lib().rb_chol_solve_work_bytes(M)
+    cwork = torch.empty(cwb, dtype=torch.uint8, device="cuda")
+    engine.call("rb_chol_solve", engine.ptr(H), M, M, engine.ptr(x), engine.ptr(cwork), cwb, engine.stream())
     x = x.cpu().numpy()
     xr = np.linalg.solve(A, b)
 
