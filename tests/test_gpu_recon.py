@@ -158,6 +158,31 @@ def test_cholesky_and_solve(M):
     np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("M,ldh,offset", [(1100, 1103, 0), (1100, 1104, 1), (1280, 1280, 1)])
+def test_cholesky_strided_and_unaligned(M, ldh, offset):
+    """A matrix inside a wider buffer (ldh > M, odd or even) and starting 8
+    bytes past a 16-byte boundary: the trailing updates then copy the panel
+    in 8-byte pieces; the factor and the solve match LAPACK's.  M = 1280 ends
+    its last outer block exactly at M (the in-block update's 2-D mode)."""
+    rng = np.random.default_rng(M + ldh + offset)
+    B = rng.standard_normal((M, M + 5))
+    A = B @ B.T + M * np.eye(M)
+    b = rng.standard_normal(M)
+    buf = torch.zeros(offset + M * ldh, dtype=torch.float64, device="cuda")
+    H = buf[offset:].view(M, ldh)
+    H[:, :M] = torch.as_tensor(A, device="cuda")
+    assert (H.data_ptr() % 16 == 0) == (offset == 0)
+    work = torch.empty(engine._lib.lib().rb_cholesky_work_bytes(), dtype=torch.uint8, device="cuda")
+    engine.call("rb_cholesky", engine.ptr(H), M, ldh, engine.ptr(work), work.numel(), engine.stream())
+    L = np.tril(H[:, :M].cpu().numpy())
+    np.testing.assert_allclose(L, np.linalg.cholesky(A), rtol=1e-10, atol=1e-12 * np.abs(L).max())
+    x = torch.as_tensor(b.copy(), device="cuda")
+    cwb = engine._lib.lib().rb_chol_solve_work_bytes(M)
+    cwork = torch.empty(cwb, dtype=torch.uint8, device="cuda")
+    engine.call("rb_chol_solve", engine.ptr(H), M, ldh, engine.ptr(x), engine.ptr(cwork), cwb, engine.stream())
+    np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-9, atol=1e-12)
+
+
 @pytest.mark.parametrize("M,K", [(5, 3), (70, 1030), (1000, 4097)])
 def test_gemv_passes_over_padded_rows(M, K):
     """J x and J^T y over FP32 (and BF16) rows padded to a multiple of 4
