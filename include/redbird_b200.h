@@ -481,7 +481,13 @@ int rb_adjoint_fields(const void* phi, int64_t nn, int64_t ld, int64_t dcol0, co
  *   H += lambda I, normalise   rb_reginv_prepare (_normalize_diag, recon.py:784-789)
  *   H = L L^T                  rb_cholesky (FP64, in place, lower; the strict
  *                              upper triangle of each 64 x 64 diagonal block
- *                              receives that block's inverse, transposed)
+ *                              receives that block's inverse, transposed).  The
+ *                              factorization forks onto two library-owned
+ *                              streams per device (created on first use: the
+ *                              panel steps at the highest priority, the bulk
+ *                              trailing updates beside them), joins them back
+ *                              into `stream` and synchronizes it before
+ *                              returning (it reads the pivot check back)
  *   L L^T x = b                rb_chol_solve (in place on x; L as rb_cholesky
  *                              leaves it, diagonal-block inverses included)
  *   out = alpha J^T y + beta out   rb_gemv_t (J aligned as for rb_gram; ldj % 4 == 0)
