@@ -94,25 +94,54 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(double* __restrict__ H,
     }
   }
   __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    // one reciprocal square root per column on the pivot chain: the pivot
-    // is d / sqrt(d), and the column is scaled by 1 / sqrt(d) (as LAPACK's
-    // dpotf2 scales by the reciprocal)
-    const double d = Ls[c][c];
-    const bool ok = d > 0.0 && isfinite(d);
-    const double rp = ok ? rsqrt(d) : 1.0;
-    if (tid == 0 && !ok) atomicExch(err, (int)(j0 + c) + 1);
-    if (tid > c && tid < nb) Ls[tid][c] *= rp;
-    __syncthreads();
-    // every thread has read the pivot: its entry takes L[c][c] now (the
-    // update below reads only entries below it in column c)
-    if (tid == c) Ls[c][c] = ok ? d * rp : 1.0;
+  // Two columns per step (one barrier pair instead of two): with c and c + 1,
+  // every thread forms both pivots itself; thread i scales its entry of
+  // column c, takes column c's update of its entry of column c + 1 and
+  // scales that; then the owned entries right of c + 1 take both updates,
+  // column c's first.  Every entry sees the same operations in the same
+  // order as in one column per step, so the factor is the same bits.
+  // One reciprocal square root per column: the pivot is d / sqrt(d), and
+  // the column is scaled by 1 / sqrt(d) (as LAPACK's dpotf2 scales by the
+  // reciprocal).
+  for (int c = 0; c < nb; c += 2) {
+    if (c + 1 < nb) {
+      const double d0 = Ls[c][c], a10 = Ls[c + 1][c], a11 = Ls[c + 1][c + 1];
+      const bool ok0 = d0 > 0.0 && isfinite(d0);
+      const double rp0 = ok0 ? rsqrt(d0) : 1.0;
+      const double l10 = a10 * rp0;
+      const double d1 = fma(-l10, l10, a11);
+      const bool ok1 = d1 > 0.0 && isfinite(d1);
+      const double rp1 = ok1 ? rsqrt(d1) : 1.0;
+      if (tid == 0 && (!ok0 || !ok1)) atomicExch(err, (int)(j0 + c + (ok0 ? 1 : 0)) + 1);
+      if (tid > c + 1 && tid < nb) {
+        const double li0 = Ls[tid][c] * rp0;
+        Ls[tid][c] = li0;
+        Ls[tid][c + 1] = fma(-li0, l10, Ls[tid][c + 1]) * rp1;
+      }
+      __syncthreads();
+      // every thread has read the pivots: their entries take L now (the
+      // update below reads only the entries below them in columns c, c + 1)
+      if (tid == c) Ls[c][c] = ok0 ? d0 * rp0 : 1.0;
+      if (tid == c + 1) {
+        Ls[c + 1][c] = l10;
+        Ls[c + 1][c + 1] = ok1 ? d1 * rp1 : 1.0;
+      }
 #pragma unroll
-    for (int v = 0; v < kTriOwn; ++v) {
-      const int i = own[v] >> 8, j = own[v] & 255;
-      if (own[v] >= 0 && j > c && i < nb) Ls[i][j] = fma(-Ls[i][c], Ls[j][c], Ls[i][j]);
+      for (int v = 0; v < kTriOwn; ++v) {
+        const int i = own[v] >> 8, j = own[v] & 255;
+        if (own[v] >= 0 && j > c + 1 && i < nb)
+          Ls[i][j] = fma(-Ls[i][c + 1], Ls[j][c + 1], fma(-Ls[i][c], Ls[j][c], Ls[i][j]));
+      }
+      __syncthreads();
+    } else {  // the last column of an odd block
+      const double d = Ls[c][c];
+      const bool ok = d > 0.0 && isfinite(d);
+      const double rp = ok ? rsqrt(d) : 1.0;
+      if (tid == 0 && !ok) atomicExch(err, (int)(j0 + c) + 1);
+      __syncthreads();
+      if (tid == c) Ls[c][c] = ok ? d * rp : 1.0;
+      __syncthreads();
     }
-    __syncthreads();
   }
   // L11 back to H (lower, whole rows)
   for (int e = tid; e < kNB * kNB; e += 256) {
