@@ -33,28 +33,6 @@ __global__ void prep_scale_kernel(double* __restrict__ H, int64_t M, int64_t ldh
   H[i * ldh + j] *= di[i] * di[j];
 }
 
-// Stage the lower triangle of the nb x nb block at (r0, c0) of H into
-// shared memory (zeros above the diagonal), all loads issued before the
-// stores so that they overlap (the block is read once from L2/HBM).
-template <int LD>
-__device__ __forceinline__ void load_lower(const double* __restrict__ H, int64_t ldh, int64_t r0, int64_t c0, int nb,
-                                           double (*A)[LD]) {
-  constexpr int kPer = 16;
-  for (int e0 = threadIdx.x; e0 < kNB * kNB; e0 += kPer * blockDim.x) {
-    double v[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int e = e0 + u * blockDim.x, i = e / kNB, j = e % kNB;
-      v[u] = (e < kNB * kNB && i < nb && j <= i) ? H[(r0 + i) * ldh + c0 + j] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int e = e0 + u * blockDim.x;
-      if (e < kNB * kNB) A[e / kNB][e % kNB] = v[u];
-    }
-  }
-}
-
 // Factor the nb x nb diagonal block at (j0, j0) (lower, L11) and form its
 // inverse X = L11^-1.  256 threads; the block's lower triangle sits in
 // shared memory.  Column c: every thread reads the pivot and forms its
