@@ -174,3 +174,84 @@ def test_gram_staging_rule():
     assert sb(M, 600001, 600008, 2, 0) == M * 65536 * 2 + 256  # BF16 rows of 1.2 MB
     assert sb(M, 300001, 300008, 2, 0) == 0              # BF16 rows of 600 KB
     assert sb(0, 1040502, 1040504, 4, 0) == 0 and sb(M, 1040502, 1040504, 3, 0) == 0
+
+
+def test_jacobian_slab_width_rule(monkeypatch):
+    """runrecon stores J whole while it fits in half the free HBM, else
+    recomputes it in node slabs of a quarter of the free memory (rows x
+    parameters x slab x element size); an explicit width is kept."""
+    torch = pytest.importorskip("torch")
+    from redbirdpy_b200 import recon
+
+    class Mesh:
+        nn = 520251
+
+    phi = torch.zeros(1, dtype=torch.complex128)  # frequency domain: [Re; Im] rows
+    sd = np.column_stack([np.zeros(4096), np.ones(4096), np.ones(4096)])
+    sd[:10, 2] = 0  # inactive pairs add no rows
+    rows = 2 * 4086
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (180e9, 183e9))
+    assert recon._slab_width("auto", Mesh, phi, sd, 2, torch.float32) == 0  # 34 GB <= 90 GB
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (40e9, 183e9))
+    w = recon._slab_width("auto", Mesh, phi, sd, 2, torch.float32)
+    assert w == int(0.25 * 40e9 / (rows * 2 * 4))
+    assert recon._slab_width("auto", Mesh, phi, sd, 2, torch.bfloat16) == 0  # BF16 rows: 17 GB <= 20 GB
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (30e9, 183e9))
+    assert recon._slab_width("auto", Mesh, phi, sd, 2, torch.bfloat16) == int(0.25 * 30e9 / (rows * 2 * 2))
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (1e6, 183e9))
+    assert recon._slab_width("auto", Mesh, phi, sd, 2, torch.float32) == 1024  # floor
+    assert recon._slab_width(None, Mesh, phi, sd, 2, torch.float32) == 0
+    assert recon._slab_width(False, Mesh, phi, sd, 2, torch.float32) == 0
+    assert recon._slab_width(5000, Mesh, phi, sd, 2, torch.float32) == 5000
+
+
+def test_solve_tuner_picks_the_fastest_and_caches_per_bucket(monkeypatch):
+    """The autotuner times every (lanes, check interval) candidate, skips
+    those that did not converge, keeps the fastest and reuses it for every
+    system of the same size bucket; another bucket is tuned afresh."""
+    torch = pytest.importorskip("torch")
+    from redbirdpy_b200 import engine
+
+    ms = {(0, 10): 9.0, (0, 20): 8.0, (8, 10): 3.0, (8, 20): 1.0, (16, 10): 2.0, (16, 20): 4.0,
+          (32, 10): 5.0, (32, 20): 6.0}
+    calls = []
+
+    def fake_solve(mat, B, **kw):
+        key = (kw["spmm_lanes"], kw["check_every"])
+        calls.append(key)
+        clock["now"] += ms[key]
+        return None, {"flag": 2 if key == (8, 20) else 0}  # the fastest shape fails here
+
+    clock = {"now": 0.0}
+
+    class Event:
+        def __init__(self, enable_timing=False):
+            self.t = None
+
+        def record(self, stream=None):
+            self.t = clock["now"]
+
+        def elapsed_time(self, other):
+            return other.t - self.t
+
+    monkeypatch.setattr(engine, "solve", fake_solve)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    monkeypatch.setattr(torch.cuda, "Event", Event)
+
+    class Mat:
+        n, nnz, is_complex = 1000, 15000, False
+
+    tuner = engine.SolveTuner()
+    B = torch.zeros(1000, 32)
+    best = tuner.options(Mat, B, precision="mixed")
+    assert (best["spmm_lanes"], best["check_every"]) == (16, 10)
+    assert len(calls) == 1 + 8  # a warm-up, then every candidate once
+    calls.clear()
+    assert tuner.options(Mat, torch.zeros(1000, 32), precision="mixed") is best  # same bucket: cached
+    assert calls == []
+
+    class Big:
+        n, nnz, is_complex = 4000, 60000, False
+
+    tuner.options(Big, torch.zeros(4000, 32), precision="mixed")
+    assert len(calls) == 9  # another size bucket is tuned again
