@@ -255,3 +255,35 @@ def test_solve_tuner_picks_the_fastest_and_caches_per_bucket(monkeypatch):
 
     tuner.options(Big, torch.zeros(4000, 32), precision="mixed")
     assert len(calls) == 9  # another size bucket is tuned again
+
+
+def test_captured_step_budget_rule(monkeypatch):
+    """The fixed solve budget of a captured step: one checked solve, its
+    sweep count and 1.25 x the most iterations a sweep took (at least 8),
+    cached per (nodes, nonzeros, columns, precision, lanes) so that models of
+    one size share it; a solve that did not converge raises."""
+    torch = pytest.importorskip("torch")
+    from redbirdpy_b200 import adjoint
+
+    infos = [{"flag": 0, "outer": 3, "sweep_iters_max": 41}, {"flag": 0, "outer": 1, "sweep_iters_max": 2},
+             {"flag": 1, "outer": 9, "sweep_iters_max": 500}]
+    monkeypatch.setattr(adjoint.engine, "assemble", lambda mesh, optics: None)
+    monkeypatch.setattr(adjoint.engine, "solve", lambda mat, B, **kw: (None, infos.pop(0)))
+    monkeypatch.setattr(adjoint, "_BUDGETS", {})
+
+    def model(nn, nnz):
+        m = object.__new__(adjoint.DeviceModel)
+        m.mesh = type("Mesh", (), {"nn": nn, "nnz": nnz})()
+        m.B = torch.zeros(nn, 16)
+        m.solve_kw = {"precision": "mixed", "budget": (1, 1)}
+        m.optics = lambda mua, dco: None
+        return m
+
+    x = torch.zeros(3)
+    a = model(1000, 15000)
+    assert a.calibrate_budget(x, x) == (3, 52)  # ceil(1.25 * 41)
+    assert model(1000, 15000).calibrate_budget(x, x) == (3, 52)  # same size: cached, no solve
+    assert len(infos) == 2
+    assert model(2000, 30000).calibrate_budget(x, x) == (1, 8)  # floor of 8 iterations
+    with pytest.raises(RuntimeError):
+        model(3000, 45000).calibrate_budget(x, x)
