@@ -287,3 +287,26 @@ def test_captured_step_budget_rule(monkeypatch):
     assert model(2000, 30000).calibrate_budget(x, x) == (1, 8)  # floor of 8 iterations
     with pytest.raises(RuntimeError):
         model(3000, 45000).calibrate_budget(x, x)
+
+
+def test_instances_host_layout():
+    """Instance row offsets: the row -> instance map (zero-row instances
+    allowed), the checks on the offsets, and the status codes the header
+    documents for rb_instances."""
+    torch = pytest.importorskip("torch")
+    from redbirdpy_b200 import engine
+
+    inst = engine.Instances([0, 3, 3, 7], "cpu")
+    assert inst.ninst == 3 and inst.n == 7
+    assert inst.row_inst.tolist() == [0, 0, 0, 2, 2, 2, 2]
+    assert inst.row_ptr.tolist() == [0, 3, 3, 7]
+    for bad in ([1, 3], [0, 5, 4], [0], [[0, 1]]):
+        with pytest.raises(ValueError):
+            engine.Instances(bad, "cpu")
+    src = open(os.path.join(ROOT, "include", "redbird_b200.h")).read()
+    text = re.search(r"int32_t\* status;\s*/\*(.*?)\*/", src, flags=re.S).group(1)
+    text = " ".join(text.split())
+    for code, word in ((0, "converged"), (1, "not converged"), (2, "breakdown"), (3, "non-finite"), (4, "gave up")):
+        assert f"{code} {word}" in text or f"{code} Krylov {word}" in text or f"{code} a bounded in-kernel wait {word}" \
+            in text, (code, text)
+    assert sorted(engine.INSTANCE_STATUS) == [0, 1, 2, 3, 4]
